@@ -1,0 +1,186 @@
+"""TEST INFRASTRUCTURE: ctypes access to the two CPU oracles.
+
+* ``ref``  -- oracle/_ref/libcyclops_ref.so: the reference Cyclops engine
+  compiled from its own sources (oracle/Makefile) driven by ref_harness.cpp.
+* ``port`` -- oracle/_ref/libccd_oracle.so: the plain-C restatement
+  (oracle/ccd_oracle.c).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this
+module.  Nothing in the product package does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("model", C.c_int), ("K", C.c_int), ("J", C.c_int),
+        ("pid", C.c_void_p), ("y", C.c_void_p), ("time", C.c_void_p),
+        ("col_format", C.c_void_p), ("col_ptr", C.c_void_p), ("col_idx", C.c_void_p),
+        ("val_ptr", C.c_void_p), ("col_val", C.c_void_p),
+        ("has_offset", C.c_int), ("has_intercept", C.c_int),
+        ("prior_type", C.c_int), ("variance", C.c_double),
+        ("exclude", C.c_void_p), ("n_exclude", C.c_int),
+        ("weights", C.c_void_p),
+    ]
+
+
+class Control(C.Structure):
+    _fields_ = [
+        ("tolerance", C.c_double), ("max_iterations", C.c_int),
+        ("convergence_type", C.c_int), ("use_kkt_swindle", C.c_int),
+        ("initial_bound", C.c_double), ("max_bound_count", C.c_int),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("beta", C.c_void_p), ("log_likelihood", C.c_double), ("log_prior", C.c_double),
+        ("iterations", C.c_int), ("return_flag", C.c_int),
+    ]
+
+
+@dataclasses.dataclass
+class Fit:
+    beta: np.ndarray
+    log_likelihood: float
+    log_prior: float
+    iterations: int
+    return_flag: int
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+def make_problem(data, prior_type=1, variance=1.0, exclude=None, weights=None):
+    """Returns (Problem, keepalive) for a cyclops_b200.data.CyclopsData."""
+    if exclude is None:
+        exclude = [1 if data.has_offset else 0] if data.has_intercept else []
+    keep = {
+        "pid": None if data.pid is None else np.ascontiguousarray(data.pid, np.int32),
+        "y": np.ascontiguousarray(data.y, np.float64),
+        "time": None if data.time is None else np.ascontiguousarray(data.time, np.float64),
+        "fmt": np.ascontiguousarray(data.col_format, np.int32),
+        "cp": np.ascontiguousarray(data.col_ptr, np.int64),
+        "ci": np.ascontiguousarray(data.col_idx, np.int32),
+        "vp": np.ascontiguousarray(data.val_ptr, np.int64),
+        "cv": np.ascontiguousarray(data.col_val, np.float64),
+        "ex": np.ascontiguousarray(exclude, np.int32),
+        "w": None if weights is None else np.ascontiguousarray(weights, np.float64),
+    }
+    p = Problem(
+        model=data.model, K=data.K, J=data.J, pid=_ptr(keep["pid"]), y=_ptr(keep["y"]),
+        time=_ptr(keep["time"]), col_format=_ptr(keep["fmt"]), col_ptr=_ptr(keep["cp"]),
+        col_idx=_ptr(keep["ci"]), val_ptr=_ptr(keep["vp"]), col_val=_ptr(keep["cv"]),
+        has_offset=int(data.has_offset), has_intercept=int(data.has_intercept),
+        prior_type=prior_type, variance=variance, exclude=_ptr(keep["ex"]),
+        n_exclude=len(exclude), weights=_ptr(keep["w"]))
+    return p, keep
+
+
+def make_control(tolerance=1e-6, max_iterations=1000, convergence_type=0, use_kkt_swindle=0,
+                 initial_bound=2.0, max_bound_count=5) -> Control:
+    """Defaults are the reference's ModeFindingArguments (src/cyclops/CcdInterface.h:70-94)."""
+    return Control(tolerance=tolerance, max_iterations=max_iterations,
+                   convergence_type=convergence_type, use_kkt_swindle=use_kkt_swindle,
+                   initial_bound=initial_bound, max_bound_count=max_bound_count)
+
+
+def build(quiet: bool = True) -> None:
+    """Build the oracle libraries (the reference engine only where its sources exist)."""
+    cmd = ["make", "-C", HERE, "-j8"]
+    subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL if quiet else None)
+
+
+class _Lib:
+    def __init__(self, name, prefix):
+        path = os.path.join(REF_DIR, name)
+        if not os.path.exists(path):
+            build()
+        self.lib = C.CDLL(path)
+        self.prefix = prefix
+        le = getattr(self.lib, prefix + "last_error")
+        le.restype = C.c_char_p
+        self._last_error = le
+
+    def err(self) -> str:
+        return self._last_error().decode()
+
+    def fit(self, data, prior_type=1, variance=1.0, control: Optional[Control] = None,
+            exclude=None, weights=None, start=None) -> Fit:
+        p, keep = make_problem(data, prior_type, variance, exclude, weights)
+        c = control or make_control()
+        beta = np.zeros(data.J)
+        r = Result(beta=beta.ctypes.data)
+        s = None if start is None else np.ascontiguousarray(start, np.float64)
+        rc = getattr(self.lib, self.prefix + "fit")(C.byref(p), C.byref(c), _ptr(s), C.byref(r))
+        if rc:
+            raise RuntimeError(self.err())
+        return Fit(beta, r.log_likelihood, r.log_prior, r.iterations, r.return_flag)
+
+    def probe(self, data, beta, prior_type=1, variance=1.0, exclude=None, weights=None):
+        p, keep = make_problem(data, prior_type, variance, exclude, weights)
+        b = np.ascontiguousarray(beta, np.float64)
+        g = np.zeros(data.J)
+        h = np.zeros(data.J)
+        xb = np.zeros(data.K)
+        ll = C.c_double()
+        fn = getattr(self.lib, self.prefix + ("engine_probe" if self.prefix == "ref_" else "probe"))
+        rc = fn(C.byref(p), _ptr(b), _ptr(g), _ptr(h), _ptr(xb), C.byref(ll))
+        if rc:
+            raise RuntimeError(self.err())
+        return g, h, xb, ll.value
+
+    def predictive_loglik(self, data, beta, held_out, weights=None):
+        p, keep = make_problem(data, 1, 1.0, None, weights)
+        b = np.ascontiguousarray(beta, np.float64)
+        w = np.ascontiguousarray(held_out, np.float64)
+        out = C.c_double()
+        rc = getattr(self.lib, self.prefix + "predictive_loglik")(C.byref(p), _ptr(b), _ptr(w),
+                                                                   C.byref(out))
+        if rc:
+            raise RuntimeError(self.err())
+        return out.value
+
+
+_cache = {}
+
+
+def ref() -> _Lib:
+    """The reference engine (raises if it cannot be built here)."""
+    if "ref" not in _cache:
+        _cache["ref"] = _Lib("libcyclops_ref.so", "ref_")
+    return _cache["ref"]
+
+
+def port() -> _Lib:
+    """The plain-C restatement."""
+    if "port" not in _cache:
+        _cache["port"] = _Lib("libccd_oracle.so", "ccd_oracle_")
+    return _cache["port"]
+
+
+def have_ref() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libcyclops_ref.so"))
+
+
+def ref_cv_weights(K, ids, fold, seed, by_row=True, n_reps=1) -> np.ndarray:
+    lib = ref().lib
+    ids = np.ascontiguousarray(ids, np.int32)
+    out = np.zeros((n_reps * fold, K))
+    rc = lib.ref_cv_weights(C.c_int(K), _ptr(ids), C.c_int(fold), C.c_long(seed),
+                            C.c_int(int(by_row)), C.c_int(n_reps), _ptr(out))
+    if rc:
+        raise RuntimeError(ref().err())
+    return out

@@ -1,0 +1,296 @@
+// ref_harness.cpp -- TEST INFRASTRUCTURE (oracle).
+//
+// A C-ABI driver around the reference Cyclops C++ engine, compiled from the
+// reference's own sources (oracle/Makefile) into oracle/_ref/libcyclops_ref.so.
+// It is the parity checker for the CUDA path and the "reference" CPU
+// baseline; it is never linked into the product library.
+//
+// What it mirrors:
+//   * data ingest       RcppModelData ctor      src/RcppModelData.cpp:751-900
+//                       (offset column first, dense, sparse, indicator; pid
+//                       renumbered by runs, :878-900)
+//   * prior set-up      .cyclopsSetPrior with the intercept excluded
+//                       R/ModelFit.R:120-144 -> MixtureJointPrior::changePrior
+//                       src/cyclops/priors/JointPrior.h:81-90
+//   * fit               CcdInterface::fitModel -> CyclicCoordinateDescent::update
+//                       src/cyclops/CcdInterface.cpp:654-672,
+//                       src/cyclops/CyclicCoordinateDescent.cpp:586-615
+//   * CV fold masks     CrossValidationSelector  src/cyclops/drivers/CrossValidationSelector.cpp:21-116
+//   * engine probes     AbstractModelSpecifics virtuals, called directly on the
+//                       same engine object the CCD uses.
+#include <cstring>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "CyclicCoordinateDescent.h"
+#include "ModelData.h"
+#include "engine/AbstractModelSpecifics.h"
+#include "priors/JointPrior.h"
+#include "priors/CovariatePrior.h"
+#include "drivers/CrossValidationSelector.h"
+#include "io/ProgressLogger.h"
+
+#ifdef CYC_REF_WITH_CUDA_ADAPTER
+#include "CudaModelSpecifics.h"
+#endif
+
+extern "C" {
+#include "ref_harness.h"
+}
+
+using namespace bsccs;
+
+namespace {
+
+thread_local std::string g_error;
+
+class QuietLogger : public loggers::ProgressLogger {
+public:
+    void writeLine(const std::ostringstream&) override {}
+    void yield() override {}
+};
+
+class ThrowingErrorHandler : public loggers::ErrorHandler {
+public:
+    void throwError(const std::ostringstream& stream) override {
+        throw std::runtime_error(stream.str());
+    }
+};
+
+// ModelData subclass that takes plain arrays, in the ingest order of
+// RcppModelData (src/RcppModelData.cpp:751-900).
+class HarnessModelData : public ModelData<double> {
+public:
+    HarnessModelData(ModelType type, const ref_problem* p,
+                     std::vector<int> pid, std::vector<double> y, std::vector<double> time)
+        : ModelData<double>(type, pid, y, std::vector<double>(), time,
+                            bsccs::make_shared<QuietLogger>(),
+                            bsccs::make_shared<ThrowingErrorHandler>()) {
+        const int K = p->K;
+        for (int j = 0; j < p->J; ++j) {
+            const long long b = p->col_ptr[j];
+            const long long e = p->col_ptr[j + 1];
+            const long long vb = p->val_ptr[j];
+            switch (p->col_format[j]) {
+            case REF_DENSE:
+                X.push_back((int*)nullptr, (int*)nullptr, p->col_val + vb, p->col_val + vb + K, DENSE);
+                break;
+            case REF_SPARSE:
+                X.push_back(p->col_idx + b, p->col_idx + e, p->col_val + vb, p->col_val + vb + (e - b), SPARSE);
+                break;
+            case REF_INDICATOR:
+                X.push_back(p->col_idx + b, p->col_idx + e, (double*)nullptr, (double*)nullptr, INDICATOR);
+                break;
+            case REF_INTERCEPT:
+                X.push_back((int*)nullptr, (int*)nullptr, (double*)nullptr, (double*)nullptr, INTERCEPT);
+                break;
+            default:
+                throw std::runtime_error("unknown column format");
+            }
+            X.getColumn(X.getNumberOfColumns() - 1).add_label(j);
+        }
+        X.nRows = K;
+        if (p->has_offset) setHasOffsetCovariate(true);
+        if (p->has_intercept) setHasInterceptCovariate(true);
+        // pid renumbering by runs (RcppModelData.cpp:878-900)
+        std::vector<int>& cpid = getPidVectorRef();
+        if (cpid.empty()) {
+            for (int i = 0; i < K; ++i) cpid.push_back(i);
+            nPatients = K;
+        } else {
+            int current = 0;
+            int last = cpid[0];
+            cpid[0] = 0;
+            for (size_t i = 1; i < cpid.size(); ++i) {
+                if (cpid[i] != last) { ++current; last = cpid[i]; }
+                cpid[i] = current;
+            }
+            nPatients = current + 1;
+        }
+    }
+};
+
+ModelType toModelType(int m) {
+    switch (m) {
+    case REF_LR: return ModelType::LOGISTIC;
+    case REF_PR: return ModelType::POISSON;
+    case REF_CLR: return ModelType::CONDITIONAL_LOGISTIC;
+    case REF_CPR: return ModelType::CONDITIONAL_POISSON;
+    case REF_COX: return ModelType::COX;
+    default: throw std::runtime_error("unknown model type");
+    }
+}
+
+priors::PriorPtr makeCovariatePrior(int type, double variance) {
+    switch (type) {
+    case REF_PRIOR_NONE: return bsccs::make_shared<priors::NoPrior>();
+    case REF_PRIOR_LAPLACE: return bsccs::make_shared<priors::LaplacePrior>(variance);
+    case REF_PRIOR_NORMAL: return bsccs::make_shared<priors::NormalPrior>(variance);
+    default: throw std::runtime_error("unknown prior type");
+    }
+}
+
+struct Instance {
+    std::unique_ptr<HarnessModelData> data;
+    std::unique_ptr<AbstractModelSpecifics> engine;
+    std::unique_ptr<CyclicCoordinateDescent> ccd;
+    bool useWeights = false;
+};
+
+std::unique_ptr<Instance> build(const ref_problem* p, int device) {
+    std::vector<int> pid;
+    if (p->pid) pid.assign(p->pid, p->pid + p->K);
+    std::vector<double> y(p->y, p->y + p->K);
+    std::vector<double> time;
+    if (p->time) time.assign(p->time, p->time + p->K);
+
+    auto inst = std::unique_ptr<Instance>(new Instance());
+    inst->data.reset(new HarnessModelData(toModelType(p->model), p, pid, y, time));
+    if (device == 0) {
+        inst->engine.reset(AbstractModelSpecifics::factory(
+            toModelType(p->model), *inst->data, DeviceType::CPU, ""));
+    } else {
+#ifdef CYC_REF_WITH_CUDA_ADAPTER
+        inst->engine.reset(cyclops_b200::makeCudaModelSpecifics(
+            toModelType(p->model), *inst->data));
+#else
+        throw std::runtime_error("harness built without the CUDA adapter");
+#endif
+    }
+    if (!inst->engine) throw std::runtime_error("Invalid model type.");
+
+    auto defaultPrior = makeCovariatePrior(p->prior_type, p->variance);
+    auto joint = bsccs::make_shared<priors::MixtureJointPrior>(defaultPrior, p->J);
+    for (int i = 0; i < p->n_exclude; ++i) {
+        joint->changePrior(bsccs::make_shared<priors::NoPrior>(), p->exclude[i]);
+    }
+    inst->ccd.reset(new CyclicCoordinateDescent(
+        *inst->data, *inst->engine, joint,
+        bsccs::make_shared<QuietLogger>(), bsccs::make_shared<ThrowingErrorHandler>()));
+    inst->ccd->setNoiseLevel(SILENT);
+    if (p->weights) {
+        std::vector<double> w(p->weights, p->weights + p->K);
+        inst->ccd->setWeights(w.data());
+        inst->useWeights = true;
+    }
+    return inst;
+}
+
+ModeFindingArguments toArguments(const ref_control* c) {
+    ModeFindingArguments a;
+    a.tolerance = c->tolerance;
+    a.maxIterations = c->max_iterations;
+    a.convergenceType = c->convergence_type;
+    a.useKktSwindle = c->use_kkt_swindle != 0;
+    a.initialBound = c->initial_bound;
+    a.maxBoundCount = c->max_bound_count;
+    return a;
+}
+
+template <class F>
+int guarded(F f) {
+    try {
+        f();
+        return 0;
+    } catch (const std::exception& e) {
+        g_error = e.what();
+        return 1;
+    } catch (const std::exception* e) {  // the engine throws pointers (ModelSpecifics.h:417)
+        g_error = e->what();
+        return 1;
+    } catch (...) {
+        g_error = "unknown exception";
+        return 1;
+    }
+}
+
+void fillResult(Instance& inst, int J, ref_result* out) {
+    for (int j = 0; j < J; ++j) out->beta[j] = inst.ccd->getBeta(j);
+    out->log_likelihood = inst.ccd->getLogLikelihood();
+    out->log_prior = inst.ccd->getLogPrior();
+    out->iterations = inst.ccd->getIterationCount();
+    out->return_flag = (int)inst.ccd->getUpdateReturnFlag();
+}
+
+int fitWithDevice(const ref_problem* p, const ref_control* c, const double* start, ref_result* out,
+                  int device) {
+    return guarded([&] {
+        auto inst = build(p, device);
+        if (start) {
+            std::vector<double> b(start, start + p->J);
+            inst->ccd->setBeta(b);
+        }
+        inst->ccd->update(toArguments(c));
+        fillResult(*inst, p->J, out);
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error(void) { return g_error.c_str(); }
+
+int ref_fit(const ref_problem* p, const ref_control* c, const double* start_beta, ref_result* out) {
+    return fitWithDevice(p, c, start_beta, out, 0);
+}
+
+int ref_fit_device(const ref_problem* p, const ref_control* c, const double* start_beta,
+                   ref_result* out, int device) {
+    return fitWithDevice(p, c, start_beta, out, device);
+}
+
+int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient, double* hessian,
+                     double* xbeta, double* log_likelihood) {
+    return guarded([&] {
+        auto inst = build(p, 0);
+        std::vector<double> b(beta, beta + p->J);
+        inst->ccd->setBeta(b);
+        *log_likelihood = inst->ccd->getLogLikelihood();  // runs the lazy set-up
+        const bool w = inst->useWeights;
+        for (int j = 0; j < p->J; ++j) {
+            inst->engine->computeNumeratorForGradient(j, w);
+            inst->engine->computeGradientAndHessian(j, gradient + j, hessian + j, w);
+        }
+        if (xbeta) {
+            auto xb = inst->engine->getXBeta();
+            std::memcpy(xbeta, xb.data(), sizeof(double) * p->K);
+        }
+    });
+}
+
+int ref_predictive_loglik(const ref_problem* p, const double* beta, const double* held_out,
+                          double* out) {
+    return guarded([&] {
+        auto inst = build(p, 0);
+        std::vector<double> b(beta, beta + p->J);
+        inst->ccd->setBeta(b);
+        inst->ccd->getLogLikelihood();
+        std::vector<double> w(held_out, held_out + p->K);
+        *out = inst->ccd->getNewPredictiveLogLikelihood(w.data());
+    });
+}
+
+int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n_reps,
+                   double* out /* n_reps*fold x K */) {
+    return guarded([&] {
+        std::vector<int> idv(ids, ids + K);
+        auto logger = bsccs::make_shared<QuietLogger>();
+        auto err = bsccs::make_shared<ThrowingErrorHandler>();
+        CrossValidationSelector sel(fold, idv, by_row ? SelectorType::BY_ROW : SelectorType::BY_PID,
+                                    seed, logger, err, nullptr, nullptr);
+        sel.reseed();
+        std::vector<double> w;
+        for (int task = 0; task < n_reps * fold; ++task) {
+            const int f = task % fold;
+            if (f == 0) sel.permute();
+            sel.getWeights(f, w);
+            std::memcpy(out + (size_t)task * K, w.data(), sizeof(double) * K);
+        }
+    });
+}
+
+}  // extern "C"

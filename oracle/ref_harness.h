@@ -1,0 +1,58 @@
+/* ref_harness.h -- TEST INFRASTRUCTURE (oracle).
+ * C ABI of oracle/_ref/libcyclops_ref.so, the reference Cyclops CPU engine
+ * built from its own sources.  Used only by tests/ and bench.py's CPU legs. */
+#ifndef CYC_REF_HARNESS_H
+#define CYC_REF_HARNESS_H
+
+enum { REF_LR = 0, REF_PR = 1, REF_CLR = 2, REF_CPR = 3, REF_COX = 4 };
+enum { REF_DENSE = 0, REF_SPARSE = 1, REF_INDICATOR = 2, REF_INTERCEPT = 3 };
+enum { REF_PRIOR_NONE = 0, REF_PRIOR_LAPLACE = 1, REF_PRIOR_NORMAL = 2 };
+
+typedef struct {
+    int model;               /* REF_LR ... */
+    int K;                   /* rows */
+    int J;                   /* columns (incl. offset / intercept) */
+    const int* pid;          /* K raw stratum ids, or NULL (one row per stratum) */
+    const double* y;         /* K outcomes */
+    const double* time;      /* K times / offsets, or NULL */
+    const int* col_format;   /* J formats */
+    const long long* col_ptr;/* J+1 offsets into col_idx (SPARSE, INDICATOR entries) */
+    const int* col_idx;      /* row ids, ascending within a column */
+    const long long* val_ptr;/* J+1 offsets into col_val (SPARSE: nnz, DENSE: K, else 0) */
+    const double* col_val;   /* values */
+    int has_offset;          /* column 0 is a fixed offset (beta = 1) */
+    int has_intercept;
+    int prior_type;
+    double variance;
+    const int* exclude;      /* column indices with a flat prior */
+    int n_exclude;
+    const double* weights;   /* K weights or NULL */
+} ref_problem;
+
+typedef struct {
+    double tolerance;
+    int max_iterations;
+    int convergence_type;    /* 0 gradient, 1 lange, 2 mittal, 3 one_step, 4 zhang_oles */
+    int use_kkt_swindle;
+    double initial_bound;
+    int max_bound_count;
+} ref_control;
+
+typedef struct {
+    double* beta;            /* J, caller-owned */
+    double log_likelihood;
+    double log_prior;
+    int iterations;
+    int return_flag;
+} ref_result;
+
+const char* ref_last_error(void);
+int ref_fit(const ref_problem* p, const ref_control* c, const double* start_beta, ref_result* out);
+int ref_fit_device(const ref_problem* p, const ref_control* c, const double* start_beta,
+                   ref_result* out, int device);
+int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient, double* hessian,
+                     double* xbeta, double* log_likelihood);
+int ref_predictive_loglik(const ref_problem* p, const double* beta, const double* held_out,
+                          double* out);
+int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n_reps, double* out);
+#endif
