@@ -1,0 +1,312 @@
+"""Host API mirroring the reference's user-facing surface for this path.
+
+    data    = cyclops_b200.data.CyclopsData(...)          # createCyclopsData
+    prior   = create_prior("laplace", variance=200)       # createPrior (R/ModelFit.R:574)
+    control = create_control(tolerance=1e-6)              # createControl (R/ModelFit.R:489)
+    fit     = fit_cyclops_model(data, prior, control)     # fitCyclopsModel (R/ModelFit.R:65)
+
+plus `Engine`, the per-coordinate AbstractModelSpecifics surface, and
+`batch_fit`, many fits sharing one dataset on the GPU.  Every call goes
+through libcyclops_b200.so; nothing here computes on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import _native as N
+from .data import (CONV_GRADIENT, CONV_LANGE, CONV_MITTAL, CONV_ONE_STEP, CONV_ZHANG_OLES,
+                   PRIOR_LAPLACE, PRIOR_NONE, PRIOR_NORMAL, CyclopsData)
+
+FP64, MIXED = 0, 1
+
+_PRIORS = {"none": PRIOR_NONE, "laplace": PRIOR_LAPLACE, "normal": PRIOR_NORMAL}
+_CONV = {"gradient": CONV_GRADIENT, "lange": CONV_LANGE, "mittal": CONV_MITTAL,
+         "onestep": CONV_ONE_STEP, "zhang-oles": CONV_ZHANG_OLES}
+
+
+@dataclasses.dataclass
+class PriorSpec:
+    prior_type: int = PRIOR_LAPLACE
+    variance: float = 1.0
+    exclude: Optional[Sequence[int]] = None      # None: exclude the intercept
+    force_intercept: bool = False
+
+
+def create_prior(prior_type: str = "none", variance: float = 1.0, exclude=None,
+                 force_intercept: bool = False) -> PriorSpec:
+    """createPrior (R/ModelFit.R:574-617).  `variance` is the prior variance;
+    a Laplace prior has rate lambda = sqrt(2/variance)."""
+    if prior_type not in _PRIORS:
+        raise ValueError(f"unknown prior type {prior_type!r}")
+    return PriorSpec(_PRIORS[prior_type], float(variance), exclude, force_intercept)
+
+
+@dataclasses.dataclass
+class ControlSpec:
+    tolerance: float = 1e-6
+    max_iterations: int = 1000
+    convergence_type: int = CONV_GRADIENT
+    initial_bound: float = 2.0
+    max_bound_count: int = 5
+    precision: int = FP64
+    polish_tolerance: float = 1e-4
+
+
+def create_control(tolerance=1e-6, max_iterations=1000, convergence_type="gradient",
+                   initial_bound=2.0, max_bound_count=5, precision="fp64",
+                   polish_tolerance=1e-4) -> ControlSpec:
+    """createControl (R/ModelFit.R:489-540); defaults are the reference's."""
+    ct = _CONV[convergence_type] if isinstance(convergence_type, str) else int(convergence_type)
+    pr = {"fp64": FP64, "mixed": MIXED}[precision] if isinstance(precision, str) else int(precision)
+    return ControlSpec(tolerance, max_iterations, ct, initial_bound, max_bound_count, pr,
+                       polish_tolerance)
+
+
+def _exclude_for(data: CyclopsData, prior: PriorSpec) -> List[int]:
+    """The intercept is excluded from regularisation unless forced
+    (R/ModelFit.R:120-144)."""
+    if prior.exclude is not None:
+        return list(prior.exclude)
+    if prior.prior_type != PRIOR_NONE and data.has_intercept and not prior.force_intercept:
+        return [1 if data.has_offset else 0]
+    return []
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+class Dataset:
+    """A CyclopsData copied to device `device` (cyc_dataset_create)."""
+
+    def __init__(self, data: CyclopsData, device: int = 0):
+        self.data = data
+        self.device = device
+        keep = {
+            "pid": None if data.pid is None else np.ascontiguousarray(data.pid, np.int32),
+            "y": np.ascontiguousarray(data.y, np.float64),
+            "time": None if data.time is None else np.ascontiguousarray(data.time, np.float64),
+            "fmt": np.ascontiguousarray(data.col_format, np.int32),
+            "cp": np.ascontiguousarray(data.col_ptr, np.int64),
+            "ci": np.ascontiguousarray(data.col_idx, np.int32),
+            "vp": np.ascontiguousarray(data.val_ptr, np.int64),
+            "cv": np.ascontiguousarray(data.col_val, np.float64),
+        }
+        d = N.DataDesc(model=data.model, K=data.K, J=data.J, pid=_ptr(keep["pid"]), y=_ptr(keep["y"]),
+                       time=_ptr(keep["time"]), col_format=_ptr(keep["fmt"]), col_ptr=_ptr(keep["cp"]),
+                       col_idx=_ptr(keep["ci"]) if data.nnz else None, val_ptr=_ptr(keep["vp"]),
+                       col_val=_ptr(keep["cv"]) if keep["cv"].size else None,
+                       has_offset=int(data.has_offset), has_intercept=int(data.has_intercept))
+        h = C.c_void_p()
+        N.check(N.lib().cyc_dataset_create(C.byref(d), device, C.byref(h)))
+        self.handle = h
+
+    def info(self):
+        K, J, nnz, b = C.c_int(), C.c_int(), C.c_longlong(), C.c_size_t()
+        N.check(N.lib().cyc_dataset_info(self.handle, C.byref(K), C.byref(J), C.byref(nnz), C.byref(b)))
+        return {"K": K.value, "J": J.value, "nnz": nnz.value, "device_bytes": b.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            N.lib().cyc_dataset_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Engine:
+    """The AbstractModelSpecifics surface (src/cyclops/engine/AbstractModelSpecifics.h:46-122)."""
+
+    def __init__(self, dataset: Dataset, _handle=None):
+        self.dataset = dataset
+        if _handle is None:
+            h = C.c_void_p()
+            N.check(N.lib().cyc_engine_create(dataset.handle, C.byref(h)))
+            _handle = h
+        self.handle = _handle
+        self.K = dataset.data.K
+        self.J = dataset.data.J
+
+    def clone(self) -> "Engine":
+        h = C.c_void_p()
+        N.check(N.lib().cyc_engine_clone(self.handle, C.byref(h)))
+        return Engine(self.dataset, h)
+
+    def set_weights(self, w=None, use_cv=None):
+        self._w = None if w is None else np.ascontiguousarray(w, np.float64)
+        uc = int(w is not None) if use_cv is None else int(use_cv)
+        N.check(N.lib().cyc_engine_set_weights(self.handle, _ptr(self._w), uc))
+
+    def compute_fixed_terms_in_log_likelihood(self, use_cv=False):
+        N.check(N.lib().cyc_engine_compute_fixed_terms_ll(self.handle, int(use_cv)))
+
+    def compute_fixed_terms_in_gradient_and_hessian(self, use_cv=False):
+        N.check(N.lib().cyc_engine_compute_fixed_terms_gh(self.handle, int(use_cv)))
+
+    def zero_xbeta(self):
+        N.check(N.lib().cyc_engine_zero_xbeta(self.handle))
+
+    def axpy_xbeta(self, beta: float, j: int):
+        N.check(N.lib().cyc_engine_axpy_xbeta(self.handle, float(beta), int(j)))
+
+    def compute_xbeta(self, beta, use_w=False):
+        b = np.ascontiguousarray(beta, np.float64)
+        N.check(N.lib().cyc_engine_compute_xbeta(self.handle, _ptr(b), int(use_w)))
+
+    def compute_remaining_statistics(self, use_w=False):
+        N.check(N.lib().cyc_engine_compute_remaining_statistics(self.handle, int(use_w)))
+
+    def compute_numerator_for_gradient(self, j, use_w=False):
+        N.check(N.lib().cyc_engine_compute_numerator_for_gradient(self.handle, int(j), int(use_w)))
+
+    def compute_gradient_and_hessian(self, j, use_w=False):
+        g, h = C.c_double(), C.c_double()
+        N.check(N.lib().cyc_engine_compute_gradient_and_hessian(self.handle, int(j), C.byref(g),
+                                                                C.byref(h), int(use_w)))
+        return g.value, h.value
+
+    def update_xbeta(self, delta, j, use_w=False):
+        N.check(N.lib().cyc_engine_update_xbeta(self.handle, float(delta), int(j), int(use_w)))
+
+    def get_log_likelihood(self, use_cv=False):
+        v = C.c_double()
+        N.check(N.lib().cyc_engine_get_log_likelihood(self.handle, int(use_cv), C.byref(v)))
+        return v.value
+
+    def get_gradient_objective(self, use_cv=False):
+        v = C.c_double()
+        N.check(N.lib().cyc_engine_get_gradient_objective(self.handle, int(use_cv), C.byref(v)))
+        return v.value
+
+    def get_predictive_log_likelihood(self, w):
+        w = np.ascontiguousarray(w, np.float64)
+        v = C.c_double()
+        N.check(N.lib().cyc_engine_get_predictive_log_likelihood(self.handle, _ptr(w), C.byref(v)))
+        return v.value
+
+    def get_predictive_estimates(self, w=None):
+        y = np.zeros(self.K)
+        ww = None if w is None else np.ascontiguousarray(w, np.float64)
+        N.check(N.lib().cyc_engine_get_predictive_estimates(self.handle, _ptr(y), _ptr(ww)))
+        return y
+
+    def get_xbeta(self):
+        out = np.zeros(self.K)
+        N.check(N.lib().cyc_engine_get_xbeta(self.handle, _ptr(out)))
+        return out
+
+    def save_xbeta(self):
+        N.check(N.lib().cyc_engine_save_xbeta(self.handle))
+
+    def get_xbeta_save(self):
+        out = np.zeros(self.K)
+        N.check(N.lib().cyc_engine_get_xbeta_save(self.handle, _ptr(out)))
+        return out
+
+    def n_denominators(self) -> int:
+        n = C.c_int()
+        N.check(N.lib().cyc_engine_get_n(self.handle, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            N.lib().cyc_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class FitResult:
+    beta: np.ndarray
+    log_likelihood: float
+    log_prior: float
+    iterations: int
+    return_flag: int
+
+
+def _control_struct(c: ControlSpec) -> N.Control:
+    return N.Control(tolerance=c.tolerance, max_iterations=c.max_iterations,
+                     convergence_type=c.convergence_type, initial_bound=c.initial_bound,
+                     max_bound_count=c.max_bound_count, precision=c.precision,
+                     polish_tolerance=c.polish_tolerance)
+
+
+def _prior_struct(data: CyclopsData, prior: PriorSpec):
+    ex = np.ascontiguousarray(_exclude_for(data, prior), np.int32)
+    return N.Prior(prior_type=prior.prior_type, exclude=_ptr(ex) if ex.size else None,
+                   n_exclude=int(ex.size)), ex
+
+
+def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional[ControlSpec] = None,
+                      weights=None, starting_coefficients=None, device: int = 0) -> FitResult:
+    """fitCyclopsModel (R/ModelFit.R:65): one fit, CCD loop on the GPU."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    prior = prior or create_prior("none")
+    control = control or create_control()
+    p, keep_ex = _prior_struct(ds.data, prior)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    s = None if starting_coefficients is None else np.ascontiguousarray(starting_coefficients, np.float64)
+    spec = N.FitSpec(weights=_ptr(w), variance=prior.variance, start_beta=_ptr(s))
+    beta = np.zeros(ds.data.J)
+    out = N.FitResult(beta=beta.ctypes.data)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_fit(ds.handle, C.byref(p), C.byref(spec), C.byref(c), C.byref(out)))
+    return FitResult(beta, out.log_likelihood, out.log_prior, out.iterations, out.return_flag)
+
+
+def batch_fit(data, prior: PriorSpec, variances: Sequence[float], weights: Optional[Sequence] = None,
+              control: Optional[ControlSpec] = None, starts=None, device: int = 0) -> List[FitResult]:
+    """F fits sharing one dataset, advanced together on the GPU.  `weights` is
+    a list of K-vectors (or None entries) or a (F, K) array."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    control = control or create_control()
+    F = len(variances)
+    p, keep_ex = _prior_struct(ds.data, prior)
+    specs = (N.FitSpec * F)()
+    results = (N.FitResult * F)()
+    keep = []
+    betas = np.zeros((F, ds.data.J))
+    for f in range(F):
+        w = None
+        if weights is not None and weights[f] is not None:
+            w = np.ascontiguousarray(weights[f], np.float64)
+            keep.append(w)
+        s = None
+        if starts is not None and starts[f] is not None:
+            s = np.ascontiguousarray(starts[f], np.float64)
+            keep.append(s)
+        specs[f] = N.FitSpec(weights=_ptr(w), variance=float(variances[f]), start_beta=_ptr(s))
+        results[f] = N.FitResult(beta=betas[f].ctypes.data)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_batch_fit(ds.handle, C.byref(p), specs, F, C.byref(c), results))
+    return [FitResult(betas[f].copy(), results[f].log_likelihood, results[f].log_prior,
+                      results[f].iterations, results[f].return_flag) for f in range(F)]
+
+
+def cv_fold_weights(K: int, folds: int, seed: int, ids=None, n_reps: int = 1) -> np.ndarray:
+    """(n_reps*folds, K) 0/1 masks, by row (ids None) or by stratum id, drawn
+    exactly as the reference's CrossValidationSelector draws them."""
+    out = np.zeros((n_reps * folds, K))
+    idv = None if ids is None else np.ascontiguousarray(ids, np.int32)
+    N.check(N.lib().cyc_cv_fold_weights(int(K), _ptr(idv), int(folds), int(seed), int(ids is None),
+                                        int(n_reps), _ptr(out)))
+    return out
+
+
+def last_run_stats() -> dict:
+    s = N.RunStats()
+    N.check(N.lib().cyc_last_run_stats(C.byref(s)))
+    return {k: getattr(s, k) for k, _ in N.RunStats._fields_}

@@ -1,0 +1,580 @@
+// engine_kernels.cuh -- FP64 kernels of the per-coordinate engine.
+//
+// Each kernel restates one piece of the reference engine
+// (src/cyclops/engine/ModelSpecifics.hpp) for the GPU; the reference
+// function is named above each kernel.  Reductions are deterministic:
+// per-block partials are combined in block order by the last block
+// (grid_sum2_finalize), so a result does not depend on scheduling.
+#pragma once
+#include "internal.cuh"
+
+namespace cyc {
+
+// ---- weights ---------------------------------------------------------------
+
+// setWeights, hKWeight (ModelSpecifics.hpp:428-440)
+__global__ void k_set_kw(int K, const double* __restrict__ w, double* __restrict__ kw) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        kw[k] = w ? w[k] : 1.0;
+}
+
+// setWeights, hNWeight for independent rows: 0 + observationCount(y)*w (:451-455)
+__global__ void k_nw_independent(int K, const double* __restrict__ kw, double* __restrict__ nw) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        nw[k] = 0.0 + 1.0 * kw[k];
+}
+
+// setWeights, hNWeight for grouped rows: per-group sequential sum of y*w in row
+// order (same order as the reference's incrementByGroup loop, :451-455)
+__global__ void k_nw_grouped(int G, const int* __restrict__ grow_ptr, const double* __restrict__ y,
+                             const double* __restrict__ kw, double* __restrict__ nw) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = grow_ptr[g]; k < grow_ptr[g + 1]; ++k) s += y[k] * kw[k];
+        nw[g] = s;
+    }
+}
+
+// computeXjY (ModelSpecifics.hpp:486-524): one block per column
+__global__ void k_xjy(int J, const int* __restrict__ fmt, const long long* __restrict__ col_ptr,
+                      const long long* __restrict__ val_ptr, const int* __restrict__ idx,
+                      const double* __restrict__ val, int K, const double* __restrict__ y,
+                      const double* __restrict__ kw, int use_w, double* __restrict__ xjy) {
+    for (int j = blockIdx.x; j < J; j += gridDim.x) {
+        ColView c;
+        c.fmt = fmt[j];
+        c.n = (c.fmt == CYC_DENSE || c.fmt == CYC_INTERCEPT) ? K : col_ptr[j + 1] - col_ptr[j];
+        c.idx = idx + col_ptr[j];
+        c.val = val + val_ptr[j];
+        double s = 0.0, dummy = 0.0;
+        for (long long e = threadIdx.x; e < c.n; e += blockDim.x) {
+            const int k = c.row(e);
+            s += use_w ? c.x(e) * y[k] * kw[k] : c.x(e) * y[k];
+        }
+        block_sum2(s, dummy);
+        if (threadIdx.x == 0) xjy[j] = s;
+        __syncthreads();
+    }
+}
+
+// computeFixedTermsInLogLikelihood (ModelSpecifics.hpp:570-587): -sum log(y!)
+__global__ void k_fixed_ll(int K, const double* __restrict__ y, const double* __restrict__ kw,
+                           int use_w, double2* partial, unsigned* ticket, double* out) {
+    double s = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        double f = 0.0;
+        for (int i = 2; i <= (int)y[k]; ++i) f -= log((double)i);
+        s += use_w ? f * kw[k] : f;
+    }
+    grid_sum2_finalize(s, 0.0, partial, ticket, [&](double a, double) { *out = a; });
+}
+
+// ---- linear predictor ------------------------------------------------------
+
+// zeroXBeta + axpyXBeta over all columns in order (CyclicCoordinateDescent.cpp:1452-1470)
+__global__ void k_xbeta_rows(int K, const long long* __restrict__ row_ptr, const int* __restrict__ row_col,
+                             const double* __restrict__ row_val, const double* __restrict__ beta,
+                             double* __restrict__ xb) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (long long p = row_ptr[k]; p < row_ptr[k + 1]; ++p) {
+            const double b = beta[row_col[p]];
+            if (b != 0.0) s = add_mul_rn(s, b, row_val[p]);
+        }
+        xb[k] = s;
+    }
+}
+
+// axpy (ModelSpecifics.hpp:384-391)
+__global__ void k_axpy(ColView c, double beta, double* __restrict__ xb) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = c.row(e);
+        xb[k] = add_mul_rn(xb[k], beta, c.x(e));
+    }
+}
+
+// ---- remaining statistics (ModelSpecifics.hpp:1588-1612) --------------------
+
+__global__ void k_rs_independent(int K, int model, const double* __restrict__ xb,
+                                 double* __restrict__ exb, double* __restrict__ denom) {
+    const double nul = denom_null(model);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const double e = exp(xb[k]);
+        exb[k] = e;
+        denom[k] = nul + e;
+    }
+}
+
+// grouped / cumulative: exp per row and a per-group sum in row order
+__global__ void k_rs_grouped(int G, const int* __restrict__ grow_ptr, const double* __restrict__ xb,
+                             const double* __restrict__ kw, int weighted, double* __restrict__ exb,
+                             double* __restrict__ denom) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int k = grow_ptr[g]; k < grow_ptr[g + 1]; ++k) {
+            const double e = exp(xb[k]);
+            exb[k] = e;
+            if (!weighted) s += e;
+            else if (kw[k] != 0.0) s += kw[k] * e;
+        }
+        denom[g] = s;
+    }
+}
+
+// ---- gradient and Hessian ---------------------------------------------------
+
+// independent rows (ModelSpecifics.hpp:1022-1038 with LogisticRegression /
+// PoissonRegression::incrementGradientAndHessian, ModelSpecifics.h:540-568, 1508-1543)
+template <int MODEL, bool IND>
+__global__ void k_gh_independent(ColView c, const double* __restrict__ exb, const double* __restrict__ denom,
+                                 const double* __restrict__ nw, int use_w, const double* __restrict__ xjy, int j,
+                                 double2* partial, unsigned* ticket, double* out) {
+    double g = 0.0, h = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = c.row(e);
+        const double x = c.x(e);
+        const double ex = exb[k];
+        const double n1 = ex * x;
+        const double w = use_w ? nw[k] : 1.0;
+        if (MODEL == CYC_LR) {
+            const double d = denom[k];
+            const double gi = n1 / d;
+            g += w * gi;
+            h += w * (IND ? gi * (1.0 - gi) : (n1 * x / d - gi * gi));
+        } else {
+            g += w * n1;
+            h += w * (IND ? n1 : n1 * x);
+        }
+    }
+    grid_sum2_finalize(g, h, partial, ticket, [&](double G, double H) {
+        out[0] = G - xjy[j];
+        out[1] = H;
+    });
+}
+
+// grouped rows (ModelSpecifics.hpp:1127-1178 with
+// ConditionalLogisticRegression::incrementGradientAndHessian, ModelSpecifics.h:820-837):
+// the first entry of each run of equal stratum walks the run.
+template <bool IND>
+__global__ void k_gh_grouped(ColView c, const int* __restrict__ group, const double* __restrict__ exb,
+                             const double* __restrict__ denom, const double* __restrict__ nw,
+                             const double* __restrict__ xjy, int j, double2* partial, unsigned* ticket,
+                             double* out) {
+    double g = 0.0, h = 0.0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int key = group[c.row(e)];
+        if (e > 0 && group[c.row(e - 1)] == key) continue;
+        double n1 = 0.0, n2 = 0.0;
+        long long f = e;
+        do {
+            const int k = c.row(f);
+            const double x = c.x(f);
+            n1 += exb[k] * x;
+            if (!IND) n2 += exb[k] * x * x;
+            ++f;
+        } while (f < c.n && group[c.row(f)] == key);
+        const double d = denom[key];
+        const double t = n1 / d;
+        const double gg = nw[key] * t;
+        g += gg;
+        h += IND ? gg * (1.0 - t) : nw[key] * (n2 / d - t * t);
+    }
+    grid_sum2_finalize(g, h, partial, ticket, [&](double G, double H) {
+        out[0] = G - xjy[j];
+        out[1] = H;
+    });
+}
+
+// computeNumeratorForGradient for cox (ModelSpecifics.hpp:1353-1464):
+// numer[g] = sum of w*exb*x over the column's rows in risk-set group g
+template <bool IND>
+__global__ void k_cox_numerator(ColView c, const int* __restrict__ group, const double* __restrict__ exb,
+                                const double* __restrict__ kw, int use_w, double* __restrict__ numer,
+                                double* __restrict__ numer2) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int key = group[c.row(e)];
+        if (e > 0 && group[c.row(e - 1)] == key) continue;
+        double n1 = 0.0, n2 = 0.0;
+        long long f = e;
+        do {
+            const int k = c.row(f);
+            const double x = c.x(f);
+            const double w = use_w ? kw[k] : 1.0;
+            if (w != 0.0) {
+                n1 += w * (exb[k] * x);
+                if (!IND) n2 += w * (exb[k] * x * x);
+            }
+            ++f;
+        } while (f < c.n && group[c.row(f)] == key);
+        numer[key] = n1;
+        if (!IND) numer2[key] = n2;
+    }
+}
+
+// cumulative gradient for Breslow cox (ModelSpecifics.hpp:904-962).
+//
+// The reference walks every risk-set group i from the column's first group
+// to N, with A_i / B_i the stratum-segmented running sums of the column's
+// numerators, adding n_i*A_i/D_i (and the Hessian terms).  Between two
+// consecutive column groups A and B are constant, so the walk over a gap
+// [g_a, e_a) collapses to A*(P1(e_a-1) - P1(g_a-1)) and A^2*(P2(..)-P2(..)),
+// where P1 / P2 are stratum-segmented prefix sums of n/D and n/D^2 kept
+// (in double-double) by the denominator scan.  One block walks the column's
+// group list in tiles, carrying the segmented running sums across tiles.
+template <bool IND>
+__global__ void k_cox_gradient(const int* __restrict__ list, int L, const int* __restrict__ gstart,
+                               const int* __restrict__ gend, const double* __restrict__ numer,
+                               const double* __restrict__ numer2, const double* __restrict__ P1h,
+                               const double* __restrict__ P1l, const double* __restrict__ P2h,
+                               const double* __restrict__ P2l, const double* __restrict__ xjy, int j,
+                               double* out) {
+    __shared__ double sA[kThreads], sB[kThreads];
+    __shared__ int sK[kThreads];
+    __shared__ double carryA, carryB;
+    __shared__ int carryKey;
+    if (threadIdx.x == 0) { carryA = 0.0; carryB = 0.0; carryKey = -1; }
+    double g = 0.0, h = 0.0;
+    for (int base = 0; base < L; base += blockDim.x) {
+        const int a = base + threadIdx.x;
+        int ga = 0, key = -2;
+        double A = 0.0, B = 0.0;
+        if (a < L) {
+            ga = list[a];
+            key = gstart[ga];
+            A = numer[ga];
+            B = IND ? 0.0 : numer2[ga];
+        }
+        __syncthreads();
+        // inclusive segmented scan over the tile (Hillis-Steele, keys equal => same segment)
+        sA[threadIdx.x] = A; sB[threadIdx.x] = B; sK[threadIdx.x] = key;
+        __syncthreads();
+        for (int off = 1; off < blockDim.x; off <<= 1) {
+            double pa = 0.0, pb = 0.0;
+            bool add = false;
+            if (threadIdx.x >= off && sK[threadIdx.x - off] == key) {
+                // contiguous keys: equal key at distance off => the whole span shares it
+                pa = sA[threadIdx.x - off]; pb = sB[threadIdx.x - off]; add = true;
+            }
+            __syncthreads();
+            if (add) { A += pa; B += pb; sA[threadIdx.x] = A; sB[threadIdx.x] = B; }
+            __syncthreads();
+        }
+        if (a < L) {
+            if (key == carryKey) { A += carryA; B += carryB; }
+            // interval end: next column group in the same stratum, else the stratum end
+            int ea;
+            if (a + 1 < L && gstart[list[a + 1]] == key) ea = list[a + 1];
+            else ea = gend[ga];
+            const DD p1e{P1h[ea - 1], P1l[ea - 1]};
+            const DD p2e{P2h[ea - 1], P2l[ea - 1]};
+            const DD p1s = (ga == key) ? DD{0.0, 0.0} : DD{P1h[ga - 1], P1l[ga - 1]};
+            const DD p2s = (ga == key) ? DD{0.0, 0.0} : DD{P2h[ga - 1], P2l[ga - 1]};
+            const DD d1 = dd_sub(p1e, p1s);
+            const DD d2 = dd_sub(p2e, p2s);
+            const double s1 = d1.hi + d1.lo;
+            const double s2 = d2.hi + d2.lo;
+            g += A * s1;
+            h += IND ? (A * s1 - A * A * s2) : (B * s1 - A * A * s2);
+        }
+        __syncthreads();
+        // carry: last valid element of the tile
+        const int last = min((int)blockDim.x, L - base) - 1;
+        if (threadIdx.x == last) {
+            carryA = A; carryB = B; carryKey = key;
+        }
+        __syncthreads();
+    }
+    block_sum2(g, h);
+    if (threadIdx.x == 0) {
+        out[0] = g - xjy[j];
+        out[1] = h;
+    }
+}
+
+// a column whose group list is empty: gradient -XjY, Hessian 0 (ModelSpecifics.hpp:906)
+__global__ void k_copy_neg_xjy(const double* __restrict__ xjy, int j, double* out) {
+    out[0] = 0.0 - xjy[j];
+    out[1] = 0.0;
+}
+
+// ---- updateXBeta (ModelSpecifics.hpp:1524-1586) -----------------------------
+
+// independent rows: each row is its own denominator
+__global__ void k_update_independent(ColView c, const double* delta_ptr, double delta_val,
+                                     double* __restrict__ xb, double* __restrict__ exb,
+                                     double* __restrict__ denom) {
+    const double delta = delta_ptr ? *delta_ptr : delta_val;
+    if (delta == 0.0) return;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int k = c.row(e);
+        const double v = add_mul_rn(xb[k], delta, c.x(e));
+        xb[k] = v;
+        const double old = exb[k];
+        const double nw_ = exp(v);
+        exb[k] = nw_;
+        denom[k] += nw_ - old;
+    }
+}
+
+// grouped / cumulative rows: the first entry of each run updates the run and
+// adds its denominator change (weighted for cox when use_w)
+__global__ void k_update_grouped(ColView c, const double* delta_ptr, double delta_val,
+                                 const int* __restrict__ group, const double* __restrict__ kw,
+                                 int weighted, double* __restrict__ xb, double* __restrict__ exb,
+                                 double* __restrict__ denom) {
+    const double delta = delta_ptr ? *delta_ptr : delta_val;
+    if (delta == 0.0) return;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < c.n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const int key = group[c.row(e)];
+        if (e > 0 && group[c.row(e - 1)] == key) continue;
+        double d = denom[key];
+        long long f = e;
+        do {
+            const int k = c.row(f);
+            const double v = add_mul_rn(xb[k], delta, c.x(f));
+            xb[k] = v;
+            const double w = weighted ? kw[k] : 1.0;
+            const double old = w * exb[k];
+            const double ne = exp(v);
+            exb[k] = ne;
+            if (w != 0.0) d += w * ne - old;
+            ++f;
+        } while (f < c.n && group[c.row(f)] == key);
+        denom[key] = d;
+    }
+}
+
+// ---- cox denominator scan (computeAccumlatedDenominator, ModelSpecifics.hpp:1670-1694)
+//
+// D_i  = stratum-segmented inclusive prefix of denom
+// P1_i = stratum-segmented inclusive prefix of n_i / D_i      (double-double)
+// P2_i = stratum-segmented inclusive prefix of n_i / D_i^2    (double-double)
+// computed over [lo, N) in tiles of kScanTile groups with three phases
+// (tile aggregates, carry scan, rewrite) for D and again for P.
+
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kThreads * kScanItems;
+
+__device__ __forceinline__ SegD seg_combine(SegD l, SegD r) { return r.f ? r : SegD{l.f, l.v + r.v}; }
+__device__ __forceinline__ SegP seg_combine(SegP l, SegP r) {
+    return r.f ? r : SegP{l.f, dd_add(l.a, r.a), dd_add(l.b, r.b)};
+}
+
+// exclusive block scan of per-thread aggregates in thread order; returns the
+// exclusive prefix for this thread and writes the block total to *total
+template <class T>
+__device__ T block_exclusive_scan(T v, T identity, T* total) {
+    __shared__ T buf[kThreads];
+    buf[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < blockDim.x; off <<= 1) {
+        T prev = identity;
+        const bool has = threadIdx.x >= off;
+        if (has) prev = buf[threadIdx.x - off];
+        __syncthreads();
+        if (has) buf[threadIdx.x] = seg_combine(prev, buf[threadIdx.x]);
+        __syncthreads();
+    }
+    T excl = threadIdx.x ? buf[threadIdx.x - 1] : identity;
+    if (total) *total = buf[blockDim.x - 1];
+    __syncthreads();
+    return excl;
+}
+
+// `gate`: when non-null and *gate == 0 (a zero coordinate step), nothing changed
+__global__ void k_scanD_tiles(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+                              const double* __restrict__ denom, SegD* __restrict__ agg) {
+    if (gate && *gate == 0.0) return;
+    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    SegD a{0, 0.0};
+    for (int q = 0; q < kScanItems; ++q) {
+        const int i = t0 + q;
+        if (i < hi) a = seg_combine(a, SegD{gstart[i] == i, denom[i]});
+    }
+    SegD tot;
+    block_exclusive_scan(a, SegD{0, 0.0}, &tot);
+    if (threadIdx.x == 0) agg[blockIdx.x] = tot;
+}
+
+template <class T>
+__device__ void scan_carry(int n, T* agg, T init) {
+    // one block: each thread folds a contiguous run of tiles, then a block scan
+    const int per = (n + blockDim.x - 1) / blockDim.x;
+    const int b = threadIdx.x * per, e = min(n, b + per);
+    T acc{};
+    acc.f = 0;
+    T id = acc;
+    for (int i = b; i < e; ++i) acc = seg_combine(acc, agg[i]);
+    T excl = block_exclusive_scan(acc, id, (T*)nullptr);
+    T run = seg_combine(init, excl);
+    for (int i = b; i < e; ++i) {
+        const T t = agg[i];
+        agg[i] = run;  // exclusive carry into tile i
+        run = seg_combine(run, t);
+    }
+}
+
+__global__ void k_carryD(const double* gate, int n, SegD* agg, int lo, const int* __restrict__ gstart,
+                         const double* __restrict__ D) {
+    if (gate && *gate == 0.0) return;
+    const SegD init{0, (lo > 0 && gstart[lo] != lo) ? D[lo - 1] : 0.0};
+    scan_carry(n, agg, init);
+}
+
+__global__ void k_carryP(const double* gate, int n, SegP* agg, int lo, const int* __restrict__ gstart,
+                         const double* __restrict__ P1h, const double* __restrict__ P1l,
+                         const double* __restrict__ P2h, const double* __restrict__ P2l) {
+    if (gate && *gate == 0.0) return;
+    SegP init{0, {0.0, 0.0}, {0.0, 0.0}};
+    if (lo > 0 && gstart[lo] != lo) {
+        init.a = DD{P1h[lo - 1], P1l[lo - 1]};
+        init.b = DD{P2h[lo - 1], P2l[lo - 1]};
+    }
+    scan_carry(n, agg, init);
+}
+
+__global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+                              const double* __restrict__ denom, const double* __restrict__ nw,
+                              const SegD* __restrict__ carry, double* __restrict__ D, SegP* __restrict__ aggP) {
+    if (gate && *gate == 0.0) return;
+    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    SegD a{0, 0.0};
+    for (int q = 0; q < kScanItems; ++q) {
+        const int i = t0 + q;
+        if (i < hi) a = seg_combine(a, SegD{gstart[i] == i, denom[i]});
+    }
+    SegD tot;
+    SegD ex = block_exclusive_scan(a, SegD{0, 0.0}, &tot);
+    SegD run = seg_combine(carry[blockIdx.x], ex);
+    SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
+    for (int q = 0; q < kScanItems; ++q) {
+        const int i = t0 + q;
+        if (i < hi) {
+            const int f = gstart[i] == i;
+            run = seg_combine(run, SegD{f, denom[i]});
+            D[i] = run.v;
+            const double r1 = nw[i] / run.v;
+            const double r2 = r1 / run.v;
+            p = seg_combine(p, SegP{f, {r1, 0.0}, {r2, 0.0}});
+        }
+    }
+    SegP totp;
+    block_exclusive_scan(p, SegP{0, {0.0, 0.0}, {0.0, 0.0}}, &totp);
+    if (threadIdx.x == 0) aggP[blockIdx.x] = totp;
+}
+
+__global__ void k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+                              const double* __restrict__ D, const double* __restrict__ nw,
+                              const SegP* __restrict__ carry, double* __restrict__ P1h, double* __restrict__ P1l,
+                              double* __restrict__ P2h, double* __restrict__ P2l) {
+    if (gate && *gate == 0.0) return;
+    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
+    for (int q = 0; q < kScanItems; ++q) {
+        const int i = t0 + q;
+        if (i < hi) {
+            const double r1 = nw[i] / D[i];
+            p = seg_combine(p, SegP{gstart[i] == i, {r1, 0.0}, {r1 / D[i], 0.0}});
+        }
+    }
+    SegP tot;
+    SegP ex = block_exclusive_scan(p, SegP{0, {0.0, 0.0}, {0.0, 0.0}}, &tot);
+    SegP run = seg_combine(carry[blockIdx.x], ex);
+    for (int q = 0; q < kScanItems; ++q) {
+        const int i = t0 + q;
+        if (i < hi) {
+            const double r1 = nw[i] / D[i];
+            run = seg_combine(run, SegP{gstart[i] == i, {r1, 0.0}, {r1 / D[i], 0.0}});
+            P1h[i] = run.a.hi; P1l[i] = run.a.lo;
+            P2h[i] = run.b.hi; P2l[i] = run.b.lo;
+        }
+    }
+}
+
+// ---- log likelihood (ModelSpecifics.hpp:605-650) -----------------------------
+
+__device__ __forceinline__ double ll_numer(int model, double y, double xb) {
+    const int yi = (int)y;                      // logLikeNumeratorContrib(int, RealType)
+    if (model == CYC_COX) return yi != 1 ? 0.0 : xb;
+    return yi * xb;
+}
+__device__ __forceinline__ double ll_denom(int model, double n, double d) {
+    return model == CYC_PR ? n * d : n * log(d);
+}
+
+__global__ void k_loglik(int model, int K, int N, const double* __restrict__ y, const double* __restrict__ xb,
+                         const double* __restrict__ kw, int use_cv, const double* __restrict__ nw,
+                         const double* __restrict__ den, const double* __restrict__ fixed,
+                         double2* partial, unsigned* ticket, double* out) {
+    double a = 0.0, b = 0.0;
+    const int M = K > N ? K : N;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M; i += gridDim.x * blockDim.x) {
+        if (i < K) {
+            const double v = ll_numer(model, y[i], xb[i]);
+            a += use_cv ? v * kw[i] : v;
+        }
+        if (i < N) b += ll_denom(model, nw[i], den[i]);
+    }
+    grid_sum2_finalize(a, b, partial, ticket, [&](double A, double B) {
+        double ll = A - B;
+        if (has_fixed_ll(model)) ll += *fixed;
+        *out = ll;
+    });
+}
+
+// getGradientObjective (ModelSpecifics.hpp:103-120)
+__global__ void k_grad_objective(int K, const double* __restrict__ y, const double* __restrict__ xb,
+                                 const double* __restrict__ kw, int use_cv, double2* partial,
+                                 unsigned* ticket, double* out) {
+    double a = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        a += use_cv ? xb[k] * y[k] * kw[k] : xb[k] * y[k];
+    grid_sum2_finalize(a, 0.0, partial, ticket, [&](double A, double) { *out = A; });
+}
+
+// getPredictiveLogLikelihood (ModelSpecifics.hpp:652-690 and logPredLikeContrib,
+// ModelSpecifics.h:1002-1009, 1137-1146, 1583-1590)
+__global__ void k_pred_loglik(int model, int K, const double* __restrict__ y, const double* __restrict__ xb,
+                              const double* __restrict__ w, const int* __restrict__ group,
+                              const double* __restrict__ den, double2* partial, unsigned* ticket,
+                              double* out) {
+    double a = 0.0;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const double yk = y[k], wk = w[k], x = xb[k];
+        double v;
+        if (model == CYC_PR) {
+            v = (yk * x - exp(x)) * wk;
+        } else {
+            const int g = group ? group[k] : k;
+            if (model == CYC_COX) v = wk == 0.0 ? 0.0 : yk * wk * (x - log(den[g]));
+            else v = yk * wk * (x - log(den[g]));
+        }
+        a += v;
+    }
+    grid_sum2_finalize(a, 0.0, partial, ticket, [&](double A, double) { *out = A; });
+}
+
+// getPredictiveEstimates (ModelSpecifics.hpp:692-707, predictEstimate)
+__global__ void k_pred_estimates(int model, int K, const double* __restrict__ xb, const double* __restrict__ w,
+                                 double* __restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        if (w && w[k] == 0.0) continue;
+        const double x = xb[k];
+        if (model == CYC_LR) {
+            const double t = exp(x);
+            out[k] = t / (t + 1.0);
+        } else if (model == CYC_PR) {
+            out[k] = exp(x);
+        } else {
+            out[k] = x;
+        }
+    }
+}
+
+}  // namespace cyc

@@ -1,0 +1,227 @@
+/*
+ * cyclops_b200.h -- C ABI of libcyclops_b200.so, the sm_100a engine for the
+ * Cyclops cyclic-coordinate-descent (CCD) inner loop.
+ *
+ * Three layers, all plain C (no C++ or torch types cross this boundary):
+ *
+ *  1. Datasets: a device-resident copy of the reference's CompressedDataMatrix
+ *     plus y / time / stratum vectors (reference: src/cyclops/ModelData.h:178-362,
+ *     src/cyclops/CompressedDataMatrix.h:243-452).
+ *
+ *  2. Engines: one fit's per-coordinate engine, a function-for-function
+ *     replacement of the virtual surface of
+ *     `bsccs::AbstractModelSpecifics` (src/cyclops/engine/AbstractModelSpecifics.h:36-122).
+ *     Each cyc_engine_* call below names the virtual it replaces.  Values
+ *     cross as FP64; state stays on the GPU between calls.  This is what
+ *     `CyclicCoordinateDescent` drives through the C++ adapter
+ *     cyclops_b200/adapter/CudaModelSpecifics.h.
+ *
+ *  3. Solvers: the whole CCD loop (coordinate step, bounds, convergence test)
+ *     kept on the GPU, for one fit or for many fits that share one dataset
+ *     (cross-validation folds x prior grid, bootstrap replicates).  The
+ *     reference runs this loop on the host in
+ *     CyclicCoordinateDescent::update/findMode (src/cyclops/CyclicCoordinateDescent.cpp:586-1216)
+ *     and runs independent fits on CPU threads
+ *     (src/cyclops/drivers/AbstractCrossValidationDriver.cpp:131-248).
+ *
+ * Every function returns 0 on success and a nonzero cyc_status otherwise;
+ * cyc_last_error() then describes the failure (thread-local).  Nothing
+ * throws across this boundary.
+ */
+#ifndef CYCLOPS_B200_H
+#define CYCLOPS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums (values match the reference's enums) ------------------------ */
+
+/* FormatType, src/cyclops/CompressedDataMatrix.h:36-38 */
+enum cyc_format { CYC_DENSE = 0, CYC_SPARSE = 1, CYC_INDICATOR = 2, CYC_INTERCEPT = 3 };
+
+/* the model types on this path (ModelType, src/cyclops/Types.h:134-147) */
+enum cyc_model { CYC_LR = 0, CYC_PR = 1, CYC_CLR = 2, CYC_CPR = 3, CYC_COX = 4 };
+
+/* PriorType, src/cyclops/Types.h:101-106 */
+enum cyc_prior_type { CYC_PRIOR_NONE = 0, CYC_PRIOR_LAPLACE = 1, CYC_PRIOR_NORMAL = 2 };
+
+/* ConvergenceType, src/cyclops/Types.h:110-116 */
+enum cyc_convergence {
+    CYC_CONV_GRADIENT = 0, CYC_CONV_LANGE = 1, CYC_CONV_MITTAL = 2,
+    CYC_CONV_ONE_STEP = 3, CYC_CONV_ZHANG_OLES = 4
+};
+
+/* UpdateReturnFlags, src/cyclops/Types.h:124-130 */
+enum cyc_return_flag {
+    CYC_SUCCESS = 0, CYC_FAIL = 1, CYC_MAX_ITERATIONS = 2, CYC_ILLCONDITIONED = 3
+};
+
+enum cyc_status {
+    CYC_OK = 0,
+    CYC_ERR_ARGUMENT = 1,     /* bad pointer, size or enum */
+    CYC_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+    CYC_ERR_MEMORY = 3,       /* device allocation failed or over budget */
+    CYC_ERR_UNSUPPORTED = 4,  /* path not offered for this model / format */
+    CYC_ERR_STATE = 5,        /* call out of order (e.g. gradient before statistics) */
+    CYC_ERR_TIMEOUT = 6       /* a device-side wait ran past its bound */
+};
+
+/* arithmetic of the device-resident solvers */
+enum cyc_precision {
+    CYC_FP64 = 0,             /* FP64 state and sums throughout */
+    CYC_MIXED = 1             /* FP32 state + compensated sums, then an FP64 polish */
+};
+
+/* ---- data --------------------------------------------------------------- */
+
+/* Column store in the reference's ingest order (src/RcppModelData.cpp:751-900):
+ * an optional fixed offset column 0, dense columns (intercept first), sparse,
+ * indicator.  Rows of survival models sorted by (stratum, -time, y); rows of
+ * stratified models by stratum. */
+typedef struct {
+    int model;                  /* cyc_model */
+    int K;                      /* rows */
+    int J;                      /* columns */
+    const int* pid;             /* K stratum ids (renumbered by runs) or NULL */
+    const double* y;            /* K outcomes */
+    const double* time;         /* K survival times (cox) or offsets, or NULL */
+    const int* col_format;      /* J cyc_format */
+    const long long* col_ptr;   /* J+1 offsets into col_idx (SPARSE/INDICATOR) */
+    const int* col_idx;         /* ascending row ids per column */
+    const long long* val_ptr;   /* J+1 offsets into col_val (SPARSE: nnz, DENSE: K) */
+    const double* col_val;      /* values */
+    int has_offset;             /* column 0 is an offset with beta fixed at 1 */
+    int has_intercept;
+} cyc_data_desc;
+
+typedef struct cyc_dataset cyc_dataset;
+typedef struct cyc_engine cyc_engine;
+
+const char* cyc_last_error(void);
+int cyc_version(void);
+
+/* Copy a dataset to device `device`.  Replaces the host-side ModelData the
+ * engine reads by const reference (src/cyclops/engine/ModelSpecifics.h:121-122). */
+int cyc_dataset_create(const cyc_data_desc* desc, int device, cyc_dataset** out);
+int cyc_dataset_destroy(cyc_dataset* ds);
+/* rows, columns, stored indices, device bytes held */
+int cyc_dataset_info(const cyc_dataset* ds, int* K, int* J, long long* nnz, size_t* device_bytes);
+
+/* ---- engine: the AbstractModelSpecifics surface ------------------------- */
+
+/* AbstractModelSpecifics::factory + initialize(N,K,J,...)
+ * (AbstractModelSpecifics.cpp:128-154, ModelSpecifics.hpp:1899-1952) */
+int cyc_engine_create(cyc_dataset* ds, cyc_engine** out);
+int cyc_engine_destroy(cyc_engine* e);
+/* clone() (ModelSpecifics.hpp:98-101): shares the dataset, own state + stream */
+int cyc_engine_clone(const cyc_engine* e, cyc_engine** out);
+/* setWeights(double*, double*, bool) (ModelSpecifics.hpp:427-484) */
+int cyc_engine_set_weights(cyc_engine* e, const double* weights, int use_cv);
+/* computeFixedTermsInLogLikelihood (ModelSpecifics.hpp:570-587) */
+int cyc_engine_compute_fixed_terms_ll(cyc_engine* e, int use_cv);
+/* computeFixedTermsInGradientAndHessian (ModelSpecifics.hpp:589-603) */
+int cyc_engine_compute_fixed_terms_gh(cyc_engine* e, int use_cv);
+/* zeroXBeta / axpyXBeta / computeXBeta (ModelSpecifics.hpp:296-423) */
+int cyc_engine_zero_xbeta(cyc_engine* e);
+int cyc_engine_axpy_xbeta(cyc_engine* e, double beta, int j);
+int cyc_engine_compute_xbeta(cyc_engine* e, const double* beta, int use_w);
+/* computeRemainingStatistics (ModelSpecifics.hpp:1588-1633) */
+int cyc_engine_compute_remaining_statistics(cyc_engine* e, int use_w);
+/* computeNumeratorForGradient (ModelSpecifics.hpp:1353-1427) */
+int cyc_engine_compute_numerator_for_gradient(cyc_engine* e, int j, int use_w);
+/* computeGradientAndHessian (ModelSpecifics.hpp:711-766, 891-1201) */
+int cyc_engine_compute_gradient_and_hessian(cyc_engine* e, int j, double* gradient,
+                                            double* hessian, int use_w);
+/* updateXBeta (ModelSpecifics.hpp:1466-1586) */
+int cyc_engine_update_xbeta(cyc_engine* e, double delta, int j, int use_w);
+/* getLogLikelihood (ModelSpecifics.hpp:605-650) */
+int cyc_engine_get_log_likelihood(cyc_engine* e, int use_cv, double* out);
+/* getGradientObjective (ModelSpecifics.hpp:103-120) */
+int cyc_engine_get_gradient_objective(cyc_engine* e, int use_cv, double* out);
+/* getPredictiveLogLikelihood (ModelSpecifics.hpp:652-690) */
+int cyc_engine_get_predictive_log_likelihood(cyc_engine* e, const double* weights, double* out);
+/* getPredictiveEstimates (ModelSpecifics.hpp:692-707) */
+int cyc_engine_get_predictive_estimates(cyc_engine* e, double* y, const double* weights);
+/* getXBeta / saveXBeta / getXBetaSave (ModelSpecifics.hpp:286-308); K doubles */
+int cyc_engine_get_xbeta(cyc_engine* e, double* out);
+int cyc_engine_save_xbeta(cyc_engine* e);
+int cyc_engine_get_xbeta_save(cyc_engine* e, double* out);
+/* number of denominators N (patients / strata / risk-set groups) */
+int cyc_engine_get_n(const cyc_engine* e, int* n);
+
+/* ---- device-resident solvers -------------------------------------------- */
+
+/* ModeFindingArguments (src/cyclops/CcdInterface.h:70-94) */
+typedef struct {
+    double tolerance;           /* default 1e-6 */
+    int max_iterations;         /* default 1000 */
+    int convergence_type;       /* cyc_convergence, default GRADIENT */
+    double initial_bound;       /* default 2.0 */
+    int max_bound_count;        /* default 5 */
+    int precision;              /* cyc_precision */
+    double polish_tolerance;    /* CYC_MIXED: FP32 phase stops at this tolerance */
+} cyc_control;
+
+/* the prior: one default prior for every column, a flat prior on `exclude`
+ * (MixtureJointPrior, src/cyclops/priors/JointPrior.h:81-160) */
+typedef struct {
+    int prior_type;             /* cyc_prior_type */
+    const int* exclude;         /* column ids with a flat prior (the intercept) */
+    int n_exclude;
+} cyc_prior;
+
+/* one fit of a batch: its row weights (0/1 CV mask or any nonnegative weights,
+ * NULL = unweighted), its prior variance and optional warm start */
+typedef struct {
+    const double* weights;      /* K, or NULL */
+    double variance;            /* prior variance (Laplace lambda = sqrt(2/variance)) */
+    const double* start_beta;   /* J, or NULL (zeros; offset column 1) */
+} cyc_fit_spec;
+
+typedef struct {
+    double* beta;               /* J, caller-owned output */
+    double log_likelihood;
+    double log_prior;
+    int iterations;             /* cycles of the final bound */
+    int return_flag;            /* cyc_return_flag */
+} cyc_fit_result;
+
+/* One fit with the CCD loop on the GPU, whole-GPU kernels per coordinate and
+ * no host round trip inside a cycle (CyclicCoordinateDescent::update,
+ * src/cyclops/CyclicCoordinateDescent.cpp:586-615). */
+int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+            const cyc_control* control, cyc_fit_result* out);
+
+/* F fits sharing `ds`, advanced together coordinate by coordinate in one
+ * persistent kernel (lr, pr, clr, cpr).  Results in `out[0..F)`. */
+int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
+                  const cyc_control* control, cyc_fit_result* out);
+
+/* Cross-validation fold masks, `n_reps * folds` rows of K weights (0 = held
+ * out), exactly as CrossValidationSelector draws them
+ * (src/cyclops/drivers/CrossValidationSelector.cpp:21-116): by row
+ * (`by_row` = 1) or by stratum id `ids` (0..S-1); seed -1 = no shuffle. */
+int cyc_cv_fold_weights(int K, const int* ids, int folds, long seed, int by_row, int n_reps,
+                        double* out);
+
+/* Statistics of the last cyc_batch_fit / cyc_fit on this thread, for
+ * roofline accounting: kernel milliseconds (CUDA events), column entries
+ * visited by gradients, entries visited by updates, coordinate steps. */
+typedef struct {
+    double kernel_ms;
+    double gradient_entries;    /* sum over (fit, coordinate) of nnz_j */
+    double update_entries;      /* sum over (fit, coordinate) with delta != 0 of nnz_j */
+    double coordinate_steps;
+    double index_entries;       /* column entries read once per coordinate (shared by fits) */
+    int launches;
+    int state_bytes;            /* bytes per (row, fit) state element */
+} cyc_run_stats;
+int cyc_last_run_stats(cyc_run_stats* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CYCLOPS_B200_H */

@@ -113,6 +113,20 @@ class _Lib:
         le = getattr(self.lib, prefix + "last_error")
         le.restype = C.c_char_p
         self._last_error = le
+        P, V = C.POINTER, C.c_void_p
+        sigs = {
+            "fit": [P(Problem), P(Control), V, P(Result)],
+            "engine_probe" if prefix == "ref_" else "probe": [P(Problem), V, V, V, V, P(C.c_double)],
+            "predictive_loglik": [P(Problem), V, V, P(C.c_double)],
+        }
+        if prefix == "ref_":
+            sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
+            sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
+        for name, args in sigs.items():
+            fn = getattr(self.lib, prefix + name, None)
+            if fn is not None:
+                fn.argtypes = args
+                fn.restype = C.c_int
 
     def err(self) -> str:
         return self._last_error().decode()
@@ -175,12 +189,34 @@ def have_ref() -> bool:
     return os.path.exists(os.path.join(REF_DIR, "libcyclops_ref.so"))
 
 
+_CV_SCRIPT = r"""
+import ctypes as C, sys, struct
+L = C.CDLL(sys.argv[1])
+f = L.ref_cv_weights
+f.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_int, C.c_int, C.c_void_p]
+K, fold, seed, by_row, reps = map(int, sys.argv[2:7])
+raw = sys.stdin.buffer.read()
+ids = (C.c_int * K).from_buffer_copy(raw)
+out = (C.c_double * (K * fold * reps))()
+rc = f(K, C.addressof(ids), fold, seed, by_row, reps, C.addressof(out))
+if rc:
+    sys.exit(3)
+sys.stdout.buffer.write(bytes(out))
+"""
+
+
 def ref_cv_weights(K, ids, fold, seed, by_row=True, n_reps=1) -> np.ndarray:
-    lib = ref().lib
+    """Fold masks from the reference's CrossValidationSelector.
+
+    Runs in a child interpreter that loads the reference library before
+    numpy: the selector's logging path crashes when numpy's C++ runtime
+    was loaded first into the same process."""
+    path = os.path.join(REF_DIR, "libcyclops_ref.so")
+    if not os.path.exists(path):
+        build()
     ids = np.ascontiguousarray(ids, np.int32)
-    out = np.zeros((n_reps * fold, K))
-    rc = lib.ref_cv_weights(C.c_int(K), _ptr(ids), C.c_int(fold), C.c_long(seed),
-                            C.c_int(int(by_row)), C.c_int(n_reps), _ptr(out))
-    if rc:
-        raise RuntimeError(ref().err())
-    return out
+    import sys
+    p = subprocess.run([sys.executable, "-c", _CV_SCRIPT, path, str(K), str(fold), str(seed),
+                        str(int(by_row)), str(n_reps)], input=ids.tobytes(), capture_output=True,
+                       check=True)
+    return np.frombuffer(p.stdout, dtype=np.float64).reshape(n_reps * fold, K).copy()

@@ -1,0 +1,130 @@
+"""Generates tests/golden/*.npz from the reference Cyclops engine.
+
+Each fixture holds a small seeded problem (the arrays themselves, so the
+fixture does not depend on the generator) and what the reference engine,
+compiled from its own sources (oracle/_ref/libcyclops_ref.so), returns for
+it: the fitted coefficients, log likelihood, log prior, iteration count and
+return flag of CyclicCoordinateDescent::update, the per-column
+(gradient, Hessian) of the engine at a fixed coefficient vector, and the
+linear predictor there.  The CV fold masks come from the reference's
+CrossValidationSelector.
+
+    python tests/golden/make_golden.py      # needs the reference sources
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from cyclops_b200 import data as D  # noqa: E402
+from oracle import oracle as O      # noqa: E402
+
+
+def cases():
+    lam01 = D.laplace_variance(0.1)
+    c = {}
+    # the reference's CPU-runnable configuration: 10k x 1k indicators at 1 %,
+    # Laplace lambda = 0.1 (variance 200), default control
+    c["lr_c1"] = dict(data=D.synth_logistic(seed=1), prior=D.PRIOR_LAPLACE, variance=lam01)
+    c["lr_laplace_small"] = dict(data=D.synth_logistic(K=3000, P=200, density=0.02, n_true=20, seed=21),
+                                 prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(1.0))
+    rng = np.random.default_rng(5)
+    d = D.synth_logistic(K=3000, P=150, density=0.02, n_true=20, seed=22)
+    c["lr_normal_weighted"] = dict(data=d, prior=D.PRIOR_NORMAL, variance=0.5,
+                                   weights=(rng.random(d.K) > 0.25).astype(float))
+    c["lr_lange"] = dict(data=D.synth_logistic(K=2000, P=80, density=0.03, n_true=10, seed=23),
+                         prior=D.PRIOR_NORMAL, variance=2.0, convergence=D.CONV_LANGE, tolerance=1e-8)
+    c["lr_zhang_oles"] = dict(data=D.synth_logistic(K=2000, P=80, density=0.03, n_true=10, seed=24),
+                              prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(2.0),
+                              convergence=D.CONV_ZHANG_OLES, tolerance=1e-7)
+    c["lr_flat"] = dict(data=D.synth_logistic(K=4000, P=12, density=0.2, n_true=6, seed=25),
+                        prior=D.PRIOR_NONE, variance=1.0, convergence=D.CONV_MITTAL, tolerance=1e-10)
+    c["pr_offset_normal"] = dict(data=D.synth_poisson(K=4000, P=200, per_row=6, n_dense=3, n_true=25, seed=31),
+                                 prior=D.PRIOR_NORMAL, variance=1.0)
+    d = D.synth_poisson(K=3000, P=120, per_row=5, n_dense=2, n_true=15, seed=32, offset=False)
+    c["pr_laplace_weighted"] = dict(data=d, prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(0.5),
+                                    weights=(rng.random(d.K) > 0.3).astype(float))
+    c["clr_laplace"] = dict(data=D.synth_conditional(K=4000, P=150, density=0.02, seed=41),
+                            prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(1.0))
+    d = D.synth_conditional(K=3000, P=100, density=0.03, seed=42)
+    c["clr_normal_weighted"] = dict(data=d, prior=D.PRIOR_NORMAL, variance=1.0,
+                                    weights=np.repeat((rng.random(d.K // 5) > 0.2).astype(float), 5))
+    c["cpr_normal"] = dict(data=D.synth_conditional(K=3000, P=100, density=0.03, seed=43, model=D.CPR),
+                           prior=D.PRIOR_NORMAL, variance=1.0)
+    c["cox_laplace"] = dict(data=D.synth_cox(K=3000, P=120, density=0.02, n_true=30, seed=51),
+                            prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(2.0))
+    c["cox_strata"] = dict(data=D.synth_cox(K=3000, P=120, density=0.02, n_strata=25, n_true=30, seed=52),
+                           prior=D.PRIOR_LAPLACE, variance=D.laplace_variance(2.0))
+    d = D.synth_cox(K=3000, P=100, density=0.02, n_strata=4, n_true=30, seed=53, ties=1)
+    c["cox_ties_weighted"] = dict(data=d, prior=D.PRIOR_NORMAL, variance=1.0,
+                                  weights=(rng.random(d.K) > 0.2).astype(float))
+    c["cox_indicator"] = dict(data=D.synth_cox(K=3000, P=100, density=0.03, n_true=30, seed=54, indicator=True),
+                              prior=D.PRIOR_NORMAL, variance=1.0)
+    # edge: an empty indicator column and a dense column under Laplace
+    d = D.synth_logistic(K=1500, P=40, density=0.05, n_true=5, seed=61)
+    b = D.ColumnBuilder(d.K).intercept()
+    b.dense(np.random.default_rng(7).normal(size=d.K))
+    for j in range(1, d.J):
+        rows, _ = d.column(j)
+        b.indicator(rows if j != 5 else [])
+    c["lr_empty_column"] = dict(data=b.build(D.LR, d.y, has_intercept=True), prior=D.PRIOR_LAPLACE,
+                                variance=D.laplace_variance(0.5))
+    return c
+
+
+def save_case(name, spec):
+    d: D.CyclopsData = spec["data"]
+    ctl = O.make_control(tolerance=spec.get("tolerance", 1e-6),
+                         convergence_type=spec.get("convergence", D.CONV_GRADIENT))
+    w = spec.get("weights")
+    fit = O.ref().fit(d, spec["prior"], spec["variance"], control=ctl, weights=w)
+    rng = np.random.default_rng(99)
+    beta_probe = fit.beta + np.where(fit.beta != 0, 0.05 * rng.normal(size=d.J), 0.0)
+    if d.has_offset:
+        beta_probe[0] = 1.0
+    g, h, xb, ll = O.ref().probe(d, beta_probe, spec["prior"], spec["variance"], weights=w)
+    arrays = dict(
+        model=d.model, y=d.y, col_format=d.col_format, col_ptr=d.col_ptr, col_idx=d.col_idx,
+        val_ptr=d.val_ptr, col_val=d.col_val,
+        pid=d.pid if d.pid is not None else np.zeros(0, np.int32),
+        time=d.time if d.time is not None else np.zeros(0),
+        has_offset=int(d.has_offset), has_intercept=int(d.has_intercept),
+        prior=spec["prior"], variance=spec["variance"],
+        weights=w if w is not None else np.zeros(0),
+        tolerance=ctl.tolerance, convergence=ctl.convergence_type,
+        beta=fit.beta, log_likelihood=fit.log_likelihood, log_prior=fit.log_prior,
+        iterations=fit.iterations, return_flag=fit.return_flag,
+        probe_beta=beta_probe, probe_gradient=g, probe_hessian=h, probe_xbeta=xb, probe_loglik=ll,
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+    print(f"{name:22s} K={d.K:6d} J={d.J:5d} nnz={d.nnz:7d} it={fit.iterations:4d} "
+          f"flag={fit.return_flag} ll={fit.log_likelihood:.8f}")
+
+
+def save_cv():
+    K = 1003
+    ids = np.arange(K, dtype=np.int32)
+    by_row = O.ref_cv_weights(K, ids, 10, 123, by_row=True, n_reps=2)
+    pid = np.repeat(np.arange(201, dtype=np.int32), 5)[:K]
+    by_pid = O.ref_cv_weights(K, pid, 5, 77, by_row=False, n_reps=1)
+    np.savez_compressed(os.path.join(HERE, "cv_folds.npz"), K=K, by_row=by_row, pid=pid, by_pid=by_pid,
+                        seed_row=123, seed_pid=77)
+    print("cv_folds", by_row.shape, by_pid.shape)
+
+
+def main():
+    if not O.have_ref():
+        O.build()
+    for name, spec in cases().items():
+        save_case(name, spec)
+    save_cv()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,48 @@
+"""The C-ABI library builds, loads and exports every symbol the header
+declares.  Loads the library but makes no compute call (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+
+def declared_symbols():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(cyc_\w+)\s*\(", txt, flags=re.M))
+    return names
+
+
+def test_header_declares_the_engine_surface():
+    names = declared_symbols()
+    for must in ("cyc_engine_compute_gradient_and_hessian", "cyc_engine_update_xbeta",
+                 "cyc_engine_compute_remaining_statistics", "cyc_engine_get_log_likelihood",
+                 "cyc_fit", "cyc_batch_fit", "cyc_dataset_create"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol(cuda_lib):
+    lib = ctypes.CDLL(os.path.join(ROOT, "cyclops_b200", "_lib", "libcyclops_b200.so"))
+    missing = [n for n in sorted(declared_symbols()) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_bindings_cover_the_header():
+    from cyclops_b200 import _native
+    assert declared_symbols() <= set(_native.exported_symbols())
+
+
+def test_errors_are_status_codes_not_exceptions(cuda_lib):
+    """Argument checks happen before any device work."""
+    from cyclops_b200 import _native as N
+    h = ctypes.c_void_p()
+    rc = cuda_lib.cyc_dataset_create(None, 0, ctypes.byref(h))
+    assert rc == 1
+    assert b"null" in cuda_lib.cyc_last_error()
+    assert cuda_lib.cyc_engine_set_weights(None, None, 0) == 1

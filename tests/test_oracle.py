@@ -1,0 +1,56 @@
+"""The CPU oracles, pinned against the golden fixtures made by the reference
+engine (tests/golden/make_golden.py).  No GPU."""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, rel_err
+from cyclops_b200 import data as D
+from oracle import oracle as O
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_port_matches_reference_fixture(name):
+    data, s = load_golden(name)
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]))
+    fit = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
+    assert fit.iterations == int(s["iterations"])
+    assert fit.return_flag == int(s["return_flag"])
+    np.testing.assert_allclose(fit.beta, s["beta"], rtol=1e-12, atol=1e-14)
+    assert abs(fit.log_likelihood - float(s["log_likelihood"])) <= 1e-12 * abs(float(s["log_likelihood"]))
+    assert abs(fit.log_prior - float(s["log_prior"])) <= 1e-12 * max(1.0, abs(float(s["log_prior"])))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_port_engine_probe_matches_reference_fixture(name):
+    data, s = load_golden(name)
+    g, h, xb, ll = O.port().probe(data, s["probe_beta"], int(s["prior"]), float(s["variance"]),
+                                  weights=s["weights"])
+    np.testing.assert_allclose(g, s["probe_gradient"], rtol=1e-12, atol=1e-10)
+    np.testing.assert_allclose(h, s["probe_hessian"], rtol=1e-12, atol=1e-10)
+    np.testing.assert_allclose(xb, s["probe_xbeta"], rtol=1e-13, atol=1e-14)
+    assert rel_err(ll, float(s["probe_loglik"])) < 1e-12
+
+
+def test_reference_and_port_agree_on_fresh_problem():
+    if not O.have_ref():
+        pytest.skip("reference engine not built here")
+    d = D.synth_cox(K=1500, P=60, density=0.03, n_strata=3, seed=1234, ties=1)
+    a = O.ref().fit(d, D.PRIOR_LAPLACE, 2.0)
+    b = O.port().fit(d, D.PRIOR_LAPLACE, 2.0)
+    assert a.iterations == b.iterations
+    np.testing.assert_array_equal(a.beta, b.beta)
+
+
+def test_oracle_rejects_bad_model():
+    d = D.synth_logistic(K=200, P=5, density=0.1, seed=3)
+    d.model = 9
+    with pytest.raises(RuntimeError):
+        O.port().fit(d, D.PRIOR_NONE, 1.0)
+
+
+def test_planted_mistake_is_caught():
+    """A wrong Laplace rate in the oracle run changes the fit beyond the
+    parity tolerance, so the comparison is sensitive."""
+    data, s = load_golden("lr_laplace_small")
+    bad = O.port().fit(data, int(s["prior"]), float(s["variance"]) * 1.01)
+    assert np.max(rel_err(bad.beta[bad.beta != 0], s["beta"][bad.beta != 0], 1e-6)) > 1e-4
