@@ -1,9 +1,812 @@
-// batch.cu -- cyc_batch_fit (filled in by the batched persistent solver)
-#include "internal.cuh"
+// batch.cu -- cyc_batch_fit: many fits sharing one dataset, advanced
+// coordinate by coordinate in one persistent kernel (lr, pr, clr, cpr).
+//
+// The reference runs such fits (CV folds x prior grid, bootstrap replicates)
+// as independent CyclicCoordinateDescent clones on CPU threads
+// (src/cyclops/drivers/AbstractCrossValidationDriver.cpp:131-248); each clone
+// runs the serial coordinate loop of findMode
+// (src/cyclops/CyclicCoordinateDescent.cpp:1008-1021).
+//
+// Layout and schedule (B200):
+//  * fits are packed G to a group; a group is one thread-block cluster of C
+//    CTAs; the cluster's CTAs split the rows into C contiguous ranges
+//    (aligned to strata for clr/cpr), so the per-row state a CTA touches is
+//    its own and only the per-fit (gradient, Hessian) partials cross CTAs,
+//    through distributed shared memory, once per coordinate;
+//  * per-(row, fit) state is the linear predictor only, stored
+//    xb[group][row][G] so the G fits of one row share one 32-byte sector
+//    (FP32) -- exp(xb) is recomputed where needed instead of stored;
+//  * every CTA of a cluster computes the coordinate step for all G fits from
+//    the same partials in the same order, so all CTAs agree on delta without
+//    a second barrier; rank 0 alone writes beta and the trust region;
+//  * the convergence test (performCheckConvergence, :839-906) runs in the
+//    kernel after every cycle; a fit that has converged stops stepping, and
+//    the cluster exits when all its fits are done.
+#include <cooperative_groups.h>
 
-extern "C" int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
-                             const cyc_control* control, cyc_fit_result* out) {
-    (void)ds; (void)prior; (void)specs; (void)F; (void)control; (void)out;
-    cyc::set_error("cyc_batch_fit: not built yet");
-    return CYC_ERR_UNSUPPORTED;
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <vector>
+
+#include "engine.cuh"
+#include "solver_common.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace cyc {
+
+namespace {
+
+constexpr int kBT = 256;          // threads per CTA
+constexpr int kMaxC = 8;          // CTAs per cluster (portable limit)
+
+struct BatchArgs {
+    int model, K, J, S, C;
+    const int* fmt;
+    const long long* col_ptr;
+    const long long* val_ptr;
+    const int* idx;
+    const double* val;
+    const int* split;             // J x (C+1): first entry of rank r's rows, relative to the column
+    const int* rpart;             // C+1 row boundaries
+    const double* y;
+    const int* strat;             // K (grouped)
+    const int* strat_ptr;         // S+1 (grouped)
+    const int* fixb;              // J
+    const int* ptype;             // J
+    void* xb;                     // [groups][K][G] T
+    const void* w;                // [groups][K][G] T
+    double* denom;                // grouped: [groups][S][G]
+    const double* nw;             // grouped: [groups][S][G]
+    const double* xjy;            // [F][J]
+    double* beta;                 // [F][J]
+    double* hdelta;               // [F][J]
+    const double* variance;       // [F]
+    const double* llfixed;        // [F]
+    const int* active;            // [F] 0 for padding fits
+    int conv;
+    double tol;
+    int max_iter;
+    int* out_iter;                // [F]
+    int* out_flag;                // [F]
+    double* out_obj;              // [F]
+    unsigned long long* counters; // [4] grad fit-entries, update fit-entries, steps, index entries
+};
+
+template <class T>
+struct Kahan {
+    T s = 0, c = 0;
+    __device__ __forceinline__ void add(T v) {
+        const T yv = v - c;
+        const T t = s + yv;
+        c = (t - s) - yv;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+template <>
+struct Kahan<double> {
+    double s = 0;
+    __device__ __forceinline__ void add(double v) { s += v; }
+    __device__ __forceinline__ double value() const { return s; }
+};
+
+__device__ __forceinline__ float fexp(float x) { return __expf(x); }
+__device__ __forceinline__ double fexp(double x) { return exp(x); }
+__device__ __forceinline__ float flog(float x) { return __logf(x); }
+__device__ __forceinline__ double flog(double x) { return log(x); }
+
+// sum (a, b) over the CTA's slots that share this thread's fit lane; result
+// for lane f lands in out[f] (threads < G then read it)
+template <int G>
+__device__ __forceinline__ void block_reduce_lanes(double a, double b, double2* out, double2 (*scratch)[G]) {
+    for (int o = G; o < 32; o <<= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane < G) scratch[wid][lane] = make_double2(a, b);
+    __syncthreads();
+    if (threadIdx.x < G) {
+        double sa = 0.0, sb = 0.0;
+        for (int q = 0; q < kBT / 32; ++q) {
+            sa += scratch[q][threadIdx.x].x;
+            sb += scratch[q][threadIdx.x].y;
+        }
+        out[threadIdx.x] = make_double2(sa, sb);
+    }
+    __syncthreads();
+}
+
+template <class T, int MODEL, int G>
+__device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp, int r0, int r1, int s0, int s1,
+                                                    const T* xbg, const T* wg, int fl, bool use_ll) {
+    Kahan<double> acc;
+    const int slot = threadIdx.x / G, nslots = kBT / G;
+    for (int k = r0 + slot; k < r1; k += nslots) {
+        const double v = (double)xbg[(size_t)k * G + fl];
+        const double wt = (double)wg[(size_t)k * G + fl];
+        const double yk = A.y[k];
+        if (!use_ll) {
+            acc.add(v * yk * wt);                                       // getGradientObjective
+        } else {
+            const int yi = (int)yk;                                     // logLikeNumeratorContrib
+            double c = yi * v * wt;
+            if (MODEL == CYC_LR) c -= wt * log(1.0 + exp(v));          // nw * log(denom), denom = 1 + exb
+            if (MODEL == CYC_PR) c -= wt * exp(v);                      // nw * denom
+            acc.add(c);
+        }
+    }
+    if (use_ll && (MODEL == CYC_CLR || MODEL == CYC_CPR)) {
+        const double* dg = A.denom + (size_t)grp * A.S * G;
+        const double* ng = A.nw + (size_t)grp * A.S * G;
+        for (int s = s0 + slot; s < s1; s += nslots) acc.add(-ng[(size_t)s * G + fl] * log(dg[(size_t)s * G + fl]));
+    }
+    return acc.value();
+}
+
+template <class T, int MODEL, int G>
+__global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
+    cg::cluster_group cluster = cg::this_cluster();
+    const int C = A.C;
+    const int rank = (int)cluster.block_rank();
+    const int grp = blockIdx.x / C;
+    const int r0 = A.rpart[rank], r1 = A.rpart[rank + 1];
+    const bool grouped = (MODEL == CYC_CLR || MODEL == CYC_CPR);
+    // strata of my rows (partition boundaries are stratum starts); none if my range is empty
+    const int s0 = (grouped && r0 < r1) ? A.strat[r0] : 0;
+    const int s1 = (grouped && r0 < r1) ? (r1 >= A.K ? A.S : A.strat[r1]) : 0;
+    T* xbg = (T*)A.xb + (size_t)grp * A.K * G;
+    const T* wg = (const T*)A.w + (size_t)grp * A.K * G;
+    double* dg = grouped ? A.denom + (size_t)grp * A.S * G : nullptr;
+    const double* ng = grouped ? A.nw + (size_t)grp * A.S * G : nullptr;
+    const int fl = threadIdx.x % G;
+    const int slot = threadIdx.x / G, nslots = kBT / G;
+
+    __shared__ double2 s_part[2][G];       // this CTA's (g, h) partial, double buffered
+    __shared__ double2 s_scr[kBT / 32][G];
+    __shared__ double2 s_red[G];
+    __shared__ double s_obj[2][G];
+    __shared__ double s_delta[G];
+    __shared__ double s_last[G];
+    __shared__ int s_done[G];
+    __shared__ int s_flag[G];
+    __shared__ int s_iter[G];
+    __shared__ int s_any, s_all_done;
+
+    const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
+    const int fg = grp * G;                   // first fit of the group
+    if (threadIdx.x < G) {
+        const int f = fg + threadIdx.x;
+        s_done[threadIdx.x] = A.active[f] ? 0 : 1;
+        s_flag[threadIdx.x] = CYC_SUCCESS;
+        s_iter[threadIdx.x] = 0;
+    }
+    __syncthreads();
+
+    // initial objective (findMode :949-953)
+    int opar = 0;
+    {
+        const double p = objective_partial<T, MODEL, G>(A, grp, r0, r1, s0, s1, xbg, wg, fl, use_ll);
+        block_reduce_lanes<G>(p, 0.0, s_red, s_scr);
+        if (threadIdx.x < G) s_obj[opar][threadIdx.x] = s_red[threadIdx.x].x;
+        cluster.sync();
+        if (threadIdx.x < G) {
+            const int f = fg + threadIdx.x;
+            double o = 0.0;
+            for (int r = 0; r < C; ++r) o += *cluster.map_shared_rank(&s_obj[opar][threadIdx.x], r);
+            if (use_ll && (MODEL == CYC_PR || MODEL == CYC_CPR)) o += A.llfixed[f];
+            if (A.conv == CYC_CONV_LANGE) {
+                const double* bf = A.beta + (size_t)f * A.J;
+                for (int j = 0; j < A.J; ++j) o += log_density(A.ptype[j], A.variance[f], bf[j]);
+            }
+            s_last[threadIdx.x] = o;
+        }
+        opar ^= 1;
+    }
+
+    unsigned long long n_grad = 0, n_upd = 0, n_steps = 0, n_idx = 0;
+    int par = 0;
+    for (int it = 1; it <= A.max_iter; ++it) {
+        for (int j = 0; j < A.J; ++j) {
+            if (A.fixb[j]) continue;
+            const int fmt = A.fmt[j];
+            const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
+            const bool ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
+            const int* cidx = A.idx + A.col_ptr[j];
+            const double* cval = A.val + A.val_ptr[j];
+            int e0, e1;
+            if (dense) { e0 = r0; e1 = r1; }
+            else { e0 = A.split[j * (C + 1) + rank]; e1 = A.split[j * (C + 1) + rank + 1]; }
+            // step inputs, read before the barrier (rank 0 rewrites them after it)
+            double b_f = 0.0, hd_f = 0.0, xjy_f = 0.0, var_f = 1.0;
+            int done_f = 1;
+            if (threadIdx.x < G) {
+                const int f = fg + threadIdx.x;
+                b_f = A.beta[(size_t)f * A.J + j];
+                hd_f = A.hdelta[(size_t)f * A.J + j];
+                xjy_f = A.xjy[(size_t)f * A.J + j];
+                var_f = A.variance[f];
+                done_f = s_done[threadIdx.x];
+            }
+            // ---- gradient and Hessian of my rows (computeGradientAndHessianImpl)
+            Kahan<T> ag, ah;
+            if (!grouped) {
+                for (int e = e0 + slot; e < e1; e += nslots) {
+                    const int k = dense ? e : __ldg(cidx + e);
+                    const T x = ind ? T(1) : (T)__ldg(cval + e);
+                    const T v = xbg[(size_t)k * G + fl];
+                    const T wt = wg[(size_t)k * G + fl];
+                    const T ex = fexp(v);
+                    if (MODEL == CYC_LR) {                // Logistic::incrementGradientAndHessian
+                        const T p = ex / (T(1) + ex);
+                        const T gi = p * x;
+                        ag.add(wt * gi);
+                        ah.add(wt * (ind ? gi * (T(1) - gi) : x * x * p * (T(1) - p)));
+                    } else {                              // PoissonRegression::incrementGradientAndHessian
+                        const T n1 = ex * x;
+                        ag.add(wt * n1);
+                        ah.add(wt * (ind ? n1 : n1 * x));
+                    }
+                }
+            } else {
+                for (int e = e0 + slot; e < e1; e += nslots) {
+                    const int k = dense ? e : __ldg(cidx + e);
+                    const int s = A.strat[k];
+                    if (e > e0) {
+                        const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
+                        if (A.strat[kp] == s) continue;
+                    }
+                    T n1 = 0, n2 = 0;
+                    int q = e;
+                    int kq = k;
+                    do {                                  // the run of stratum s in this column
+                        const T x = ind ? T(1) : (T)__ldg(cval + q);
+                        const T ex = fexp(xbg[(size_t)kq * G + fl]);
+                        n1 += ex * x;
+                        if (!ind) n2 += ex * x * x;
+                        ++q;
+                        if (q >= e1) break;
+                        kq = dense ? q : __ldg(cidx + q);
+                    } while (A.strat[kq] == s);
+                    const double d = dg[(size_t)s * G + fl];
+                    const double nwv = ng[(size_t)s * G + fl];
+                    const double t = (double)n1 / d;        // ConditionalLogisticRegression::incrementGradientAndHessian
+                    const double gg = nwv * t;
+                    ag.add((T)gg);
+                    ah.add((T)(ind ? gg * (1.0 - t) : nwv * ((double)n2 / d - t * t)));
+                }
+            }
+            block_reduce_lanes<G>(ag.value(), ah.value(), s_red, s_scr);
+            if (threadIdx.x < G) s_part[par][threadIdx.x] = s_red[threadIdx.x];
+            cluster.sync();
+            // ---- coordinate step, identical in every CTA of the cluster
+            if (threadIdx.x < G) {
+                const int f = fg + threadIdx.x;
+                double g = 0.0, h = 0.0;
+                for (int r = 0; r < C; ++r) {
+                    const double2 p = *cluster.map_shared_rank(&s_part[par][threadIdx.x], r);
+                    g += p.x;
+                    h += p.y;
+                }
+                g -= xjy_f;                                     // :1181-1183
+                double delta = 0.0;
+                if (!done_f) {
+                    if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
+                    delta = prior_delta(A.ptype[j], var_f, b_f, g, h);
+                    delta = apply_bounds(&hd_f, delta);
+                    if (rank == 0) {
+                        A.hdelta[(size_t)f * A.J + j] = hd_f;
+                        if (delta != 0.0) A.beta[(size_t)f * A.J + j] = b_f + delta;
+                    }
+                }
+                s_delta[threadIdx.x] = delta;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int any = 0;
+                for (int q = 0; q < G; ++q) any |= (s_delta[q] != 0.0);
+                s_any = any;
+                if (rank == 0) {
+                    int act = 0, upd = 0;
+                    for (int q = 0; q < G; ++q) { act += !s_done[q]; upd += (s_delta[q] != 0.0); }
+                    const long long n = A.col_ptr[j + 1] - A.col_ptr[j];
+                    const long long nn = dense ? A.K : n;
+                    n_grad += (unsigned long long)(act * nn);
+                    n_upd += (unsigned long long)(upd * nn);
+                    n_steps += act;
+                    n_idx += (unsigned long long)(nn * (1 + (any ? 1 : 0)));
+                }
+            }
+            __syncthreads();
+            // ---- updateXBeta for my rows
+            if (s_any) {
+                const double dl = s_delta[fl];
+                const T d = (T)dl;
+                if (!grouped) {
+                    if (dl != 0.0) {
+                        for (int e = e0 + slot; e < e1; e += nslots) {
+                            const int k = dense ? e : __ldg(cidx + e);
+                            const T x = ind ? T(1) : (T)__ldg(cval + e);
+                            T* p = xbg + (size_t)k * G + fl;
+                            *p = *p + d * x;
+                        }
+                    }
+                } else if (dl != 0.0) {
+                    for (int e = e0 + slot; e < e1; e += nslots) {
+                        const int k = dense ? e : __ldg(cidx + e);
+                        const int s = A.strat[k];
+                        if (e > e0) {
+                            const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
+                            if (A.strat[kp] == s) continue;
+                        }
+                        double acc = dg[(size_t)s * G + fl];
+                        int q = e;
+                        int kq = k;
+                        do {
+                            const T x = ind ? T(1) : (T)__ldg(cval + q);
+                            T* p = xbg + (size_t)kq * G + fl;
+                            const T old = *p;
+                            const T nv = old + d * x;
+                            *p = nv;
+                            acc += (double)fexp(nv) - (double)fexp(old);
+                            ++q;
+                            if (q >= e1) break;
+                            kq = dense ? q : __ldg(cidx + q);
+                        } while (A.strat[kq] == s);
+                        dg[(size_t)s * G + fl] = acc;
+                    }
+                }
+            }
+            __syncthreads();
+            par ^= 1;
+        }
+        // ---- convergence test (performCheckConvergence)
+        const double p = objective_partial<T, MODEL, G>(A, grp, r0, r1, s0, s1, xbg, wg, fl, use_ll);
+        block_reduce_lanes<G>(p, 0.0, s_red, s_scr);
+        if (threadIdx.x < G) s_obj[opar][threadIdx.x] = s_red[threadIdx.x].x;
+        cluster.sync();
+        if (threadIdx.x < G) {
+            const int f = fg + threadIdx.x;
+            double o = 0.0;
+            for (int r = 0; r < C; ++r) o += *cluster.map_shared_rank(&s_obj[opar][threadIdx.x], r);
+            if (use_ll && (MODEL == CYC_PR || MODEL == CYC_CPR)) o += A.llfixed[f];
+            if (A.conv == CYC_CONV_LANGE) {
+                const double* bf = A.beta + (size_t)f * A.J;
+                for (int j = 0; j < A.J; ++j) o += log_density(A.ptype[j], A.variance[f], bf[j]);
+            }
+            if (!s_done[threadIdx.x]) {
+                double convv;
+                int ill = 0;
+                if (o != o) { convv = 0.0; ill = 1; }
+                else convv = fabs(o - s_last[threadIdx.x]) / (fabs(o) + 1.0);
+                s_iter[threadIdx.x] = it;
+                if (A.tol > 0 && convv < A.tol) {
+                    s_done[threadIdx.x] = 1;
+                    s_flag[threadIdx.x] = ill ? CYC_ILLCONDITIONED : CYC_SUCCESS;
+                } else if (it == A.max_iter) {
+                    s_done[threadIdx.x] = 1;
+                    s_flag[threadIdx.x] = CYC_MAX_ITERATIONS;
+                }
+                s_last[threadIdx.x] = o;
+            }
+        }
+        opar ^= 1;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int all = 1;
+            for (int q = 0; q < G; ++q) all &= s_done[q];
+            s_all_done = all;
+        }
+        __syncthreads();
+        if (s_all_done) break;
+    }
+    cluster.sync();   // no CTA leaves while others may still read its shared memory
+    if (rank == 0 && threadIdx.x < G) {
+        const int f = fg + threadIdx.x;
+        A.out_iter[f] = s_iter[threadIdx.x];
+        A.out_flag[f] = s_flag[threadIdx.x];
+        A.out_obj[f] = s_last[threadIdx.x];
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        atomicAdd(A.counters + 0, n_grad);
+        atomicAdd(A.counters + 1, n_upd);
+        atomicAdd(A.counters + 2, n_steps);
+        atomicAdd(A.counters + 3, n_idx);
+    }
+}
+
+// ---- set-up kernels ----------------------------------------------------------
+
+// first entry of column j whose row is >= rpart[r]
+__global__ void k_splits(int J, int C, const int* fmt, const long long* col_ptr, const int* idx,
+                         const int* rpart, int* split) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= J * (C + 1)) return;
+    const int j = t / (C + 1), r = t % (C + 1);
+    const int f = fmt[j];
+    if (f == CYC_DENSE || f == CYC_INTERCEPT) { split[t] = rpart[r]; return; }
+    const int* c = idx + col_ptr[j];
+    int lo = 0, hi = (int)(col_ptr[j + 1] - col_ptr[j]);
+    const int key = rpart[r];
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (c[mid] < key) lo = mid + 1;
+        else hi = mid;
+    }
+    split[t] = lo;
+}
+
+// one fit's weights (K doubles, or all ones) into the [group][K][G] layout
+template <class T>
+__global__ void k_scatter_weights(int K, int G, int f, const double* __restrict__ src, T* __restrict__ w) {
+    const int grp = f / G, lane = f % G;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
+        w[((size_t)grp * K + k) * G + lane] = src ? (T)src[k] : T(1);
+}
+
+// initial linear predictor of every fit from its starting coefficients
+// (zeroXBeta + axpyXBeta in column order, FP64 sums)
+template <class T>
+__global__ void k_init_xb(int K, int G, int F, const long long* __restrict__ row_ptr, const int* __restrict__ row_col,
+                          const double* __restrict__ row_val, const double* __restrict__ beta, int J,
+                          T* __restrict__ xb) {
+    const long long total = (long long)K * F;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t % F);
+        const int k = (int)(t / F);
+        const double* bf = beta + (size_t)f * J;
+        double s = 0.0;
+        for (long long p = row_ptr[k]; p < row_ptr[k + 1]; ++p) {
+            const double b = bf[row_col[p]];
+            if (b != 0.0) s = add_mul_rn(s, b, row_val[p]);
+        }
+        xb[((size_t)(f / G) * K + k) * G + (f % G)] = (T)s;
+    }
+}
+
+// per-fit XjY (computeXjY, ModelSpecifics.hpp:486-524): one block per column
+template <class T>
+__global__ void k_batch_xjy(int J, int K, int G, int ngroups, const int* fmt, const long long* col_ptr,
+                            const long long* val_ptr, const int* idx, const double* val, const double* y,
+                            const T* w, double* xjy) {
+    __shared__ double s_scr[kBT / 32][32];
+    for (int j = blockIdx.x; j < J; j += gridDim.x) {
+        const int f = fmt[j];
+        const bool dense = (f == CYC_DENSE || f == CYC_INTERCEPT);
+        const long long n = dense ? K : col_ptr[j + 1] - col_ptr[j];
+        const int* c = idx + col_ptr[j];
+        const double* v = val + val_ptr[j];
+        for (int grp = 0; grp < ngroups; ++grp) {
+            // thread = (lane, slot) over G lanes
+            const int lane = threadIdx.x % G, slot = threadIdx.x / G, ns = kBT / G;
+            double acc = 0.0;
+            for (long long e = slot; e < n; e += ns) {
+                const int k = dense ? (int)e : c[e];
+                const double x = (f == CYC_SPARSE || f == CYC_DENSE) ? v[e] : 1.0;
+                acc += x * y[k] * (double)w[((size_t)grp * K + k) * G + lane];
+            }
+            for (int o = G; o < 32; o <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            const int l = threadIdx.x & 31, wid = threadIdx.x >> 5;
+            if (l < G) s_scr[wid][l] = acc;
+            __syncthreads();
+            if (threadIdx.x < G) {
+                double s = 0.0;
+                for (int q = 0; q < kBT / 32; ++q) s += s_scr[q][threadIdx.x];
+                xjy[(size_t)(grp * G + threadIdx.x) * J + j] = s;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// grouped models: per (stratum, fit) events sum(y*w) and denominator sum(exp(xb))
+template <class T>
+__global__ void k_batch_strata(int S, int K, int G, int ngroups, const int* strat_ptr, const double* y, const T* w,
+                               const T* xb, double* nw, double* denom) {
+    const long long total = (long long)S * G * ngroups;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int lane = (int)(t % G);
+        const int s = (int)((t / G) % S);
+        const int grp = (int)(t / ((long long)G * S));
+        double a = 0.0, d = 0.0;
+        for (int k = strat_ptr[s]; k < strat_ptr[s + 1]; ++k) {
+            const size_t o = ((size_t)grp * K + k) * G + lane;
+            a += y[k] * (double)w[o];
+            d += exp((double)xb[o]);
+        }
+        nw[((size_t)grp * S + s) * G + lane] = a;
+        denom[((size_t)grp * S + s) * G + lane] = d;
+    }
+}
+
+// fixed likelihood terms per fit: sum_k w_fk * c_k with c_k = -log(y_k!)
+template <class T>
+__global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w, double* out) {
+    const int f = blockIdx.x;
+    if (f >= F) return;
+    const int grp = f / G, lane = f % G;
+    double a = 0.0, dummy = 0.0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) a += c[k] * (double)w[((size_t)grp * K + k) * G + lane];
+    block_sum2(a, dummy);
+    if (threadIdx.x == 0) out[f] = a;
+}
+
+thread_local cyc_run_stats g_batch_stats{};
+
+}  // namespace
+
+cyc_run_stats& batch_stats() { return g_batch_stats; }
+
+template <class T, int MODEL, int G>
+static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(ngroups * a.C);
+    cfg.blockDim = dim3(kBT);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = a.C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CYC_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_batch<T, MODEL, G>, a));
+}
+
+template <class T, int G>
+static void launch_model(const BatchArgs& a, int ngroups, cudaStream_t stream) {
+    switch (a.model) {
+    case CYC_LR: launch_batch<T, CYC_LR, G>(a, ngroups, stream); break;
+    case CYC_PR: launch_batch<T, CYC_PR, G>(a, ngroups, stream); break;
+    case CYC_CLR: launch_batch<T, CYC_CLR, G>(a, ngroups, stream); break;
+    case CYC_CPR: launch_batch<T, CYC_CPR, G>(a, ngroups, stream); break;
+    default: throw Error{CYC_ERR_UNSUPPORTED, "batched fits support lr, pr, clr, cpr"};
+    }
+}
+
+// One batched solve at precision T over fits [0, F) with starting
+// coefficients `h_beta` (F x J, updated in place) and trust regions.
+template <class T>
+struct BatchRunner {
+    Dataset& ds;
+    cudaStream_t stream;
+    int F, G, ngroups, Fp, C;
+    std::vector<int> rpart;
+    DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag;
+    DevBuf<T> d_xb, d_w;
+    DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
+    DevBuf<unsigned long long> d_counters;
+
+    BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_) : ds(d), stream(s), F(F_), G(G_) {
+        ngroups = (F + G - 1) / G;
+        Fp = ngroups * G;
+        const int K = ds.K;
+        C = std::max(1, std::min(kMaxC, (K + 16383) / 16384));
+        // row partition, aligned to strata for grouped models
+        rpart.assign(C + 1, K);
+        for (int r = 0; r < C; ++r) {
+            int b = (int)((long long)K * r / C);
+            if (model_grouped(ds.model)) {
+                auto it = std::lower_bound(ds.strat_ptr.begin(), ds.strat_ptr.end(), b);
+                b = (it == ds.strat_ptr.end()) ? K : *it;
+            }
+            rpart[r] = b;
+        }
+        rpart[C] = K;
+        for (int r = 1; r <= C; ++r) rpart[r] = std::max(rpart[r], rpart[r - 1]);
+    }
+
+    void setup(const cyc_prior& prior, const cyc_fit_spec* specs, const std::vector<double>& h_beta,
+               const std::vector<double>& h_hdelta) {
+        const int K = ds.K, J = ds.J;
+        d_rpart.alloc(C + 1);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_rpart.get(), rpart.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
+        d_split.alloc((size_t)J * (C + 1));
+        k_splits<<<(J * (C + 1) + 255) / 256, 256, 0, stream>>>(J, C, ds.d_fmt.get(), ds.d_col_ptr.get(), ds.d_idx.get(),
+                                                                  d_rpart.get(), d_split.get());
+        CYC_CHECK_LAUNCH();
+        std::vector<int> fixb(J, 0), pt(J, prior.prior_type), act(Fp, 0);
+        if (ds.has_offset) fixb[0] = 1;
+        for (int i = 0; i < prior.n_exclude; ++i) pt[prior.exclude[i]] = CYC_PRIOR_NONE;
+        for (int f = 0; f < F; ++f) act[f] = 1;
+        std::vector<double> var(Fp, 1.0);
+        for (int f = 0; f < F; ++f) var[f] = specs[f].variance;
+        d_fixb.alloc(J); d_ptype.alloc(J); d_active.alloc(Fp); d_var.alloc(Fp);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixb.get(), fixb.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_ptype.get(), pt.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_active.get(), act.data(), Fp * sizeof(int), cudaMemcpyHostToDevice, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_var.get(), var.data(), Fp * sizeof(double), cudaMemcpyHostToDevice, stream));
+        // weights
+        d_w.alloc((size_t)ngroups * K * G);
+        d_stage.alloc(K);
+        for (int f = 0; f < Fp; ++f) {
+            const double* src = nullptr;
+            if (f < F && specs[f].weights) {
+                CYC_CHECK_CUDA(cudaMemcpyAsync(d_stage.get(), specs[f].weights, K * sizeof(double), cudaMemcpyHostToDevice, stream));
+                src = d_stage.get();
+            }
+            k_scatter_weights<T><<<grid_for(K, 4), 256, 0, stream>>>(K, G, f, src, d_w.get());
+            CYC_CHECK_LAUNCH();
+            if (src) CYC_CHECK_CUDA(cudaStreamSynchronize(stream));  // staging buffer reuse
+        }
+        // coefficients and trust regions
+        d_beta.alloc((size_t)Fp * J);
+        d_hdelta.alloc((size_t)Fp * J);
+        std::vector<double> b((size_t)Fp * J, 0.0), hd((size_t)Fp * J, 2.0);
+        std::copy(h_beta.begin(), h_beta.end(), b.begin());
+        std::copy(h_hdelta.begin(), h_hdelta.end(), hd.begin());
+        if (ds.has_offset) for (int f = F; f < Fp; ++f) b[(size_t)f * J] = 1.0;
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_beta.get(), b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_hdelta.get(), hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
+        // linear predictors
+        ds.ensure_csr();
+        d_xb.alloc((size_t)ngroups * K * G);
+        k_init_xb<T><<<grid_for((long long)K * Fp, 1), 256, 0, stream>>>(K, G, Fp, ds.d_row_ptr.get(), ds.d_row_col.get(),
+                                                                         ds.d_row_val.get(), d_beta.get(), J, d_xb.get());
+        CYC_CHECK_LAUNCH();
+        // fixed gradient terms
+        d_xjy.alloc((size_t)Fp * J);
+        k_batch_xjy<T><<<std::min(J, 148 * 8), kBT, 0, stream>>>(J, K, G, ngroups, ds.d_fmt.get(), ds.d_col_ptr.get(),
+                                                                 ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(),
+                                                                 ds.d_y.get(), d_w.get(), d_xjy.get());
+        CYC_CHECK_LAUNCH();
+        if (model_grouped(ds.model)) {
+            d_nw.alloc((size_t)ngroups * ds.S * G);
+            d_denom.alloc((size_t)ngroups * ds.S * G);
+            k_batch_strata<T><<<grid_for((long long)ds.S * Fp, 1), 256, 0, stream>>>(
+                ds.S, K, G, ngroups, ds.d_strat_ptr.get(), ds.d_y.get(), d_w.get(), d_xb.get(), d_nw.get(), d_denom.get());
+            CYC_CHECK_LAUNCH();
+        }
+        d_llfixed.alloc(Fp);
+        CYC_CHECK_CUDA(cudaMemsetAsync(d_llfixed.get(), 0, Fp * sizeof(double), stream));
+        if (has_fixed_ll(ds.model)) {
+            std::vector<double> c(K, 0.0);
+            for (int k = 0; k < K; ++k)
+                for (int i = 2; i <= (int)ds.y[k]; ++i) c[k] -= std::log((double)i);
+            d_fixedc.alloc(K);
+            CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixedc.get(), c.data(), K * sizeof(double), cudaMemcpyHostToDevice, stream));
+            k_batch_llfixed<T><<<Fp, 256, 0, stream>>>(K, G, Fp, d_fixedc.get(), d_w.get(), d_llfixed.get());
+            CYC_CHECK_LAUNCH();
+            CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+        }
+        d_iter.alloc(Fp); d_flag.alloc(Fp); d_obj.alloc(Fp); d_counters.alloc(4);
+        CYC_CHECK_CUDA(cudaMemsetAsync(d_counters.get(), 0, 4 * sizeof(unsigned long long), stream));
+    }
+
+    void run(const cyc_control& ctl, double tol, float* ms) {
+        BatchArgs a{};
+        a.model = ds.model; a.K = ds.K; a.J = ds.J; a.S = ds.S; a.C = C;
+        a.fmt = ds.d_fmt.get(); a.col_ptr = ds.d_col_ptr.get(); a.val_ptr = ds.d_val_ptr.get();
+        a.idx = ds.d_idx.get(); a.val = ds.d_val.get(); a.split = d_split.get(); a.rpart = d_rpart.get();
+        a.y = ds.d_y.get(); a.strat = ds.d_strat.get(); a.strat_ptr = ds.d_strat_ptr.get();
+        a.fixb = d_fixb.get(); a.ptype = d_ptype.get(); a.xb = d_xb.get(); a.w = d_w.get();
+        a.denom = d_denom.get(); a.nw = d_nw.get(); a.xjy = d_xjy.get(); a.beta = d_beta.get();
+        a.hdelta = d_hdelta.get(); a.variance = d_var.get(); a.llfixed = d_llfixed.get(); a.active = d_active.get();
+        a.conv = ctl.convergence_type; a.tol = tol; a.max_iter = ctl.max_iterations;
+        a.out_iter = d_iter.get(); a.out_flag = d_flag.get(); a.out_obj = d_obj.get(); a.counters = d_counters.get();
+        cudaEvent_t e0, e1;
+        CYC_CHECK_CUDA(cudaEventCreate(&e0));
+        CYC_CHECK_CUDA(cudaEventCreate(&e1));
+        CYC_CHECK_CUDA(cudaEventRecord(e0, stream));
+        if (G == 1) launch_model<T, 1>(a, ngroups, stream);
+        else launch_model<T, 8>(a, ngroups, stream);
+        CYC_CHECK_CUDA(cudaEventRecord(e1, stream));
+        CYC_CHECK_CUDA(cudaEventSynchronize(e1));
+        CYC_CHECK_CUDA(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        CYC_CHECK_LAUNCH();
+    }
+
+    void results(std::vector<double>& beta, std::vector<double>& hd, std::vector<int>& iters, std::vector<int>& flags,
+                 unsigned long long* counters) {
+        const int J = ds.J;
+        beta.resize((size_t)F * J);
+        hd.resize((size_t)F * J);
+        iters.resize(F);
+        flags.resize(F);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(beta.data(), d_beta.get(), beta.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(hd.data(), d_hdelta.get(), hd.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(iters.data(), d_iter.get(), F * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(flags.data(), d_flag.get(), F * sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(counters, d_counters.get(), 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+    }
+};
+
+}  // namespace cyc
+
+using namespace cyc;
+
+extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
+                             const cyc_control* ctl, cyc_fit_result* out) {
+    return guarded([&] {
+        CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
+        Dataset& ds = dsh->ds;
+        CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
+                    "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
+        CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
+                        ctl->convergence_type == CYC_CONV_LANGE,
+                    CYC_ERR_UNSUPPORTED, "batched fits support gradient, mittal and lange convergence");
+        CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL, CYC_ERR_ARGUMENT,
+                    "Unknown prior type");
+        for (int i = 0; i < prior->n_exclude; ++i)
+            CYC_REQUIRE(prior->exclude[i] >= 0 && prior->exclude[i] < ds.J, CYC_ERR_ARGUMENT, "exclude index out of range");
+        for (int f = 0; f < F; ++f) {
+            CYC_REQUIRE(out[f].beta, CYC_ERR_ARGUMENT, "null result buffer");
+            CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || specs[f].variance > 0, CYC_ERR_ARGUMENT,
+                        "prior variance must be positive");
+        }
+        CYC_CHECK_CUDA(cudaSetDevice(ds.device));
+        cudaStream_t stream;
+        CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{stream};
+        const int J = ds.J;
+        std::vector<double> beta((size_t)F * J, 0.0), hd((size_t)F * J, ctl->initial_bound);
+        for (int f = 0; f < F; ++f) {
+            if (specs[f].start_beta) std::copy(specs[f].start_beta, specs[f].start_beta + J, beta.begin() + (size_t)f * J);
+            if (ds.has_offset) beta[(size_t)f * J] = 1.0;
+        }
+        const int G = F >= 4 ? 8 : 1;
+        std::vector<int> iters, flags;
+        unsigned long long ctr[4] = {0, 0, 0, 0};
+        float ms_total = 0.f;
+        double grad = 0, upd = 0, steps = 0, idx = 0;
+        int launches = 0;
+        int state_bytes = 8;
+        if (ctl->precision == CYC_MIXED) {
+            // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
+            BatchRunner<float> r32(ds, stream, F, G);
+            r32.setup(*prior, specs, beta, hd);
+            float ms = 0.f;
+            cyc_control c32 = *ctl;
+            r32.run(c32, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
+            r32.results(beta, hd, iters, flags, ctr);
+            ms_total += ms;
+            grad += ctr[0]; upd += ctr[1]; steps += ctr[2]; idx += ctr[3];
+            launches++;
+            state_bytes = 4;
+            // the FP64 phase restarts the trust regions (resetBounds, :943)
+            std::fill(hd.begin(), hd.end(), ctl->initial_bound);
+        }
+        BatchRunner<double> r64(ds, stream, F, G);
+        r64.setup(*prior, specs, beta, hd);
+        float ms = 0.f;
+        r64.run(*ctl, ctl->tolerance, &ms);
+        std::vector<int> it64;
+        r64.results(beta, hd, it64, flags, ctr);
+        ms_total += ms;
+        grad += ctr[0]; upd += ctr[1]; steps += ctr[2]; idx += ctr[3];
+        launches++;
+        // log likelihood and prior of every result through the FP64 engine
+        Engine eng(&ds);
+        for (int f = 0; f < F; ++f) {
+            std::copy(beta.begin() + (size_t)f * J, beta.begin() + (size_t)(f + 1) * J, out[f].beta);
+            out[f].iterations = it64[f];
+            out[f].return_flag = flags[f];
+            eng.set_weights(specs[f].weights, specs[f].weights != nullptr);
+            eng.fixed_terms_ll(true);
+            eng.compute_xbeta(out[f].beta);
+            eng.remaining_statistics(true);
+            out[f].log_likelihood = eng.log_likelihood(true);
+            double lp = 0.0;
+            std::vector<int> pt(J, prior->prior_type);
+            for (int i = 0; i < prior->n_exclude; ++i) pt[prior->exclude[i]] = CYC_PRIOR_NONE;
+            for (int j = 0; j < J; ++j) lp += log_density(pt[j], specs[f].variance, out[f].beta[j]);
+            out[f].log_prior = lp;
+        }
+        cyc_run_stats& st = batch_stats();
+        st = cyc_run_stats{};
+        st.kernel_ms = ms_total;
+        st.gradient_entries = grad;
+        st.update_entries = upd;
+        st.coordinate_steps = steps;
+        st.index_entries = idx;
+        st.launches = launches;
+        st.state_bytes = state_bytes;
+    });
 }

@@ -17,7 +17,7 @@
 
 namespace cyc {
 
-Engine::Engine(Dataset* d) : ds(d) {
+Engine::Engine(Dataset* d) : ds(d), device(d->device) {
     CYC_CHECK_CUDA(cudaSetDevice(ds->device));
     CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     CYC_CHECK_CUDA(cudaMallocHost(&h_result, 8 * sizeof(double)));
@@ -46,7 +46,7 @@ Engine::Engine(Dataset* d) : ds(d) {
 }
 
 Engine::~Engine() {
-    cudaSetDevice(ds->device);
+    cudaSetDevice(device);
     if (stream) cudaStreamDestroy(stream);
     if (h_result) cudaFreeHost(h_result);
 }
@@ -192,7 +192,7 @@ void Engine::set_weights(const double* w, bool use_cv) {
     } else {
         k_nw_grouped<<<grid_for(N, 1), kThreads, 0, stream>>>(N, group_rows(), ds->d_y.get(), kw.get(), nw.get());
     }
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     stats_known = false;
 }
 
@@ -202,7 +202,7 @@ void Engine::fixed_terms_ll(bool use_cv) {
     const int blocks = grid_for(K, 4);
     k_fixed_ll<<<blocks, kThreads, 0, stream>>>(K, ds->d_y.get(), kw.get(), use_cv && use_w,
                                                 partial.get(), ticket.get(), ll_fixed.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 void Engine::fixed_terms_gh(bool use_cv) {
@@ -210,7 +210,7 @@ void Engine::fixed_terms_gh(bool use_cv) {
     k_xjy<<<std::min(J, 148 * 16), 128, 0, stream>>>(J, ds->d_fmt.get(), ds->d_col_ptr.get(),
                                                      ds->d_val_ptr.get(), ds->d_idx.get(), ds->d_val.get(),
                                                      ds->K, ds->d_y.get(), kw.get(), use_cv && use_w, xjy.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 void Engine::zero_xbeta() {
@@ -222,7 +222,7 @@ void Engine::axpy_xbeta(double beta, int j) {
     if (beta == 0.0) return;
     ColView c = ds->view(j);
     k_axpy<<<grid_for(c.n, 4), kThreads, 0, stream>>>(c, beta, xb.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     stats_known = false;
 }
 
@@ -243,7 +243,7 @@ void Engine::compute_xbeta_device(const double* d_beta) {
     const int K = ds->K;
     k_xbeta_rows<<<grid_for(K, 1), kThreads, 0, stream>>>(K, ds->d_row_ptr.get(), ds->d_row_col.get(),
                                                           ds->d_row_val.get(), d_beta, xb.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     stats_known = false;
 }
 
@@ -265,7 +265,7 @@ void Engine::remaining_statistics(bool use_weights) {
             exb.get(), denom.get());
         if (model_cumulative(model)) cox_rescan(0);
     }
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     stats_known = true;
 }
 
@@ -280,7 +280,7 @@ void Engine::numerator_for_gradient(int j, bool use_weights) {
     else
         k_cox_numerator<false><<<blocks, kThreads, 0, stream>>>(c, group.get(), exb.get(), kw.get(),
                                                                use_weights && use_w, numer.get(), numer2.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 // launches the gradient/Hessian of column j into out[0..1] (device)
@@ -320,7 +320,7 @@ void Engine::launch_gradient(int j, bool use_weights, double* out) {
             k_cox_gradient<false><<<1, kThreads, 0, stream>>>(glist.get() + b, L, gstart.get(), gend.get(), numer.get(), numer2.get(), P1h.get(), P1l.get(), P2h.get(), P2l.get(), xjy.get(), j, out);
         }
     }
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 void Engine::gradient_hessian(int j, bool use_weights, double* g, double* h) {
@@ -346,7 +346,7 @@ void Engine::launch_update(int j, bool use_weights, const double* d_delta, doubl
                                                           xb.get(), exb.get(), denom.get());
         if (model_cumulative(model)) cox_rescan_gated(d_delta, first_group(j));
     }
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 int Engine::first_group(int j) const { return h_first_group[j]; }
@@ -365,7 +365,7 @@ void Engine::cox_rescan_gated(const double* gate, int lo) {
                                          P2h.get(), P2l.get());
     k_scanP_write<<<ntiles, kThreads, 0, stream>>>(gate, lo, hi, gstart.get(), D.get(), nw.get(), aggP.get(),
                                                    P1h.get(), P1l.get(), P2h.get(), P2l.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 void Engine::update_xbeta(double delta, int j, bool use_weights) {
@@ -380,7 +380,7 @@ void Engine::launch_loglik(bool use_cv, double* out) {
     k_loglik<<<grid_for(M, 4), kThreads, 0, stream>>>(model, K, N, ds->d_y.get(), xb.get(), kw.get(),
                                                       use_cv && use_w, nw.get(), den, ll_fixed.get(),
                                                       partial.get(), ticket.get(), out);
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 double Engine::log_likelihood(bool use_cv) {
@@ -394,7 +394,7 @@ void Engine::launch_gradient_objective(bool use_cv, double* out) {
     const int K = ds->K;
     k_grad_objective<<<grid_for(K, 4), kThreads, 0, stream>>>(K, ds->d_y.get(), xb.get(), kw.get(),
                                                               use_cv && use_w, partial.get(), ticket.get(), out);
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
 }
 
 double Engine::gradient_objective(bool use_cv) {
@@ -421,7 +421,7 @@ double Engine::predictive_log_likelihood(const double* w) {
     k_pred_loglik<<<grid_for(K, 4), kThreads, 0, stream>>>(model, K, ds->d_y.get(), xb.get(), weights_buf.get(),
                                                            groups(), den, partial.get(), ticket.get(),
                                                            result.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     CYC_CHECK_CUDA(cudaMemcpyAsync(h_result, result.get(), sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
     const double out = h_result[0];
@@ -445,7 +445,7 @@ void Engine::predictive_estimates(double* y, const double* w) {
         dw = weights_buf.get();
     }
     k_pred_estimates<<<grid_for(K, 1), kThreads, 0, stream>>>(model, K, xb.get(), dw, out.get());
-    CYC_CHECK_CUDA(cudaGetLastError());
+    CYC_CHECK_LAUNCH();
     CYC_CHECK_CUDA(cudaMemcpyAsync(y, out.get(), K * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
 }

@@ -12,7 +12,8 @@ struct Engine {
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
 
-    Dataset* ds;
+    Dataset* ds;                  // borrowed: the caller keeps the dataset alive
+    int device = 0;
     cudaStream_t stream = nullptr;
     int model = 0;
     int N = 0;              // denominators: K (lr/pr), strata (clr/cpr), risk-set groups (cox)

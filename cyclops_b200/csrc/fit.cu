@@ -148,6 +148,7 @@ struct FitRunner {
         e.numerator_for_gradient(j, true);
         e.launch_gradient(j, true, gh.get());
         k_step<<<1, 32, 0, e.stream>>>(j, gh.get(), step_state());
+        CYC_CHECK_LAUNCH();
         e.launch_update(j, true, delta.get(), 0.0);
     }
 
@@ -178,7 +179,7 @@ struct FitRunner {
         } else if (conv == CYC_CONV_ONE_STEP) {
             CYC_CHECK_CUDA(cudaMemsetAsync(obj.get(), 0, sizeof(double), e.stream));
         }
-        CYC_CHECK_CUDA(cudaGetLastError());
+        CYC_CHECK_LAUNCH();
     }
 
     // findMode (CyclicCoordinateDescent.cpp:909-1216), cyclic branch
@@ -192,6 +193,7 @@ struct FitRunner {
         if (conv < CYC_CONV_ZHANG_OLES) {
             launch_objective(conv);
             k_copy<<<1, 1, 0, e.stream>>>(1, obj.get(), last.get());
+            CYC_CHECK_LAUNCH();
         } else {
             e.xb_save.alloc(K);
             k_copy<<<grid_for(K, 1), kThreads, 0, e.stream>>>(K, e.xb.get(), e.xb_save.get());
@@ -204,6 +206,7 @@ struct FitRunner {
             if (conv < CYC_CONV_ZHANG_OLES) {
                 launch_objective(conv);
                 k_check<<<1, 32, 0, e.stream>>>(obj.get(), last.get(), ctl.tolerance, it, ctl.max_iterations, 0, flags.get());
+                CYC_CHECK_LAUNCH();
             } else {
                 k_zhang_oles<<<grid_for(K, 4), kThreads, 0, e.stream>>>(K, e.xb.get(), e.xb_save.get(), e.kw.get(),
                                                                         e.use_w, e.partial.get(), e.ticket.get(), obj.get());

@@ -32,6 +32,15 @@ struct Error {
         }                                                                               \
     } while (0)
 
+// reports a failed (or pending) launch with the call site
+#define CYC_CHECK_LAUNCH()                                                              \
+    do {                                                                                \
+        cudaError_t e_ = cudaGetLastError();                                            \
+        if (e_ != cudaSuccess)                                                          \
+            throw ::cyc::Error{CYC_ERR_CUDA, std::string(__FILE__ ":") +                \
+                               std::to_string(__LINE__) + ": " + cudaGetErrorString(e_)}; \
+    } while (0)
+
 #define CYC_REQUIRE(cond, status, msg)                                                  \
     do {                                                                                \
         if (!(cond)) throw ::cyc::Error{(status), (msg)};                               \
@@ -39,6 +48,9 @@ struct Error {
 
 template <class F>
 int guarded(F&& f) {
+    // a non-sticky error left by an earlier, unrelated runtime call must not
+    // be reported against this call's launches
+    (void)cudaGetLastError();
     try {
         f();
         return CYC_OK;

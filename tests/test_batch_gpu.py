@@ -1,0 +1,94 @@
+"""Batched device-resident CCD (cyc_batch_fit): every fit of a batch equals
+the reference engine's fit of the same (weights, prior) on its own."""
+import numpy as np
+import pytest
+
+from conftest import exclude_for, load_golden, rel_err
+from cyclops_b200 import data as D
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_fit(data, prior, variance, weights, tol=1e-6, conv=D.CONV_GRADIENT):
+    from oracle import oracle as O
+    return O.port().fit(data, prior, variance, control=O.make_control(tolerance=tol, convergence_type=conv),
+                        weights=weights)
+
+
+def _check(fit, ref, beta_tol=1e-4):
+    np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
+    err = np.abs(fit.beta - ref.beta) / np.maximum(np.abs(ref.beta), 1.0)
+    assert err.max() < beta_tol, err.max()
+
+
+@pytest.mark.parametrize("name", ["lr_laplace_small", "lr_normal_weighted", "pr_laplace_weighted",
+                                  "clr_laplace", "clr_normal_weighted", "cpr_normal", "pr_offset_normal"])
+@pytest.mark.parametrize("nfits", [1, 6, 11])
+def test_batch_fits_match_reference(cuda_lib, name, nfits):
+    from cyclops_b200 import api
+    data, s = load_golden(name)
+    rng = np.random.default_rng(nfits)
+    var0 = float(s["variance"])
+    variances = [var0 * (1.0 + 0.5 * (f % 3)) for f in range(nfits)]
+    weights = []
+    for f in range(nfits):
+        if f == 0:
+            weights.append(s["weights"])
+        elif data.model in (D.CLR, D.CPR):
+            strata = data.strata()
+            keep = (rng.random(strata.max() + 1) > 0.2).astype(float)
+            weights.append(keep[strata])
+        else:
+            weights.append((rng.random(data.K) > 0.2).astype(float))
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    fits = api.batch_fit(data, prior, variances, weights, api.create_control(tolerance=1e-6))
+    for f in range(nfits):
+        ref = _ref_fit(data, int(s["prior"]), variances[f], weights[f])
+        assert fits[f].return_flag == ref.return_flag
+        assert abs(fits[f].iterations - ref.iterations) <= 1, (f, fits[f].iterations, ref.iterations)
+        _check(fits[f], ref)
+        assert rel_err(fits[f].log_likelihood, ref.log_likelihood) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["lr_c1", "clr_laplace", "pr_laplace_weighted"])
+def test_mixed_precision_batch_reaches_fp64_fit(cuda_lib, name):
+    """FP32 state with compensated sums, then the FP64 polish: the result is
+    the FP64 oracle's fit to 1e-6 relative when both are converged tightly."""
+    from cyclops_b200 import api
+    data, s = load_golden(name)
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    ctl = api.create_control(tolerance=1e-12, convergence_type="mittal", precision="mixed", polish_tolerance=1e-5,
+                             max_iterations=3000)
+    fits = api.batch_fit(data, prior, [float(s["variance"])] * 3, [s["weights"]] * 3, ctl)
+    ref = _ref_fit(data, int(s["prior"]), float(s["variance"]), s["weights"], tol=1e-12, conv=D.CONV_MITTAL)
+    for fit in fits:
+        np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
+        ok = np.abs(fit.beta - ref.beta) <= 1e-6 * np.abs(ref.beta) + 1e-9
+        assert ok.all(), np.max(np.abs(fit.beta - ref.beta) / (np.abs(ref.beta) + 1e-9))
+        assert rel_err(fit.log_likelihood, ref.log_likelihood) < 1e-9
+
+
+def test_cv_folds_times_grid(cuda_lib):
+    """5 folds x 3 prior variances from the reference's fold rule, as one batch."""
+    from cyclops_b200 import api
+    data, s = load_golden("lr_laplace_small")
+    folds = api.cv_fold_weights(data.K, 5, 17)
+    lams = [0.5, 1.0, 2.0]
+    variances, weights = [], []
+    for lam in lams:
+        for f in range(5):
+            variances.append(D.laplace_variance(lam))
+            weights.append(folds[f])
+    prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, exclude_for(data))
+    fits = api.batch_fit(data, prior, variances, weights, api.create_control())
+    for i, fit in enumerate(fits):
+        ref = _ref_fit(data, D.PRIOR_LAPLACE, variances[i], weights[i])
+        _check(fit, ref)
+
+
+def test_batch_rejects_cox(cuda_lib):
+    from cyclops_b200 import api, _native
+    data, s = load_golden("cox_laplace")
+    with pytest.raises(_native.CyclopsError) as ei:
+        api.batch_fit(data, api.create_prior("laplace", 1.0), [1.0, 2.0])
+    assert ei.value.status == 4

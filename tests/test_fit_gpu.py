@@ -17,11 +17,12 @@ BETA_ATOL = 1e-9
 LL_RTOL = 1e-9
 
 
-def _gpu_fit(data, s, tolerance=None, convergence=None):
+def _gpu_fit(data, s, tolerance=None, convergence=None, max_iterations=1000):
     from cyclops_b200 import api
     prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
     ctl = api.create_control(tolerance=float(s["tolerance"]) if tolerance is None else tolerance,
-                             convergence_type=int(s["convergence"]) if convergence is None else convergence)
+                             convergence_type=int(s["convergence"]) if convergence is None else convergence,
+                             max_iterations=max_iterations)
     return api.fit_cyclops_model(data, prior, ctl, weights=s["weights"])
 
 
@@ -49,7 +50,8 @@ def test_device_fit_tight_contract(cuda_lib, name):
     data, s = load_golden(name)
     ctl = O.make_control(tolerance=1e-12, convergence_type=D.CONV_MITTAL, max_iterations=5000)
     ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
-    fit = _gpu_fit(data, s, tolerance=1e-12, convergence=D.CONV_MITTAL)
+    fit = _gpu_fit(data, s, tolerance=1e-12, convergence=D.CONV_MITTAL, max_iterations=5000)
+    assert fit.iterations == ref.iterations
     np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
     ok = np.abs(fit.beta - ref.beta) <= BETA_RTOL * np.abs(ref.beta) + BETA_ATOL
     assert ok.all(), np.max(np.abs(fit.beta - ref.beta) / (np.abs(ref.beta) + 1e-3))
