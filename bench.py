@@ -1,0 +1,376 @@
+"""Benchmark: batched cross-validation of Laplace logistic regression.
+
+Workload (one step): 10 folds x 20 Laplace rates lambda log-spaced over
+1e-4..1 = 200 fits of L1 logistic regression that share one matrix of
+K = 500,000 rows and P = 20,000 binary indicator columns (Zipf(1.1) column
+frequencies, 0.2 % mean density, ~20M stored entries) plus an intercept,
+seeded synthetic data.  Every fit runs to the reference's default
+convergence (gradient criterion, tolerance 1e-6); folds follow the
+reference's CrossValidationSelector rule.  Metric: fits per second.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+Our arm times cyc_cv_grid_fit (device-resident data, one persistent kernel
+per precision phase); `e2e` times the same call with the data uploaded from
+pinned host memory and the coefficients read back inside every step.  The
+reference arm times the reference Cyclops CPU engine (compiled from its own
+sources, oracle/_ref) on a bounded sample of the same fits, all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from cyclops_b200 import data as D  # noqa: E402
+
+N_FOLDS = 10
+N_LAMBDA = 20
+FOLD_SEED = 123
+
+
+def workload(quick: bool):
+    if quick:
+        K, P, density = 20_000, 500, 0.01
+    else:
+        K, P, density = 500_000, 20_000, 0.002
+    t0 = time.time()
+    data = D.synth_logistic(K=K, P=P, density=density, zipf=1.1, n_true=200, sd_true=0.5, intercept=-1.0,
+                            seed=4)
+    lambdas = D.lambda_grid(1e-4, 1.0, N_LAMBDA)
+    variances = np.array([D.laplace_variance(l) for l in lambdas])
+    desc = {
+        "workload": (f"cv grid: {N_FOLDS} folds x {N_LAMBDA} lambda (1e-4..1) = {N_FOLDS * N_LAMBDA} "
+                     f"Laplace logistic fits; K={K} rows, P={P} indicators at {density * 100:g}% Zipf(1.1) + "
+                     f"intercept, seed 4"),
+        "rows": K, "columns": data.J, "stored_entries": data.nnz, "fits": N_FOLDS * N_LAMBDA,
+        "convergence": "gradient", "tolerance": 1e-6, "prior": "laplace, intercept excluded",
+        "lambda_to_variance": "variance = 2/lambda^2",
+        "l2": "inputs larger than L2: per-fit state 200 fits x K rows x 4-8 B",
+    }
+    return data, lambdas, variances, desc, time.time() - t0
+
+
+def fold_ids(K: int, seed: int) -> np.ndarray:
+    from cyclops_b200 import api
+    masks = api.cv_fold_weights(K, N_FOLDS, seed)
+    return api.fold_ids_from_weights(masks)
+
+
+class Clocks:
+    """nvidia-smi sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
+                                 f".clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sms, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9 or not p[0].isdigit() or int(p[0]) != self.device:
+                    continue
+                sms.append(float(p[1]))
+                mx = float(p[2])
+                for n, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        finally:
+            try:
+                os.remove(self.path)
+            except OSError:
+                pass
+        return {"sm_mhz": statistics.median(sms) if sms else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_record(workload_name):
+    """DRAM bytes per launch of the dominant kernel from a committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "batch_cv_traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        if t.get("workload") == workload_name:
+            return t
+    except Exception:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------------
+# CPU legs (reference engine; port if the reference was not built)
+# --------------------------------------------------------------------------
+
+def cpu_fits(data, variances, folds, fit_ids, threads):
+    from oracle import oracle as O
+    kind = "reference" if O.have_ref() else "port"
+    lib = O.ref() if kind == "reference" else O.port()
+    excl = [0]
+
+    def one(i):
+        v = variances[i // N_FOLDS]
+        f = i % N_FOLDS
+        w = (folds != f).astype(np.float64)
+        return lib.fit(data, D.PRIOR_LAPLACE, float(v), control=None, exclude=excl, weights=w)
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        res = list(ex.map(one, fit_ids))
+    return res, time.perf_counter() - t0, kind
+
+
+def sample_ids(n: int):
+    F = N_FOLDS * N_LAMBDA
+    step = max(1, F // n)
+    return [(i * step + (i % N_FOLDS)) % F for i in range(n)]
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    data, lambdas, variances, desc, _ = workload(args.quick)
+    folds = fold_ids(data.K, FOLD_SEED)
+    threads = os.cpu_count() or 1
+    ids = sample_ids(threads)
+    for _ in range(args.warmup):
+        cpu_fits(data, variances, folds, ids, threads)
+    total, n, kind = 0.0, 0, None
+    for _ in range(args.steps):
+        res, dt, kind = cpu_fits(data, variances, folds, ids, threads)
+        total += dt
+        n += len(ids)
+    value = n / total
+    line = {
+        "impl": "reference", "metric": "cv_fits_per_second", "value": value, "unit": "fits/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": desc,
+        "cpu_baseline": {"value": value, "unit": "fits/s", "cores": threads, "kind": kind,
+                         "sample": f"{len(ids)} fits of the grid per step (one per thread), spread over folds and lambda"},
+        "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# --------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist_
+        dist = dist_
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    device = local
+
+    from cyclops_b200 import api, build as B
+    B.build()
+    data, lambdas, variances, desc, gen_s = workload(args.quick)
+    folds = fold_ids(data.K, FOLD_SEED + rank)     # independent replicas per rank
+    prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, [0])
+    control = api.create_control(tolerance=1e-6, precision=args.precision, polish_tolerance=1e-4)
+    F = N_FOLDS * N_LAMBDA
+
+    ds = api.Dataset(data, device)
+
+    def step():
+        return api.cv_grid_fit(ds, prior, folds, N_FOLDS, variances, control)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    launches0 = api.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms, phase_ms, phase_bytes = 0.0, [0.0, 0.0], [0.0, 0.0]
+    state_bytes = [0, 0]
+    with Clocks(device) as clk:
+        torch.cuda.synchronize(device)
+        ev0.record()
+        for _ in range(args.steps):
+            res = step()
+            st = api.last_run_stats()
+            kernel_ms += st["kernel_ms"]
+            for p in range(st["phases"]):
+                phase_ms[p] += st["phase_ms"][p]
+                phase_bytes[p] += st["phase_bytes"][p]
+                state_bytes[p] = st["phase_state_bytes"][p]
+        ev1.record()
+        torch.cuda.synchronize(device)
+    barrier()
+    launches = api.launch_count() - launches0
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    value = F * world * args.steps / (ms / 1000.0)
+    clocks = clk.summary()
+
+    # end to end: upload from pinned host memory + solve + read back, every step
+    pinned = {}
+    for name in ("y", "col_format", "col_ptr", "col_idx", "val_ptr", "col_val"):
+        a = getattr(data, name)
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        pinned[name] = t
+    hdata = D.CyclopsData(model=data.model, y=pinned["y"].numpy(), col_format=pinned["col_format"].numpy(),
+                          col_ptr=pinned["col_ptr"].numpy(), col_idx=pinned["col_idx"].numpy(),
+                          val_ptr=pinned["val_ptr"].numpy(), col_val=pinned["col_val"].numpy(),
+                          has_intercept=True)
+    h2d = sum(t.numel() * t.element_size() for t in pinned.values()) + folds.nbytes + variances.nbytes
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d2 = api.Dataset(hdata, device)
+        r2 = api.cv_grid_fit(d2, prior, folds, N_FOLDS, variances, control)
+        d2.close()
+    e1.record()
+    torch.cuda.synchronize(device)
+    barrier()
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1))
+    d2h = F * data.J * 8 + F * (8 * 4)
+    e2e = F * world * args.steps / (ms_e2e / 1000.0)
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        dom = int(np.argmax(phase_ms))
+        achieved = phase_bytes[dom] / (phase_ms[dom] / 1000.0) / 1e9 if phase_ms[dom] > 0 else 0.0
+        tr = traffic_record(desc["workload"])
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_source": peak_kind,
+                    "kernel": f"k_batch<{'float' if state_bytes[dom] == 4 else 'double'},LR,8>",
+                    "algorithmic_bytes_per_launch": phase_bytes[dom] / args.steps,
+                    "launch_ms": phase_ms[dom] / args.steps,
+                    "traffic": (tr["dram_bytes_per_launch"] if tr else None)}
+        mean_cycles = float(np.mean([f.iterations for f in res.fits]))
+        line = {
+            "metric": "cv_fits_per_second", "value": value, "unit": "fits/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+            "config": dict(desc, precision=args.precision, mean_cycles_per_fit=mean_cycles,
+                           converged=int(sum(f.return_flag == 0 for f in res.fits))),
+            "clocks": clocks,
+            "e2e": {"value": e2e, "unit": "fits/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "kernel_ms_per_step": kernel_ms / args.steps,
+            "cv": {"best_lambda": float(lambdas[res.best]) if res.best >= 0 else None,
+                   "grid_mean_pred_loglik": [float(x) for x in res.grid_mean]},
+        }
+    if dist:
+        dist.barrier()
+    if rank == 0 and world == 1 and not args.no_baselines:
+        # plain FP64 single-fit GPU CCD (host-driven loop): 2 cycles of one fit
+        i0 = sample_ids(1)[0]
+        w = (folds != (i0 % N_FOLDS)).astype(np.float64)
+        ctl2 = api.create_control(tolerance=1e-6, max_iterations=2)
+        pr = api.PriorSpec(D.PRIOR_LAPLACE, float(variances[i0 // N_FOLDS]), [0])
+        t0 = time.perf_counter()
+        api.fit_cyclops_model(ds, pr, ctl2, weights=w, host_loop=True)
+        per_cycle = (time.perf_counter() - t0) / 2.0
+        plain = 1.0 / (per_cycle * mean_cycles)
+        line["plain_fp64_gpu_ccd"] = {"fits_per_s": plain, "seconds_per_cycle": per_cycle,
+                                      "sample": "1 fit, 2 cycles timed, scaled by the batch's mean cycles per fit"}
+        line["speedup_vs_plain_fp64_gpu_ccd"] = value / plain
+        # CPU baseline on a bounded sample; checks our fits against it
+        threads = os.cpu_count() or 1
+        ids = sample_ids(min(threads, 16))
+        cres, dt, kind = cpu_fits(data, variances, folds, ids, min(threads, 16))
+        err = 0.0
+        for i, c in zip(ids, cres):
+            g = res.fits[i].beta
+            err = max(err, float(np.max(np.abs(g - c.beta) / np.maximum(np.abs(c.beta), 1.0))))
+        line["cpu_baseline"] = {"value": len(ids) / dt, "unit": "fits/s", "cores": min(threads, 16), "kind": kind,
+                                "sample": f"{len(ids)} fits of the grid, one per thread"}
+        line["check"] = {"fits_compared": len(ids), "max_rel_err_beta_vs_cpu": err}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--quick", action="store_true", help="small problem (smoke runs)")
+    ap.add_argument("--no-baselines", action="store_true")
+    args = ap.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -54,9 +54,11 @@ class FitResult(C.Structure):
 
 
 class RunStats(C.Structure):
-    _fields_ = [("kernel_ms", C.c_double), ("gradient_entries", C.c_double),
-                ("update_entries", C.c_double), ("coordinate_steps", C.c_double),
-                ("index_entries", C.c_double), ("launches", C.c_int), ("state_bytes", C.c_int)]
+    _fields_ = [("kernel_ms", C.c_double), ("algorithmic_bytes", C.c_double),
+                ("gradient_entries", C.c_double), ("update_entries", C.c_double),
+                ("coordinate_steps", C.c_double), ("index_entries", C.c_double), ("cycles", C.c_double),
+                ("launches", C.c_int), ("phases", C.c_int), ("phase_ms", C.c_double * 2),
+                ("phase_bytes", C.c_double * 2), ("phase_state_bytes", C.c_int * 2)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)
@@ -94,8 +96,13 @@ _SIGS = {
                       C.POINTER(FitResult)],
     "cyc_last_run_stats": [C.POINTER(RunStats)],
     "cyc_cv_fold_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_int, C.c_int, C.c_void_p],
+    "cyc_launch_count": [],
+    "cyc_cv_grid_fit": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                        C.POINTER(Control), C.POINTER(FitResult), C.c_void_p, C.c_void_p],
+    "cyc_fit_host_loop": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control),
+                          C.POINTER(FitResult)],
 }
-_RESTYPE = {"cyc_last_error": C.c_char_p}
+_RESTYPE = {"cyc_last_error": C.c_char_p, "cyc_launch_count": C.c_longlong}
 
 _lock = threading.Lock()
 _lib = None

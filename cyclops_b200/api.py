@@ -251,8 +251,13 @@ def _prior_struct(data: CyclopsData, prior: PriorSpec):
 
 
 def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional[ControlSpec] = None,
-                      weights=None, starting_coefficients=None, device: int = 0) -> FitResult:
-    """fitCyclopsModel (R/ModelFit.R:65): one fit, CCD loop on the GPU."""
+                      weights=None, starting_coefficients=None, device: int = 0,
+                      host_loop: bool = False) -> FitResult:
+    """fitCyclopsModel (R/ModelFit.R:65): one fit, CCD loop on the GPU.
+
+    ``host_loop=True`` runs the plain FP64 single-fit GPU CCD instead: the
+    host drives the engine coordinate by coordinate, reading (gradient,
+    Hessian) back each time, as the reference's CyclicCoordinateDescent does."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     prior = prior or create_prior("none")
     control = control or create_control()
@@ -263,8 +268,14 @@ def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional
     beta = np.zeros(ds.data.J)
     out = N.FitResult(beta=beta.ctypes.data)
     c = _control_struct(control)
-    N.check(N.lib().cyc_fit(ds.handle, C.byref(p), C.byref(spec), C.byref(c), C.byref(out)))
+    fn = N.lib().cyc_fit_host_loop if host_loop else N.lib().cyc_fit
+    N.check(fn(ds.handle, C.byref(p), C.byref(spec), C.byref(c), C.byref(out)))
     return FitResult(beta, out.log_likelihood, out.log_prior, out.iterations, out.return_flag)
+
+
+def launch_count() -> int:
+    """Kernels launched by libcyclops_b200.so in this process."""
+    return int(N.lib().cyc_launch_count())
 
 
 def batch_fit(data, prior: PriorSpec, variances: Sequence[float], weights: Optional[Sequence] = None,
@@ -296,6 +307,48 @@ def batch_fit(data, prior: PriorSpec, variances: Sequence[float], weights: Optio
                       results[f].iterations, results[f].return_flag) for f in range(F)]
 
 
+@dataclasses.dataclass
+class CvGridResult:
+    fits: List[FitResult]          # n_var * n_folds, variance-major
+    pred_loglik: np.ndarray        # held-out predictive log likelihood per fit
+    grid_mean: np.ndarray          # per variance: mean over folds (NaN ignored)
+    variances: np.ndarray
+    best: int                      # index of the variance with the largest mean
+
+
+def cv_grid_fit(data, prior: PriorSpec, fold_of_row, n_folds: int, variances: Sequence[float],
+                control: Optional[ControlSpec] = None, device: int = 0) -> CvGridResult:
+    """Cross-validation over a prior-variance grid as one batched GPU solve
+    (GridSearchCrossValidationDriver + AbstractCrossValidationDriver)."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    control = control or create_control()
+    p, keep_ex = _prior_struct(ds.data, prior)
+    fold = np.ascontiguousarray(fold_of_row, np.int32)
+    var = np.ascontiguousarray(variances, np.float64)
+    F = n_folds * var.size
+    results = (N.FitResult * F)()
+    betas = np.zeros((F, ds.data.J))
+    for f in range(F):
+        results[f] = N.FitResult(beta=betas[f].ctypes.data)
+    pll = np.zeros(F)
+    gm = np.zeros(var.size)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_cv_grid_fit(ds.handle, C.byref(p), _ptr(fold), int(n_folds), _ptr(var), int(var.size),
+                                    C.byref(c), results, _ptr(pll), _ptr(gm)))
+    fits = [FitResult(betas[f].copy(), results[f].log_likelihood, results[f].log_prior,
+                      results[f].iterations, results[f].return_flag) for f in range(F)]
+    best = int(np.nanargmax(gm)) if np.any(np.isfinite(gm)) else -1
+    return CvGridResult(fits, pll, gm, var, best)
+
+
+def fold_ids_from_weights(masks: np.ndarray) -> np.ndarray:
+    """(folds, K) 0/1 masks that partition the rows -> fold id per row."""
+    held = masks == 0
+    if not np.all(held.sum(axis=0) == 1):
+        raise ValueError("masks must hold out every row exactly once")
+    return np.argmax(held, axis=0).astype(np.int32)
+
+
 def cv_fold_weights(K: int, folds: int, seed: int, ids=None, n_reps: int = 1) -> np.ndarray:
     """(n_reps*folds, K) 0/1 masks, by row (ids None) or by stratum id, drawn
     exactly as the reference's CrossValidationSelector draws them."""
@@ -309,4 +362,8 @@ def cv_fold_weights(K: int, folds: int, seed: int, ids=None, n_reps: int = 1) ->
 def last_run_stats() -> dict:
     s = N.RunStats()
     N.check(N.lib().cyc_last_run_stats(C.byref(s)))
-    return {k: getattr(s, k) for k, _ in N.RunStats._fields_}
+    out = {}
+    for k, _ in N.RunStats._fields_:
+        v = getattr(s, k)
+        out[k] = list(v) if hasattr(v, "__len__") else v
+    return out

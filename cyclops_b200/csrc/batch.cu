@@ -317,7 +317,10 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
                     n_grad += (unsigned long long)(act * nn);
                     n_upd += (unsigned long long)(upd * nn);
                     n_steps += act;
-                    n_idx += (unsigned long long)(nn * (1 + (any ? 1 : 0)));
+                    // the column streamed by this group: row ids (not for dense) and
+                    // values (sparse, dense), once for the gradient, again for an update
+                    const long long cb = nn * ((dense ? 0 : 4) + (ind ? 0 : 8));
+                    n_idx += (unsigned long long)(cb * (1 + (any ? 1 : 0)));
                 }
             }
             __syncthreads();
@@ -447,6 +450,60 @@ __global__ void k_scatter_weights(int K, int G, int f, const double* __restrict_
         w[((size_t)grp * K + k) * G + lane] = src ? (T)src[k] : T(1);
 }
 
+// CV grid weights: fit f trains on the rows outside its fold (padding fits: none)
+template <class T>
+__global__ void k_fold_weights(int K, int G, int Fp, const int* __restrict__ fold, const int* __restrict__ fitfold,
+                               T* __restrict__ w) {
+    const long long total = (long long)K * Fp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t % Fp);
+        const int k = (int)(t / Fp);
+        const int ff = fitfold[f];
+        w[((size_t)(f / G) * K + k) * G + (f % G)] = (ff >= -1 && fold[k] != ff) ? T(1) : T(0);
+    }
+}
+
+// per fit: log likelihood under its training weights (getLogLikelihood,
+// ModelSpecifics.hpp:605-650) and, for a CV grid, the predictive log
+// likelihood of its held-out rows (getPredictiveLogLikelihood, :652-690 with
+// logPredLikeContrib, ModelSpecifics.h:1002-1009, 1583-1590, 871-874)
+__global__ void k_batch_final(int model, int K, int S, int G, int F, const double* __restrict__ y,
+                              const double* __restrict__ xb, const double* __restrict__ w,
+                              const double* __restrict__ denom, const double* __restrict__ nw,
+                              const int* __restrict__ strat, const int* __restrict__ fold,
+                              const int* __restrict__ fitfold, const double* __restrict__ llfixed,
+                              double* __restrict__ ll, double* __restrict__ pll) {
+    const int f = blockIdx.x;
+    if (f >= F) return;
+    const int grp = f / G, lane = f % G;
+    const bool grouped = (model == CYC_CLR || model == CYC_CPR);
+    double a = 0.0, p = 0.0;
+    for (int k = threadIdx.x; k < K; k += blockDim.x) {
+        const size_t o = ((size_t)grp * K + k) * G + lane;
+        const double v = xb[o], wt = w[o], yk = y[k];
+        const int yi = (int)yk;
+        a += yi * v * wt;
+        if (model == CYC_LR) a -= wt * log(1.0 + exp(v));
+        if (model == CYC_PR) a -= wt * exp(v);
+        if (fold) {
+            const double h = (fold[k] == fitfold[f]) ? 1.0 : 0.0;
+            if (model == CYC_LR) p += yk * h * (v - log(1.0 + exp(v)));
+            else if (model == CYC_PR) p += (yk * v - exp(v)) * h;
+            else p += yk * h * (v - log(denom[((size_t)grp * S + strat[k]) * G + lane]));
+        }
+    }
+    if (grouped)
+        for (int s = threadIdx.x; s < S; s += blockDim.x) {
+            const size_t o = ((size_t)grp * S + s) * G + lane;
+            a -= nw[o] * log(denom[o]);
+        }
+    block_sum2(a, p);
+    if (threadIdx.x == 0) {
+        ll[f] = a + ((model == CYC_PR || model == CYC_CPR) ? llfixed[f] : 0.0);
+        pll[f] = p;
+    }
+}
+
 // initial linear predictor of every fit from its starting coefficients
 // (zeroXBeta + axpyXBeta in column order, FP64 sums)
 template <class T>
@@ -534,11 +591,7 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
     if (threadIdx.x == 0) out[f] = a;
 }
 
-thread_local cyc_run_stats g_batch_stats{};
-
 }  // namespace
-
-cyc_run_stats& batch_stats() { return g_batch_stats; }
 
 template <class T, int MODEL, int G>
 static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
@@ -555,6 +608,7 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CYC_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_batch<T, MODEL, G>, a));
+    count_launch();
 }
 
 template <class T, int G>
@@ -600,13 +654,26 @@ struct BatchRunner {
         for (int r = 1; r <= C; ++r) rpart[r] = std::max(rpart[r], rpart[r - 1]);
     }
 
+    // weights come either from per-fit host vectors (`specs`) or, for a CV
+    // grid, from fold ids on the device: fit f trains on fold_of_row != fold[f]
+    const int* d_fold = nullptr;
+    DevBuf<int> d_fitfold;
+
+    void set_folds(const int* d_fold_of_row, const std::vector<int>& fit_fold) {
+        d_fold = d_fold_of_row;
+        std::vector<int> ff(Fp, -2);
+        std::copy(fit_fold.begin(), fit_fold.end(), ff.begin());
+        d_fitfold.alloc(Fp);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_fitfold.get(), ff.data(), Fp * sizeof(int), cudaMemcpyHostToDevice, stream));
+    }
+
     void setup(const cyc_prior& prior, const cyc_fit_spec* specs, const std::vector<double>& h_beta,
                const std::vector<double>& h_hdelta) {
         const int K = ds.K, J = ds.J;
         d_rpart.alloc(C + 1);
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_rpart.get(), rpart.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
         d_split.alloc((size_t)J * (C + 1));
-        k_splits<<<(J * (C + 1) + 255) / 256, 256, 0, stream>>>(J, C, ds.d_fmt.get(), ds.d_col_ptr.get(), ds.d_idx.get(),
+        launch(k_splits, (J * (C + 1) + 255) / 256, 256, 0, stream, J, C, ds.d_fmt.get(), ds.d_col_ptr.get(), ds.d_idx.get(),
                                                                   d_rpart.get(), d_split.get());
         CYC_CHECK_LAUNCH();
         std::vector<int> fixb(J, 0), pt(J, prior.prior_type), act(Fp, 0);
@@ -622,16 +689,20 @@ struct BatchRunner {
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_var.get(), var.data(), Fp * sizeof(double), cudaMemcpyHostToDevice, stream));
         // weights
         d_w.alloc((size_t)ngroups * K * G);
-        d_stage.alloc(K);
-        for (int f = 0; f < Fp; ++f) {
+        if (d_fold) {
+            launch(k_fold_weights<T>, grid_for((long long)K * Fp, 1), 256, 0, stream, K, G, Fp, d_fold,
+                   (const int*)d_fitfold.get(), d_w.get());
+        } else {
+          d_stage.alloc(K);
+          for (int f = 0; f < Fp; ++f) {
             const double* src = nullptr;
             if (f < F && specs[f].weights) {
                 CYC_CHECK_CUDA(cudaMemcpyAsync(d_stage.get(), specs[f].weights, K * sizeof(double), cudaMemcpyHostToDevice, stream));
                 src = d_stage.get();
             }
-            k_scatter_weights<T><<<grid_for(K, 4), 256, 0, stream>>>(K, G, f, src, d_w.get());
-            CYC_CHECK_LAUNCH();
+            launch(k_scatter_weights<T>, grid_for(K, 4), 256, 0, stream, K, G, f, src, d_w.get());
             if (src) CYC_CHECK_CUDA(cudaStreamSynchronize(stream));  // staging buffer reuse
+          }
         }
         // coefficients and trust regions
         d_beta.alloc((size_t)Fp * J);
@@ -645,19 +716,19 @@ struct BatchRunner {
         // linear predictors
         ds.ensure_csr();
         d_xb.alloc((size_t)ngroups * K * G);
-        k_init_xb<T><<<grid_for((long long)K * Fp, 1), 256, 0, stream>>>(K, G, Fp, ds.d_row_ptr.get(), ds.d_row_col.get(),
+        launch(k_init_xb<T>, grid_for((long long)K * Fp, 1), 256, 0, stream, K, G, Fp, ds.d_row_ptr.get(), ds.d_row_col.get(),
                                                                          ds.d_row_val.get(), d_beta.get(), J, d_xb.get());
         CYC_CHECK_LAUNCH();
         // fixed gradient terms
         d_xjy.alloc((size_t)Fp * J);
-        k_batch_xjy<T><<<std::min(J, 148 * 8), kBT, 0, stream>>>(J, K, G, ngroups, ds.d_fmt.get(), ds.d_col_ptr.get(),
+        launch(k_batch_xjy<T>, std::min(J, 148 * 8), kBT, 0, stream, J, K, G, ngroups, ds.d_fmt.get(), ds.d_col_ptr.get(),
                                                                  ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(),
                                                                  ds.d_y.get(), d_w.get(), d_xjy.get());
         CYC_CHECK_LAUNCH();
         if (model_grouped(ds.model)) {
             d_nw.alloc((size_t)ngroups * ds.S * G);
             d_denom.alloc((size_t)ngroups * ds.S * G);
-            k_batch_strata<T><<<grid_for((long long)ds.S * Fp, 1), 256, 0, stream>>>(
+            launch(k_batch_strata<T>, grid_for((long long)ds.S * Fp, 1), 256, 0, stream, 
                 ds.S, K, G, ngroups, ds.d_strat_ptr.get(), ds.d_y.get(), d_w.get(), d_xb.get(), d_nw.get(), d_denom.get());
             CYC_CHECK_LAUNCH();
         }
@@ -669,7 +740,7 @@ struct BatchRunner {
                 for (int i = 2; i <= (int)ds.y[k]; ++i) c[k] -= std::log((double)i);
             d_fixedc.alloc(K);
             CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixedc.get(), c.data(), K * sizeof(double), cudaMemcpyHostToDevice, stream));
-            k_batch_llfixed<T><<<Fp, 256, 0, stream>>>(K, G, Fp, d_fixedc.get(), d_w.get(), d_llfixed.get());
+            launch(k_batch_llfixed<T>, Fp, 256, 0, stream, K, G, Fp, d_fixedc.get(), d_w.get(), d_llfixed.get());
             CYC_CHECK_LAUNCH();
             CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
         }
@@ -702,6 +773,23 @@ struct BatchRunner {
         CYC_CHECK_LAUNCH();
     }
 
+    // log likelihood (and held-out predictive log likelihood for CV) per fit
+    void finalize(std::vector<double>& ll, std::vector<double>& pll) {
+        DevBuf<double> d_ll, d_pll;
+        d_ll.alloc(Fp);
+        d_pll.alloc(Fp);
+        const bool grouped = model_grouped(ds.model);
+        launch(k_batch_final, Fp, kBT, 0, stream, ds.model, ds.K, ds.S, G, Fp, (const double*)ds.d_y.get(),
+               (const double*)d_xb.get(), (const double*)d_w.get(), grouped ? (const double*)d_denom.get() : nullptr,
+               grouped ? (const double*)d_nw.get() : nullptr, (const int*)ds.d_strat.get(), d_fold,
+               (const int*)d_fitfold.get(), (const double*)d_llfixed.get(), d_ll.get(), d_pll.get());
+        ll.resize(Fp);
+        pll.resize(Fp);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(ll.data(), d_ll.get(), Fp * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(pll.data(), d_pll.get(), Fp * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+    }
+
     void results(std::vector<double>& beta, std::vector<double>& hd, std::vector<int>& iters, std::vector<int>& flags,
                  unsigned long long* counters) {
         const int J = ds.J;
@@ -722,91 +810,154 @@ struct BatchRunner {
 
 using namespace cyc;
 
+namespace {
+
+// The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` /
+// `fit_fold` select the CV-grid weights; otherwise `specs[f].weights`.
+void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F, const cyc_control* ctl,
+               cyc_fit_result* out, const int* d_fold, const std::vector<int>* fit_fold, std::vector<double>* pll) {
+    CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
+                "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
+    CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
+                    ctl->convergence_type == CYC_CONV_LANGE,
+                CYC_ERR_UNSUPPORTED, "batched fits support gradient, mittal and lange convergence");
+    CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL, CYC_ERR_ARGUMENT,
+                "Unknown prior type");
+    for (int i = 0; i < prior->n_exclude; ++i)
+        CYC_REQUIRE(prior->exclude[i] >= 0 && prior->exclude[i] < ds.J, CYC_ERR_ARGUMENT, "exclude index out of range");
+    for (int f = 0; f < F; ++f) {
+        CYC_REQUIRE(out[f].beta, CYC_ERR_ARGUMENT, "null result buffer");
+        CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || specs[f].variance > 0, CYC_ERR_ARGUMENT,
+                    "prior variance must be positive");
+    }
+    CYC_CHECK_CUDA(cudaSetDevice(ds.device));
+    cudaStream_t stream;
+    CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{stream};
+    const int J = ds.J;
+    std::vector<double> beta((size_t)F * J, 0.0), hd((size_t)F * J, ctl->initial_bound);
+    for (int f = 0; f < F; ++f) {
+        if (specs[f].start_beta) std::copy(specs[f].start_beta, specs[f].start_beta + J, beta.begin() + (size_t)f * J);
+        if (ds.has_offset) beta[(size_t)f * J] = 1.0;
+    }
+    const int G = F >= 4 ? 8 : 1;
+    std::vector<int> iters, flags;
+    unsigned long long ctr[4] = {0, 0, 0, 0};
+    cyc_run_stats st{};
+    // algorithmic bytes of one phase: the columns each group streams, the
+    // (xb, weight) pair of every active fit per gradient entry, the xb
+    // read + write per updated entry, and the convergence passes over
+    // (xb, weight) per fit plus y once per group
+    auto account = [&](int phase, float ms, const std::vector<int>& it, int s) {
+        const double K = ds.K;
+        double conv = 0.0;
+        for (int f = 0; f < F; ++f) conv += (it[f] + 1) * K * 2.0 * s;
+        for (int g0 = 0; g0 < F; g0 += G) {
+            int mx = 0;
+            for (int f = g0; f < std::min(F, g0 + G); ++f) mx = std::max(mx, it[f]);
+            conv += (mx + 1) * K * 8.0;
+        }
+        const double bytes = (double)ctr[3] + ((double)ctr[0] + (double)ctr[1]) * 2.0 * s + conv;
+        st.phase_ms[phase] = ms;
+        st.phase_bytes[phase] = bytes;
+        st.phase_state_bytes[phase] = s;
+        st.kernel_ms += ms;
+        st.algorithmic_bytes += bytes;
+        st.gradient_entries += (double)ctr[0];
+        st.update_entries += (double)ctr[1];
+        st.coordinate_steps += (double)ctr[2];
+        st.index_entries += (double)ctr[3];
+        for (int f = 0; f < F; ++f) st.cycles += it[f];
+        st.launches += 1;
+        st.phases = phase + 1;
+    };
+    int phase = 0;
+    if (ctl->precision == CYC_MIXED) {
+        // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
+        BatchRunner<float> r32(ds, stream, F, G);
+        if (d_fold) r32.set_folds(d_fold, *fit_fold);
+        r32.setup(*prior, specs, beta, hd);
+        float ms = 0.f;
+        r32.run(*ctl, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
+        r32.results(beta, hd, iters, flags, ctr);
+        account(phase++, ms, iters, (int)sizeof(float));
+        // the FP64 phase restarts the trust regions (resetBounds, :943)
+        std::fill(hd.begin(), hd.end(), ctl->initial_bound);
+    }
+    BatchRunner<double> r64(ds, stream, F, G);
+    if (d_fold) r64.set_folds(d_fold, *fit_fold);
+    r64.setup(*prior, specs, beta, hd);
+    float ms = 0.f;
+    r64.run(*ctl, ctl->tolerance, &ms);
+    std::vector<int> it64;
+    r64.results(beta, hd, it64, flags, ctr);
+    account(phase, ms, it64, (int)sizeof(double));
+    std::vector<double> ll, p;
+    r64.finalize(ll, p);
+    std::vector<int> pt(J, prior->prior_type);
+    for (int i = 0; i < prior->n_exclude; ++i) pt[prior->exclude[i]] = CYC_PRIOR_NONE;
+    for (int f = 0; f < F; ++f) {
+        std::copy(beta.begin() + (size_t)f * J, beta.begin() + (size_t)(f + 1) * J, out[f].beta);
+        out[f].iterations = it64[f];
+        out[f].return_flag = flags[f];
+        out[f].log_likelihood = ll[f];
+        double lp = 0.0;
+        for (int j = 0; j < J; ++j) lp += log_density(pt[j], specs[f].variance, out[f].beta[j]);
+        out[f].log_prior = lp;
+    }
+    if (pll) pll->assign(p.begin(), p.begin() + F);
+    set_last_stats(st);
+}
+
+}  // namespace
+
 extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
                              const cyc_control* ctl, cyc_fit_result* out) {
     return guarded([&] {
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
+        run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, nullptr, nullptr);
+    });
+}
+
+extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const int* fold_of_row, int n_folds,
+                               const double* variances, int n_var, const cyc_control* ctl, cyc_fit_result* out,
+                               double* pred_loglik, double* grid_mean) {
+    return guarded([&] {
+        CYC_REQUIRE(dsh && prior && fold_of_row && variances && ctl && out && n_folds > 1 && n_var > 0,
+                    CYC_ERR_ARGUMENT, "null argument");
         Dataset& ds = dsh->ds;
-        CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
-                    "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
-        CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
-                        ctl->convergence_type == CYC_CONV_LANGE,
-                    CYC_ERR_UNSUPPORTED, "batched fits support gradient, mittal and lange convergence");
-        CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL, CYC_ERR_ARGUMENT,
-                    "Unknown prior type");
-        for (int i = 0; i < prior->n_exclude; ++i)
-            CYC_REQUIRE(prior->exclude[i] >= 0 && prior->exclude[i] < ds.J, CYC_ERR_ARGUMENT, "exclude index out of range");
-        for (int f = 0; f < F; ++f) {
-            CYC_REQUIRE(out[f].beta, CYC_ERR_ARGUMENT, "null result buffer");
-            CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || specs[f].variance > 0, CYC_ERR_ARGUMENT,
-                        "prior variance must be positive");
-        }
+        for (int k = 0; k < ds.K; ++k)
+            CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
         CYC_CHECK_CUDA(cudaSetDevice(ds.device));
-        cudaStream_t stream;
-        CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{stream};
-        const int J = ds.J;
-        std::vector<double> beta((size_t)F * J, 0.0), hd((size_t)F * J, ctl->initial_bound);
-        for (int f = 0; f < F; ++f) {
-            if (specs[f].start_beta) std::copy(specs[f].start_beta, specs[f].start_beta + J, beta.begin() + (size_t)f * J);
-            if (ds.has_offset) beta[(size_t)f * J] = 1.0;
+        const int F = n_folds * n_var;
+        std::vector<cyc_fit_spec> specs(F);
+        std::vector<int> fit_fold(F);
+        for (int i = 0; i < F; ++i) {
+            specs[i].weights = nullptr;
+            specs[i].variance = variances[i / n_folds];
+            specs[i].start_beta = nullptr;
+            fit_fold[i] = i % n_folds;
         }
-        const int G = F >= 4 ? 8 : 1;
-        std::vector<int> iters, flags;
-        unsigned long long ctr[4] = {0, 0, 0, 0};
-        float ms_total = 0.f;
-        double grad = 0, upd = 0, steps = 0, idx = 0;
-        int launches = 0;
-        int state_bytes = 8;
-        if (ctl->precision == CYC_MIXED) {
-            // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
-            BatchRunner<float> r32(ds, stream, F, G);
-            r32.setup(*prior, specs, beta, hd);
-            float ms = 0.f;
-            cyc_control c32 = *ctl;
-            r32.run(c32, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
-            r32.results(beta, hd, iters, flags, ctr);
-            ms_total += ms;
-            grad += ctr[0]; upd += ctr[1]; steps += ctr[2]; idx += ctr[3];
-            launches++;
-            state_bytes = 4;
-            // the FP64 phase restarts the trust regions (resetBounds, :943)
-            std::fill(hd.begin(), hd.end(), ctl->initial_bound);
-        }
-        BatchRunner<double> r64(ds, stream, F, G);
-        r64.setup(*prior, specs, beta, hd);
-        float ms = 0.f;
-        r64.run(*ctl, ctl->tolerance, &ms);
-        std::vector<int> it64;
-        r64.results(beta, hd, it64, flags, ctr);
-        ms_total += ms;
-        grad += ctr[0]; upd += ctr[1]; steps += ctr[2]; idx += ctr[3];
-        launches++;
-        // log likelihood and prior of every result through the FP64 engine
-        Engine eng(&ds);
-        for (int f = 0; f < F; ++f) {
-            std::copy(beta.begin() + (size_t)f * J, beta.begin() + (size_t)(f + 1) * J, out[f].beta);
-            out[f].iterations = it64[f];
-            out[f].return_flag = flags[f];
-            eng.set_weights(specs[f].weights, specs[f].weights != nullptr);
-            eng.fixed_terms_ll(true);
-            eng.compute_xbeta(out[f].beta);
-            eng.remaining_statistics(true);
-            out[f].log_likelihood = eng.log_likelihood(true);
-            double lp = 0.0;
-            std::vector<int> pt(J, prior->prior_type);
-            for (int i = 0; i < prior->n_exclude; ++i) pt[prior->exclude[i]] = CYC_PRIOR_NONE;
-            for (int j = 0; j < J; ++j) lp += log_density(pt[j], specs[f].variance, out[f].beta[j]);
-            out[f].log_prior = lp;
-        }
-        cyc_run_stats& st = batch_stats();
-        st = cyc_run_stats{};
-        st.kernel_ms = ms_total;
-        st.gradient_entries = grad;
-        st.update_entries = upd;
-        st.coordinate_steps = steps;
-        st.index_entries = idx;
-        st.launches = launches;
-        st.state_bytes = state_bytes;
+        DevBuf<int> d_fold;
+        d_fold.alloc(ds.K);
+        CYC_CHECK_CUDA(cudaMemcpy(d_fold.get(), fold_of_row, ds.K * sizeof(int), cudaMemcpyHostToDevice));
+        std::vector<double> pll;
+        run_batch(ds, prior, specs.data(), F, ctl, out, d_fold.get(), &fit_fold, &pll);
+        // AbstractCrossValidationDriver: NaN for fits that did not converge;
+        // the grid point's estimate is the mean over folds ignoring NaN
+        // (computePointEstimate, AbstractCrossValidationDriver.cpp:252-264)
+        for (int i = 0; i < F; ++i)
+            if (out[i].return_flag != CYC_SUCCESS) pll[i] = std::nan("");
+        if (pred_loglik) std::copy(pll.begin(), pll.end(), pred_loglik);
+        if (grid_mean)
+            for (int v = 0; v < n_var; ++v) {
+                double tot = 0.0;
+                int cnt = 0;
+                for (int f = 0; f < n_folds; ++f) {
+                    const double x = pll[v * n_folds + f];
+                    if (x == x) { tot += x; ++cnt; }
+                }
+                grid_mean[v] = tot / cnt;
+            }
     });
 }

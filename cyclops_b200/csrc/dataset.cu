@@ -20,11 +20,15 @@
 #include <cstring>
 #include <memory>
 #include <mutex>
+#include <atomic>
 
 namespace cyc {
 
 static thread_local std::string g_last_error;
 void set_error(const std::string& msg) { g_last_error = msg; }
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 size_t Dataset::device_bytes() const {
     return d_fmt.bytes() + d_col_ptr.bytes() + d_val_ptr.bytes() + d_idx.bytes() + d_val.bytes() +
@@ -81,6 +85,7 @@ using namespace cyc;
 
 extern "C" const char* cyc_last_error(void) { return g_last_error.c_str(); }
 extern "C" int cyc_version(void) { return 1; }
+extern "C" long long cyc_launch_count(void) { return g_launches.load(); }
 
 extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_dataset** out) {
     return guarded([&] {

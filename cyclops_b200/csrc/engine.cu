@@ -181,16 +181,16 @@ void Engine::set_weights(const double* w, bool use_cv) {
     if (wp) {
         weights_buf.alloc(K);
         CYC_CHECK_CUDA(cudaMemcpyAsync(weights_buf.get(), wp, K * sizeof(double), cudaMemcpyHostToDevice, stream));
-        k_set_kw<<<grid_for(K, 1), kThreads, 0, stream>>>(K, weights_buf.get(), kw.get());
+        launch(k_set_kw, grid_for(K, 1), kThreads, 0, stream, K, weights_buf.get(), kw.get());
         sync();  // the caller's host buffer may go away after return
     } else {
-        k_set_kw<<<grid_for(K, 1), kThreads, 0, stream>>>(K, nullptr, kw.get());
+        launch(k_set_kw, grid_for(K, 1), kThreads, 0, stream, K, nullptr, kw.get());
     }
     CYC_CHECK_CUDA(cudaMemsetAsync(nw.get(), 0, (N + 1) * sizeof(double), stream));
     if (model_independent(model)) {
-        k_nw_independent<<<grid_for(K, 1), kThreads, 0, stream>>>(K, kw.get(), nw.get());
+        launch(k_nw_independent, grid_for(K, 1), kThreads, 0, stream, K, kw.get(), nw.get());
     } else {
-        k_nw_grouped<<<grid_for(N, 1), kThreads, 0, stream>>>(N, group_rows(), ds->d_y.get(), kw.get(), nw.get());
+        launch(k_nw_grouped, grid_for(N, 1), kThreads, 0, stream, N, group_rows(), ds->d_y.get(), kw.get(), nw.get());
     }
     CYC_CHECK_LAUNCH();
     stats_known = false;
@@ -200,14 +200,14 @@ void Engine::fixed_terms_ll(bool use_cv) {
     if (!has_fixed_ll(model)) return;
     const int K = ds->K;
     const int blocks = grid_for(K, 4);
-    k_fixed_ll<<<blocks, kThreads, 0, stream>>>(K, ds->d_y.get(), kw.get(), use_cv && use_w,
+    launch(k_fixed_ll, blocks, kThreads, 0, stream, K, ds->d_y.get(), kw.get(), use_cv && use_w,
                                                 partial.get(), ticket.get(), ll_fixed.get());
     CYC_CHECK_LAUNCH();
 }
 
 void Engine::fixed_terms_gh(bool use_cv) {
     const int J = ds->J;
-    k_xjy<<<std::min(J, 148 * 16), 128, 0, stream>>>(J, ds->d_fmt.get(), ds->d_col_ptr.get(),
+    launch(k_xjy, std::min(J, 148 * 16), 128, 0, stream, J, ds->d_fmt.get(), ds->d_col_ptr.get(),
                                                      ds->d_val_ptr.get(), ds->d_idx.get(), ds->d_val.get(),
                                                      ds->K, ds->d_y.get(), kw.get(), use_cv && use_w, xjy.get());
     CYC_CHECK_LAUNCH();
@@ -221,7 +221,7 @@ void Engine::zero_xbeta() {
 void Engine::axpy_xbeta(double beta, int j) {
     if (beta == 0.0) return;
     ColView c = ds->view(j);
-    k_axpy<<<grid_for(c.n, 4), kThreads, 0, stream>>>(c, beta, xb.get());
+    launch(k_axpy, grid_for(c.n, 4), kThreads, 0, stream, c, beta, xb.get());
     CYC_CHECK_LAUNCH();
     stats_known = false;
 }
@@ -241,7 +241,7 @@ void Engine::compute_xbeta(const double* beta_host) {
 void Engine::compute_xbeta_device(const double* d_beta) {
     ds->ensure_csr();
     const int K = ds->K;
-    k_xbeta_rows<<<grid_for(K, 1), kThreads, 0, stream>>>(K, ds->d_row_ptr.get(), ds->d_row_col.get(),
+    launch(k_xbeta_rows, grid_for(K, 1), kThreads, 0, stream, K, ds->d_row_ptr.get(), ds->d_row_col.get(),
                                                           ds->d_row_val.get(), d_beta, xb.get());
     CYC_CHECK_LAUNCH();
     stats_known = false;
@@ -258,9 +258,9 @@ void Engine::cox_rescan(int lo) {
 void Engine::remaining_statistics(bool use_weights) {
     const int K = ds->K;
     if (model_independent(model)) {
-        k_rs_independent<<<grid_for(K, 1), kThreads, 0, stream>>>(K, model, xb.get(), exb.get(), denom.get());
+        launch(k_rs_independent, grid_for(K, 1), kThreads, 0, stream, K, model, xb.get(), exb.get(), denom.get());
     } else {
-        k_rs_grouped<<<grid_for(N, 1), kThreads, 0, stream>>>(
+        launch(k_rs_grouped, grid_for(N, 1), kThreads, 0, stream, 
             N, group_rows(), xb.get(), kw.get(), model_cumulative(model) && use_weights && use_w,
             exb.get(), denom.get());
         if (model_cumulative(model)) cox_rescan(0);
@@ -275,10 +275,10 @@ void Engine::numerator_for_gradient(int j, bool use_weights) {
     if (c.n == 0) return;
     const int blocks = grid_for(c.n, 4);
     if (c.indicator())
-        k_cox_numerator<true><<<blocks, kThreads, 0, stream>>>(c, group.get(), exb.get(), kw.get(),
+        launch(k_cox_numerator<true>, blocks, kThreads, 0, stream, c, group.get(), exb.get(), kw.get(),
                                                               use_weights && use_w, numer.get(), numer2.get());
     else
-        k_cox_numerator<false><<<blocks, kThreads, 0, stream>>>(c, group.get(), exb.get(), kw.get(),
+        launch(k_cox_numerator<false>, blocks, kThreads, 0, stream, c, group.get(), exb.get(), kw.get(),
                                                                use_weights && use_w, numer.get(), numer2.get());
     CYC_CHECK_LAUNCH();
 }
@@ -295,29 +295,29 @@ void Engine::launch_gradient(int j, bool use_weights, double* out) {
     if (model_independent(model)) {
         if (model == CYC_LR) {
             if (c.indicator())
-                k_gh_independent<CYC_LR, true><<<blocks, kThreads, 0, stream>>>(c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
+                launch(k_gh_independent<CYC_LR, true>, blocks, kThreads, 0, stream, c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
             else
-                k_gh_independent<CYC_LR, false><<<blocks, kThreads, 0, stream>>>(c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
+                launch(k_gh_independent<CYC_LR, false>, blocks, kThreads, 0, stream, c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
         } else {
             if (c.indicator())
-                k_gh_independent<CYC_PR, true><<<blocks, kThreads, 0, stream>>>(c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
+                launch(k_gh_independent<CYC_PR, true>, blocks, kThreads, 0, stream, c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
             else
-                k_gh_independent<CYC_PR, false><<<blocks, kThreads, 0, stream>>>(c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
+                launch(k_gh_independent<CYC_PR, false>, blocks, kThreads, 0, stream, c, exb.get(), denom.get(), nw.get(), uw, xjy.get(), j, partial.get(), ticket.get(), out);
         }
     } else if (model_grouped(model)) {
         if (c.indicator())
-            k_gh_grouped<true><<<blocks, kThreads, 0, stream>>>(c, groups(), exb.get(), denom.get(), nw.get(), xjy.get(), j, partial.get(), ticket.get(), out);
+            launch(k_gh_grouped<true>, blocks, kThreads, 0, stream, c, groups(), exb.get(), denom.get(), nw.get(), xjy.get(), j, partial.get(), ticket.get(), out);
         else
-            k_gh_grouped<false><<<blocks, kThreads, 0, stream>>>(c, groups(), exb.get(), denom.get(), nw.get(), xjy.get(), j, partial.get(), ticket.get(), out);
+            launch(k_gh_grouped<false>, blocks, kThreads, 0, stream, c, groups(), exb.get(), denom.get(), nw.get(), xjy.get(), j, partial.get(), ticket.get(), out);
     } else {
         const long long b = h_glist_ptr[j], e = h_glist_ptr[j + 1];
         const int L = (int)(e - b);
         if (L == 0) {
-            k_copy_neg_xjy<<<1, 1, 0, stream>>>(xjy.get(), j, out);
+            launch(k_copy_neg_xjy, 1, 1, 0, stream, xjy.get(), j, out);
         } else if (c.indicator()) {
-            k_cox_gradient<true><<<1, kThreads, 0, stream>>>(glist.get() + b, L, gstart.get(), gend.get(), numer.get(), numer2.get(), P1h.get(), P1l.get(), P2h.get(), P2l.get(), xjy.get(), j, out);
+            launch(k_cox_gradient<true>, 1, kThreads, 0, stream, glist.get() + b, L, gstart.get(), gend.get(), numer.get(), numer2.get(), P1h.get(), P1l.get(), P2h.get(), P2l.get(), xjy.get(), j, out);
         } else {
-            k_cox_gradient<false><<<1, kThreads, 0, stream>>>(glist.get() + b, L, gstart.get(), gend.get(), numer.get(), numer2.get(), P1h.get(), P1l.get(), P2h.get(), P2l.get(), xjy.get(), j, out);
+            launch(k_cox_gradient<false>, 1, kThreads, 0, stream, glist.get() + b, L, gstart.get(), gend.get(), numer.get(), numer2.get(), P1h.get(), P1l.get(), P2h.get(), P2l.get(), xjy.get(), j, out);
         }
     }
     CYC_CHECK_LAUNCH();
@@ -339,9 +339,9 @@ void Engine::launch_update(int j, bool use_weights, const double* d_delta, doubl
     if (c.n == 0) return;
     const int blocks = grid_for(c.n, 4);
     if (model_independent(model)) {
-        k_update_independent<<<blocks, kThreads, 0, stream>>>(c, d_delta, delta, xb.get(), exb.get(), denom.get());
+        launch(k_update_independent, blocks, kThreads, 0, stream, c, d_delta, delta, xb.get(), exb.get(), denom.get());
     } else {
-        k_update_grouped<<<blocks, kThreads, 0, stream>>>(c, d_delta, delta, groups(), kw.get(),
+        launch(k_update_grouped, blocks, kThreads, 0, stream, c, d_delta, delta, groups(), kw.get(),
                                                           model_cumulative(model) && use_weights && use_w,
                                                           xb.get(), exb.get(), denom.get());
         if (model_cumulative(model)) cox_rescan_gated(d_delta, first_group(j));
@@ -357,13 +357,13 @@ void Engine::cox_rescan_gated(const double* gate, int lo) {
     if (lo >= N) return;
     const int hi = N;
     const int ntiles = (hi - lo + kScanTile - 1) / kScanTile;
-    k_scanD_tiles<<<ntiles, kThreads, 0, stream>>>(gate, lo, hi, gstart.get(), denom.get(), aggD.get());
-    k_carryD<<<1, kThreads, 0, stream>>>(gate, ntiles, aggD.get(), lo, gstart.get(), D.get());
-    k_scanD_write<<<ntiles, kThreads, 0, stream>>>(gate, lo, hi, gstart.get(), denom.get(), nw.get(),
+    launch(k_scanD_tiles, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), aggD.get());
+    launch(k_carryD, 1, kThreads, 0, stream, gate, ntiles, aggD.get(), lo, gstart.get(), D.get());
+    launch(k_scanD_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), nw.get(),
                                                    aggD.get(), D.get(), aggP.get());
-    k_carryP<<<1, kThreads, 0, stream>>>(gate, ntiles, aggP.get(), lo, gstart.get(), P1h.get(), P1l.get(),
+    launch(k_carryP, 1, kThreads, 0, stream, gate, ntiles, aggP.get(), lo, gstart.get(), P1h.get(), P1l.get(),
                                          P2h.get(), P2l.get());
-    k_scanP_write<<<ntiles, kThreads, 0, stream>>>(gate, lo, hi, gstart.get(), D.get(), nw.get(), aggP.get(),
+    launch(k_scanP_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), D.get(), nw.get(), aggP.get(),
                                                    P1h.get(), P1l.get(), P2h.get(), P2l.get());
     CYC_CHECK_LAUNCH();
 }
@@ -377,7 +377,7 @@ void Engine::launch_loglik(bool use_cv, double* out) {
     const int K = ds->K;
     const int M = std::max(K, N);
     const double* den = model_cumulative(model) ? D.get() : denom.get();
-    k_loglik<<<grid_for(M, 4), kThreads, 0, stream>>>(model, K, N, ds->d_y.get(), xb.get(), kw.get(),
+    launch(k_loglik, grid_for(M, 4), kThreads, 0, stream, model, K, N, ds->d_y.get(), xb.get(), kw.get(),
                                                       use_cv && use_w, nw.get(), den, ll_fixed.get(),
                                                       partial.get(), ticket.get(), out);
     CYC_CHECK_LAUNCH();
@@ -392,7 +392,7 @@ double Engine::log_likelihood(bool use_cv) {
 
 void Engine::launch_gradient_objective(bool use_cv, double* out) {
     const int K = ds->K;
-    k_grad_objective<<<grid_for(K, 4), kThreads, 0, stream>>>(K, ds->d_y.get(), xb.get(), kw.get(),
+    launch(k_grad_objective, grid_for(K, 4), kThreads, 0, stream, K, ds->d_y.get(), xb.get(), kw.get(),
                                                               use_cv && use_w, partial.get(), ticket.get(), out);
     CYC_CHECK_LAUNCH();
 }
@@ -418,7 +418,7 @@ double Engine::predictive_log_likelihood(const double* w) {
     weights_buf.alloc(K);
     CYC_CHECK_CUDA(cudaMemcpyAsync(weights_buf.get(), w, K * sizeof(double), cudaMemcpyHostToDevice, stream));
     const double* den = model_cumulative(model) ? D.get() : denom.get();
-    k_pred_loglik<<<grid_for(K, 4), kThreads, 0, stream>>>(model, K, ds->d_y.get(), xb.get(), weights_buf.get(),
+    launch(k_pred_loglik, grid_for(K, 4), kThreads, 0, stream, model, K, ds->d_y.get(), xb.get(), weights_buf.get(),
                                                            groups(), den, partial.get(), ticket.get(),
                                                            result.get());
     CYC_CHECK_LAUNCH();
@@ -444,7 +444,7 @@ void Engine::predictive_estimates(double* y, const double* w) {
         CYC_CHECK_CUDA(cudaMemcpyAsync(weights_buf.get(), w, K * sizeof(double), cudaMemcpyHostToDevice, stream));
         dw = weights_buf.get();
     }
-    k_pred_estimates<<<grid_for(K, 1), kThreads, 0, stream>>>(model, K, xb.get(), dw, out.get());
+    launch(k_pred_estimates, grid_for(K, 1), kThreads, 0, stream, model, K, xb.get(), dw, out.get());
     CYC_CHECK_LAUNCH();
     CYC_CHECK_CUDA(cudaMemcpyAsync(y, out.get(), K * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();

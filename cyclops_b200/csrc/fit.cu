@@ -17,9 +17,9 @@
 
 namespace cyc {
 
-namespace {
+static thread_local cyc_run_stats g_stats{};
 
-thread_local cyc_run_stats g_stats{};
+namespace {
 
 __global__ void k_step(int j, const double* __restrict__ gh, StepState st) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
@@ -147,7 +147,7 @@ struct FitRunner {
     void launch_coordinate(int j) {
         e.numerator_for_gradient(j, true);
         e.launch_gradient(j, true, gh.get());
-        k_step<<<1, 32, 0, e.stream>>>(j, gh.get(), step_state());
+        launch(k_step, 1, 32, 0, e.stream, j, gh.get(), step_state());
         CYC_CHECK_LAUNCH();
         e.launch_update(j, true, delta.get(), 0.0);
     }
@@ -175,7 +175,7 @@ struct FitRunner {
             e.launch_loglik(true, obj.get());
         } else if (conv == CYC_CONV_LANGE) {
             e.launch_loglik(true, obj.get());
-            k_add_logprior<<<1, kThreads, 0, e.stream>>>(J, beta.get(), ptype.get(), variance, obj.get(), obj.get());
+            launch(k_add_logprior, 1, kThreads, 0, e.stream, J, beta.get(), ptype.get(), variance, obj.get(), obj.get());
         } else if (conv == CYC_CONV_ONE_STEP) {
             CYC_CHECK_CUDA(cudaMemsetAsync(obj.get(), 0, sizeof(double), e.stream));
         }
@@ -192,11 +192,11 @@ struct FitRunner {
         const int K = e.ds->K;
         if (conv < CYC_CONV_ZHANG_OLES) {
             launch_objective(conv);
-            k_copy<<<1, 1, 0, e.stream>>>(1, obj.get(), last.get());
+            launch(k_copy, 1, 1, 0, e.stream, 1, obj.get(), last.get());
             CYC_CHECK_LAUNCH();
         } else {
             e.xb_save.alloc(K);
-            k_copy<<<grid_for(K, 1), kThreads, 0, e.stream>>>(K, e.xb.get(), e.xb_save.get());
+            launch(k_copy, grid_for(K, 1), kThreads, 0, e.stream, K, e.xb.get(), e.xb_save.get());
         }
         e.sync();
         int it = 0;
@@ -205,13 +205,13 @@ struct FitRunner {
             it++;
             if (conv < CYC_CONV_ZHANG_OLES) {
                 launch_objective(conv);
-                k_check<<<1, 32, 0, e.stream>>>(obj.get(), last.get(), ctl.tolerance, it, ctl.max_iterations, 0, flags.get());
+                launch(k_check, 1, 32, 0, e.stream, obj.get(), last.get(), ctl.tolerance, it, ctl.max_iterations, 0, flags.get());
                 CYC_CHECK_LAUNCH();
             } else {
-                k_zhang_oles<<<grid_for(K, 4), kThreads, 0, e.stream>>>(K, e.xb.get(), e.xb_save.get(), e.kw.get(),
+                launch(k_zhang_oles, grid_for(K, 4), kThreads, 0, e.stream, K, e.xb.get(), e.xb_save.get(), e.kw.get(),
                                                                         e.use_w, e.partial.get(), e.ticket.get(), obj.get());
-                k_copy<<<grid_for(K, 1), kThreads, 0, e.stream>>>(K, e.xb.get(), e.xb_save.get());
-                k_check<<<1, 32, 0, e.stream>>>(obj.get(), last.get(), ctl.tolerance, it, ctl.max_iterations, 1, flags.get());
+                launch(k_copy, grid_for(K, 1), kThreads, 0, e.stream, K, e.xb.get(), e.xb_save.get());
+                launch(k_check, 1, 32, 0, e.stream, obj.get(), last.get(), ctl.tolerance, it, ctl.max_iterations, 1, flags.get());
             }
             CYC_CHECK_CUDA(cudaMemcpyAsync(h_flags, flags.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, e.stream));
             e.sync();
@@ -250,7 +250,7 @@ struct FitRunner {
         // results
         CYC_CHECK_CUDA(cudaMemcpyAsync(out->beta, beta.get(), J * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
         e.launch_loglik(true, obj.get());
-        k_add_logprior<<<1, kThreads, 0, e.stream>>>(J, beta.get(), ptype.get(), variance, nullptr, last.get());
+        launch(k_add_logprior, 1, kThreads, 0, e.stream, J, beta.get(), ptype.get(), variance, nullptr, last.get());
         double h2[2];
         CYC_CHECK_CUDA(cudaMemcpyAsync(&h2[0], obj.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(&h2[1], last.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
@@ -263,15 +263,122 @@ struct FitRunner {
         out->return_flag = flag;
         float ms = 0.f;
         CYC_CHECK_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-        g_stats = cyc_run_stats{};
-        g_stats.kernel_ms = ms;
-        g_stats.launches = 0;
-        g_stats.state_bytes = 8;
+        cyc_run_stats st{};
+        st.kernel_ms = ms;
+        st.coordinate_steps = (double)iters * J;
+        st.cycles = iters;
+        st.phases = 1;
+        st.phase_ms[0] = ms;
+        st.phase_state_bytes[0] = 8;
+        set_last_stats(st);
         (void)nup;
     }
 };
 
-cyc_run_stats& fit_stats() { return g_stats; }
+void set_last_stats(const cyc_run_stats& s) { g_stats = s; }
+
+// CyclicCoordinateDescent::findMode / update with the host driving the
+// engine one call at a time (src/cyclops/CyclicCoordinateDescent.cpp:586-615,
+// 909-1216): every coordinate reads (gradient, Hessian) back, takes the
+// step on the host and launches the update.  The plain FP64 single-fit GPU
+// CCD, kept as the measured baseline of the device-resident solvers.
+static void host_loop_fit(Engine& e, const cyc_prior& prior, const cyc_fit_spec& spec, const cyc_control& ctl,
+                          cyc_fit_result* out) {
+    const int J = e.ds->J;
+    const int K = e.ds->K;
+    std::vector<int> fixb(J, 0), pt(J, prior.prior_type);
+    for (int i = 0; i < prior.n_exclude; ++i) {
+        CYC_REQUIRE(prior.exclude[i] >= 0 && prior.exclude[i] < J, CYC_ERR_ARGUMENT, "exclude index out of range");
+        pt[prior.exclude[i]] = CYC_PRIOR_NONE;
+    }
+    std::vector<double> beta(J, 0.0);
+    if (spec.start_beta) std::copy(spec.start_beta, spec.start_beta + J, beta.begin());
+    if (e.ds->has_offset) { fixb[0] = 1; beta[0] = 1.0; }
+    const int conv = ctl.convergence_type;
+    CYC_REQUIRE(conv >= CYC_CONV_GRADIENT && conv <= CYC_CONV_ZHANG_OLES, CYC_ERR_ARGUMENT,
+                "Unknown convergence criterion");
+    auto log_prior = [&]() {
+        double s = 0.0;
+        for (int j = 0; j < J; ++j) s += log_density(pt[j], spec.variance, beta[j]);
+        return s;
+    };
+    auto objective = [&]() {
+        if (conv == CYC_CONV_GRADIENT) return e.gradient_objective(true);
+        if (conv == CYC_CONV_MITTAL) return e.log_likelihood(true);
+        if (conv == CYC_CONV_LANGE) return e.log_likelihood(true) + log_prior();
+        return 0.0;
+    };
+    std::vector<double> xb(K), xs(K), kw(K, 1.0);
+    if (spec.weights) std::copy(spec.weights, spec.weights + K, kw.begin());
+    auto zhang_oles = [&]() {
+        e.get_xbeta(xb.data());
+        double d = 0.0, r = 0.0;
+        for (int k = 0; k < K; ++k) {
+            const double w = spec.weights ? kw[k] : 1.0;
+            d += std::fabs(xb[k] - xs[k]) * w;
+            r += std::fabs(xb[k]) * w;
+        }
+        xs = xb;
+        return d / (1.0 + r);
+    };
+    e.fixed_terms_ll(true);
+    e.fixed_terms_gh(true);
+    e.compute_xbeta(beta.data());
+    e.remaining_statistics(true);
+    std::vector<double> hd(J);
+    double bound = ctl.initial_bound;
+    int count = 0, flag = CYC_SUCCESS, it = 0;
+    for (;;) {
+        std::fill(hd.begin(), hd.end(), bound);
+        double last = 0.0;
+        if (conv < CYC_CONV_ZHANG_OLES) last = objective();
+        else e.get_xbeta(xs.data());
+        it = 0;
+        bool done = false;
+        while (!done) {
+            for (int j = 0; j < J; ++j) {
+                if (fixb[j]) continue;
+                double g, h;
+                e.numerator_for_gradient(j, true);
+                e.gradient_hessian(j, true, &g, &h);
+                if (h < 0.0) { g = 0.0; h = 0.0; }
+                double delta = prior_delta(pt[j], spec.variance, beta[j], g, h);
+                delta = apply_bounds(&hd[j], delta);
+                if (delta != 0.0) {
+                    beta[j] += delta;
+                    e.update_xbeta(delta, j, true);
+                }
+            }
+            ++it;
+            double c;
+            bool ill = false;
+            if (conv < CYC_CONV_ZHANG_OLES) {
+                const double o = objective();
+                if (o != o) { c = 0.0; ill = true; }
+                else c = std::fabs(o - last) / (std::fabs(o) + 1.0);
+                last = o;
+            } else {
+                c = zhang_oles();
+            }
+            if (ctl.tolerance > 0 && c < ctl.tolerance) { flag = ill ? CYC_ILLCONDITIONED : CYC_SUCCESS; done = true; }
+            else if (it == ctl.max_iterations) { flag = CYC_MAX_ITERATIONS; done = true; }
+        }
+        ++count;
+        if (flag == CYC_ILLCONDITIONED && count < ctl.max_bound_count) {
+            bound /= 10.0;
+            for (int j = e.ds->has_offset ? 1 : 0; j < J; ++j) beta[j] = 0.0;
+            e.compute_xbeta(beta.data());
+            e.remaining_statistics(true);
+        } else {
+            break;
+        }
+    }
+    std::copy(beta.begin(), beta.end(), out->beta);
+    out->log_likelihood = e.log_likelihood(true);
+    out->log_prior = log_prior();
+    out->iterations = it;
+    out->return_flag = flag;
+}
 
 }  // namespace cyc
 
@@ -293,9 +400,39 @@ extern "C" int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_sp
     });
 }
 
+extern "C" int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                                 const cyc_control* control, cyc_fit_result* out) {
+    return guarded([&] {
+        CYC_REQUIRE(ds && prior && spec && control && out && out->beta, CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
+                    CYC_ERR_ARGUMENT, "Unknown prior type");
+        CYC_CHECK_CUDA(cudaSetDevice(ds->ds.device));
+        Engine eng(&ds->ds);
+        eng.set_weights(spec->weights, spec->weights != nullptr);
+        cudaEvent_t e0, e1;
+        CYC_CHECK_CUDA(cudaEventCreate(&e0));
+        CYC_CHECK_CUDA(cudaEventCreate(&e1));
+        CYC_CHECK_CUDA(cudaEventRecord(e0, eng.stream));
+        host_loop_fit(eng, *prior, *spec, *control, out);
+        CYC_CHECK_CUDA(cudaEventRecord(e1, eng.stream));
+        CYC_CHECK_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cyc_run_stats st{};
+        st.kernel_ms = ms;
+        st.cycles = out->iterations;
+        st.phases = 1;
+        st.phase_ms[0] = ms;
+        st.phase_state_bytes[0] = 8;
+        set_last_stats(st);
+    });
+}
+
 extern "C" int cyc_last_run_stats(cyc_run_stats* out) {
     return guarded([&] {
         CYC_REQUIRE(out, CYC_ERR_ARGUMENT, "null argument");
-        *out = fit_stats();
+        *out = g_stats;
     });
 }

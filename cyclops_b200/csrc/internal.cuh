@@ -32,6 +32,11 @@ struct Error {
         }                                                                               \
     } while (0)
 
+// kernels launched by this library (counted by launch() below)
+void count_launch();
+// statistics reported by cyc_last_run_stats for the calling thread
+void set_last_stats(const cyc_run_stats& s);
+
 // reports a failed (or pending) launch with the call site
 #define CYC_CHECK_LAUNCH()                                                              \
     do {                                                                                \
@@ -45,6 +50,14 @@ struct Error {
     do {                                                                                \
         if (!(cond)) throw ::cyc::Error{(status), (msg)};                               \
     } while (0)
+
+// every kernel of the library is launched through here: counted and checked
+template <class Kern, class... Args>
+inline void launch(Kern kernel, dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args... args) {
+    kernel<<<grid, block, smem, stream>>>(args...);
+    count_launch();
+    CYC_CHECK_LAUNCH();
+}
 
 template <class F>
 int guarded(F&& f) {

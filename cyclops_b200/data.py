@@ -206,8 +206,20 @@ def _bernoulli_csc(rng, K: int, P: int, density: float):
 
 
 def _zipf_column_counts(rng, K: int, P: int, total: int, s: float):
+    """Column sizes proportional to rank^-s, capped at K, scaled so that the
+    capped sizes still add up to `total` (bisection on the scale)."""
     w = np.arange(1, P + 1, dtype=np.float64) ** (-s)
-    n = np.minimum(np.floor(w / w.sum() * total + rng.random(P)).astype(np.int64), K)
+    w /= w.sum()
+    lo, hi = 1.0, 1.0
+    while np.minimum(w * total * hi, K).sum() < total and hi < 1e6:
+        hi *= 2.0
+    for _ in range(60):
+        mid = 0.5 * (lo + hi)
+        if np.minimum(w * total * mid, K).sum() < total:
+            lo = mid
+        else:
+            hi = mid
+    n = np.minimum(np.floor(w * total * hi + rng.random(P)).astype(np.int64), K)
     return n
 
 

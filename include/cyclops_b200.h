@@ -200,6 +200,21 @@ int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
 int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
                   const cyc_control* control, cyc_fit_result* out);
 
+/* Cross-validation grid on the GPU: `n_folds` folds x `n_var` prior
+ * variances = n_folds * n_var fits (fit i = variance i / n_folds, fold
+ * i % n_folds), each trained on the rows whose fold id differs from its fold
+ * (fold_of_row: K ids in 0..n_folds-1, e.g. from cyc_cv_fold_weights) and
+ * scored on the held-out rows with the reference's predictive log likelihood
+ * (ModelSpecifics.hpp:652-690).  The per-fold, per-grid-point loop of
+ * GridSearchCrossValidationDriver / AbstractCrossValidationDriver
+ * (src/cyclops/drivers/GridSearchCrossValidationDriver.cpp:96-140,
+ * AbstractCrossValidationDriver.cpp:131-261) as one batched solve.
+ * `pred_loglik` (F values, NaN where the fit did not converge) and
+ * `grid_mean` (n_var values: mean over folds ignoring NaN) may be NULL. */
+int cyc_cv_grid_fit(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds,
+                    const double* variances, int n_var, const cyc_control* control,
+                    cyc_fit_result* out, double* pred_loglik, double* grid_mean);
+
 /* Cross-validation fold masks, `n_reps * folds` rows of K weights (0 = held
  * out), exactly as CrossValidationSelector draws them
  * (src/cyclops/drivers/CrossValidationSelector.cpp:21-116): by row
@@ -211,15 +226,31 @@ int cyc_cv_fold_weights(int K, const int* ids, int folds, long seed, int by_row,
  * roofline accounting: kernel milliseconds (CUDA events), column entries
  * visited by gradients, entries visited by updates, coordinate steps. */
 typedef struct {
-    double kernel_ms;
+    double kernel_ms;           /* solver kernels, CUDA events */
+    double algorithmic_bytes;   /* unique bytes the algorithm must move (all phases) */
     double gradient_entries;    /* sum over (fit, coordinate) of nnz_j */
     double update_entries;      /* sum over (fit, coordinate) with delta != 0 of nnz_j */
-    double coordinate_steps;
-    double index_entries;       /* column entries read once per coordinate (shared by fits) */
-    int launches;
-    int state_bytes;            /* bytes per (row, fit) state element */
+    double coordinate_steps;    /* (fit, coordinate) steps taken */
+    double index_entries;       /* column entries streamed per fit group */
+    double cycles;              /* sum over fits of CCD cycles */
+    int launches;               /* solver kernel launches */
+    int phases;                 /* 1 (FP64) or 2 (FP32, then FP64 polish) */
+    double phase_ms[2];
+    double phase_bytes[2];
+    int phase_state_bytes[2];   /* bytes per (row, fit) state element of each phase */
 } cyc_run_stats;
 int cyc_last_run_stats(cyc_run_stats* out);
+
+/* Kernels this library has launched in this process (all entry points). */
+long long cyc_launch_count(void);
+
+/* The plain FP64 single-fit GPU CCD: the host runs the coordinate loop and
+ * reads each coordinate's (gradient, Hessian) back, as
+ * CyclicCoordinateDescent does through AbstractModelSpecifics
+ * (src/cyclops/CyclicCoordinateDescent.cpp:1394-1413).  The baseline the
+ * device-resident solvers are measured against. */
+int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                      const cyc_control* control, cyc_fit_result* out);
 
 #ifdef __cplusplus
 }
