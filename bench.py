@@ -145,17 +145,18 @@ def traffic_record(workload_name):
 # CPU legs (reference engine; port if the reference was not built)
 # --------------------------------------------------------------------------
 
-def cpu_fits(data, variances, folds, fit_ids, threads):
+def cpu_fits(data, variances, folds, fit_ids, threads, max_iterations=1000):
     from oracle import oracle as O
     kind = "reference" if O.have_ref() else "port"
     lib = O.ref() if kind == "reference" else O.port()
     excl = [0]
+    ctl = O.make_control(max_iterations=max_iterations)
 
     def one(i):
         v = variances[i // N_FOLDS]
         f = i % N_FOLDS
         w = (folds != f).astype(np.float64)
-        return lib.fit(data, D.PRIOR_LAPLACE, float(v), control=None, exclude=excl, weights=w)
+        return lib.fit(data, D.PRIOR_LAPLACE, float(v), control=ctl, exclude=excl, weights=w)
 
     t0 = time.perf_counter()
     with cf.ThreadPoolExecutor(max_workers=threads) as ex:
@@ -177,13 +178,20 @@ def run_reference(args):
     folds = fold_ids(data.K, FOLD_SEED)
     threads = os.cpu_count() or 1
     ids = sample_ids(threads)
+    # warm-up steps run two cycles per fit (page-in, thread start-up); timed
+    # steps run every sampled fit to convergence, one fit per host thread,
+    # and stop early once 150 s are spent (steps reports the steps done)
     for _ in range(args.warmup):
-        cpu_fits(data, variances, folds, ids, threads)
-    total, n, kind = 0.0, 0, None
+        cpu_fits(data, variances, folds, ids, threads, max_iterations=2)
+    total, n, kind, done = 0.0, 0, None, 0
     for _ in range(args.steps):
         res, dt, kind = cpu_fits(data, variances, folds, ids, threads)
         total += dt
         n += len(ids)
+        done += 1
+        if total > 150.0:
+            break
+    args.steps = done
     value = n / total
     line = {
         "impl": "reference", "metric": "cv_fits_per_second", "value": value, "unit": "fits/s",
