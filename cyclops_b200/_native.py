@@ -97,6 +97,8 @@ _SIGS = {
     "cyc_last_run_stats": [C.POINTER(RunStats)],
     "cyc_cv_fold_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_int, C.c_int, C.c_void_p],
     "cyc_launch_count": [],
+    "cyc_gradient_hessian_noalloc": [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p],
     "cyc_cv_grid_fit": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                         C.POINTER(Control), C.POINTER(FitResult), C.c_void_p, C.c_void_p],
     "cyc_fit_host_loop": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control),

@@ -252,6 +252,30 @@ long long cyc_launch_count(void);
 int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
                       const cyc_control* control, cyc_fit_result* out);
 
+/* ---- allocation-free entry point ----------------------------------------- */
+
+/* No counterpart in the reference.  For callers that cannot let this
+ * library allocate device memory (they own the GPU's memory through their
+ * own pool or caching allocator, or cannot afford the device-wide
+ * synchronisation an allocation implies): the gradient and Hessian of one
+ * lr / pr column, as cyc_engine_compute_gradient_and_hessian computes them,
+ * with every buffer supplied by the caller as a device pointer and the
+ * reduction scratch taken from a fixed 64 KiB area compiled into the library
+ * (held on every GPU that loads it until the process exits).
+ *   rows / values: the column's row ids and values as cyc_data_desc stores
+ *   them (dense: K values, no rows; indicator: rows only; intercept: none);
+ *   exb = exp(x beta) and, for lr, denom = 1 + exb, K doubles each;
+ *   weights: K row weights or NULL (unweighted); xjy: the column's sum x*y*w;
+ *   out: 2 doubles on the device receiving (gradient, Hessian);
+ *   stream: a cudaStream_t (NULL = the default stream).
+ * At most 4,194,304 column entries per call; larger columns are rejected.
+ * Runs on the calling thread's current device; the first call on a device
+ * looks up the scratch address there, so make it before any stream capture.
+ * Calls share the scratch: calls that overlap on the GPU race. */
+int cyc_gradient_hessian_noalloc(int model, int format, long long n, const int* rows,
+                                 const double* values, const double* exb, const double* denom,
+                                 const double* weights, double xjy, double* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
