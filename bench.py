@@ -229,7 +229,8 @@ def run_ours(args):
     data, lambdas, variances, desc, gen_s = workload(args.quick)
     folds = fold_ids(data.K, FOLD_SEED + rank)     # independent replicas per rank
     prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, [0])
-    control = api.create_control(tolerance=1e-6, precision=args.precision, polish_tolerance=1e-4)
+    control = api.create_control(tolerance=1e-6, precision=args.precision, polish_tolerance=1e-4,
+                                 max_iterations=args.max_iterations)
     F = N_FOLDS * N_LAMBDA
 
     ds = api.Dataset(data, device)
@@ -277,6 +278,16 @@ def run_ours(args):
     clocks = clk.summary()
 
     # end to end: upload from pinned host memory + solve + read back, every step
+    if args.no_e2e:
+        line = {"metric": "cv_fits_per_second", "value": value, "unit": "fits/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "kernel_ms_per_step": kernel_ms / args.steps, "gpu_launches": int(launches),
+                "phase_ms": phase_ms, "phase_bytes": phase_bytes}
+        if rank == 0:
+            print(json.dumps(line))
+        if dist:
+            dist.destroy_process_group()
+        return 0
     pinned = {}
     for name in ("y", "col_format", "col_ptr", "col_idx", "val_ptr", "col_val"):
         a = getattr(data, name)
@@ -374,6 +385,9 @@ def main(argv=None):
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--quick", action="store_true", help="small problem (smoke runs)")
     ap.add_argument("--no-baselines", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
+    ap.add_argument("--max-iterations", type=int, default=1000,
+                    help="cap on CCD cycles per fit (the reference default is 1000)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <memory>
 #include <vector>
 
@@ -65,6 +66,8 @@ struct BatchArgs {
     const double* variance;       // [F]
     const double* llfixed;        // [F]
     const int* active;            // [F] 0 for padding fits
+    const signed char* fold;      // K fold id per row (CV grid) or null
+    const int* fitfold;           // [F] held-out fold of each fit (CV grid)
     int conv;
     double tol;
     int max_iter;
@@ -120,14 +123,22 @@ __device__ __forceinline__ void block_reduce_lanes(double a, double b, double2* 
     __syncthreads();
 }
 
-template <class T, int MODEL, int G>
+// weight of (row k, fit lane) for one group: from the per-fit weight array,
+// or, for a CV grid, 1 when the row's fold is not the fit's held-out fold
+template <class T, int WM>
+__device__ __forceinline__ T row_weight(const T* wg, const signed char* fold, int fitfold, int k, int G, int fl) {
+    if (WM == 1) return (fitfold >= -1 && (int)__ldg(fold + k) != fitfold) ? T(1) : T(0);
+    return wg[(size_t)k * G + fl];
+}
+
+template <class T, int MODEL, int G, int WM>
 __device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp, int r0, int r1, int s0, int s1,
-                                                    const T* xbg, const T* wg, int fl, bool use_ll) {
+                                                    const T* xbg, const T* wg, int fitfold, int fl, bool use_ll) {
     Kahan<double> acc;
     const int slot = threadIdx.x / G, nslots = kBT / G;
     for (int k = r0 + slot; k < r1; k += nslots) {
         const double v = (double)xbg[(size_t)k * G + fl];
-        const double wt = (double)wg[(size_t)k * G + fl];
+        const double wt = (double)row_weight<T, WM>(wg, A.fold, fitfold, k, G, fl);
         const double yk = A.y[k];
         if (!use_ll) {
             acc.add(v * yk * wt);                                       // getGradientObjective
@@ -147,8 +158,36 @@ __device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp,
     return acc.value();
 }
 
-template <class T, int MODEL, int G>
-__global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
+// per-row contribution to (gradient, Hessian) of an independent-rows model
+// (Logistic / PoissonRegression::incrementGradientAndHessian,
+// ModelSpecifics.h:540-568, 1508-1543); the logistic probability is formed as
+// 1 / (1 + exp(-xb)), which equals exb / (1 + exb) without overflowing
+template <class T, int MODEL>
+__device__ __forceinline__ void row_gh(T v, T x, T wt, bool ind, Kahan<T>& ag, Kahan<T>& ah) {
+    if (MODEL == CYC_LR) {
+        const T p = T(1) / (T(1) + fexp(-v));
+        const T gi = p * x;
+        ag.add(wt * gi);
+        ah.add(wt * (ind ? gi * (T(1) - gi) : x * x * p * (T(1) - p)));
+    } else {
+        const T n1 = fexp(v) * x;
+        ag.add(wt * n1);
+        ah.add(wt * (ind ? n1 : n1 * x));
+    }
+}
+
+// Items of one coordinate a thread keeps in registers between the gradient
+// and the update: columns with at most kRegItems * (kBT / G) entries in this
+// CTA's rows take this path (one load round trip, no reload for the update);
+// longer ones stream through twice.
+constexpr int kRegItems = 8;
+// coordinates staged in shared memory at a time
+constexpr int kChunk = 128;
+// row ids of short columns staged per chunk (dynamic shared memory)
+constexpr int kStage = 4096;
+
+template <class T, int MODEL, int G, int WM>
+__global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     cg::cluster_group cluster = cg::this_cluster();
     const int C = A.C;
     const int rank = (int)cluster.block_rank();
@@ -159,16 +198,35 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
     const int s0 = (grouped && r0 < r1) ? A.strat[r0] : 0;
     const int s1 = (grouped && r0 < r1) ? (r1 >= A.K ? A.S : A.strat[r1]) : 0;
     T* xbg = (T*)A.xb + (size_t)grp * A.K * G;
-    const T* wg = (const T*)A.w + (size_t)grp * A.K * G;
+    const T* wg = (WM == 0) ? (const T*)A.w + (size_t)grp * A.K * G : nullptr;
     double* dg = grouped ? A.denom + (size_t)grp * A.S * G : nullptr;
     const double* ng = grouped ? A.nw + (size_t)grp * A.S * G : nullptr;
     const int fl = threadIdx.x % G;
-    const int slot = threadIdx.x / G, nslots = kBT / G;
+    const int slot = threadIdx.x / G;
+    constexpr int NS = kBT / G;
+    const int fg = grp * G;                   // first fit of the group
+    const int fitfold = (WM == 1) ? A.fitfold[fg + fl] : 0;
 
-    __shared__ double2 s_part[2][G];       // this CTA's (g, h) partial, double buffered
+    // every CTA's (g, h) partial for every fit lane, pushed into each CTA of the
+    // cluster before the barrier (double buffered by coordinate parity)
+    __shared__ double2 s_part[2][kMaxC][G];
+    // the current chunk of coordinates: column metadata and this group's
+    // beta / trust region / XjY, kept identical in every CTA of the cluster
+    __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk];
+    __shared__ long long c_cp[kChunk], c_vp[kChunk];
+    __shared__ double c_beta[kChunk][G], c_hd[kChunk][G], c_xjy[kChunk][G];
+    // row ids (and values) of the chunk's short columns, staged in one
+    // coalesced pass so a coordinate's critical path starts at the state load
+    __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
+    __shared__ int c_sq[kChunk + 1];       // staged coordinates in order
+    __shared__ int c_soff[kChunk + 1];     // their offsets (prefix sums)
+    __shared__ int c_ns;                   // how many coordinates are staged
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    int* s_sidx = reinterpret_cast<int*>(dyn_smem);
+    T* s_sx = reinterpret_cast<T*>(dyn_smem + kStage * sizeof(int));
     __shared__ double2 s_scr[kBT / 32][G];
     __shared__ double2 s_red[G];
-    __shared__ double s_obj[2][G];
+    __shared__ double s_obj[2][kMaxC][G];
     __shared__ double s_delta[G];
     __shared__ double s_last[G];
     __shared__ int s_done[G];
@@ -177,7 +235,6 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
     __shared__ int s_any, s_all_done;
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
-    const int fg = grp * G;                   // first fit of the group
     if (threadIdx.x < G) {
         const int f = fg + threadIdx.x;
         s_done[threadIdx.x] = A.active[f] ? 0 : 1;
@@ -189,14 +246,15 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
     // initial objective (findMode :949-953)
     int opar = 0;
     {
-        const double p = objective_partial<T, MODEL, G>(A, grp, r0, r1, s0, s1, xbg, wg, fl, use_ll);
+        const double p = objective_partial<T, MODEL, G, WM>(A, grp, r0, r1, s0, s1, xbg, wg, fitfold, fl, use_ll);
         block_reduce_lanes<G>(p, 0.0, s_red, s_scr);
-        if (threadIdx.x < G) s_obj[opar][threadIdx.x] = s_red[threadIdx.x].x;
-        cluster.sync();
+        if (threadIdx.x < G)
+            for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_obj[opar][rank][threadIdx.x], r) = s_red[threadIdx.x].x;
+        if (C > 1) cluster.sync(); else __syncthreads();
         if (threadIdx.x < G) {
             const int f = fg + threadIdx.x;
             double o = 0.0;
-            for (int r = 0; r < C; ++r) o += *cluster.map_shared_rank(&s_obj[opar][threadIdx.x], r);
+            for (int r = 0; r < C; ++r) o += s_obj[opar][r][threadIdx.x];
             if (use_ll && (MODEL == CYC_PR || MODEL == CYC_CPR)) o += A.llfixed[f];
             if (A.conv == CYC_CONV_LANGE) {
                 const double* bf = A.beta + (size_t)f * A.J;
@@ -206,53 +264,150 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
         }
         opar ^= 1;
     }
+    __syncthreads();
+    bool done_l = s_done[fl] != 0;   // this thread's fit lane has converged
+    const double var_l = A.variance[fg + fl];
 
     unsigned long long n_grad = 0, n_upd = 0, n_steps = 0, n_idx = 0;
     int par = 0;
     for (int it = 1; it <= A.max_iter; ++it) {
-        for (int j = 0; j < A.J; ++j) {
-            if (A.fixb[j]) continue;
-            const int fmt = A.fmt[j];
+      for (int j0 = 0; j0 < A.J; j0 += kChunk) {
+        const int jn = min(kChunk, A.J - j0);
+        // stage the chunk (coalesced), then run its coordinates from shared memory
+        for (int q = threadIdx.x; q < jn; q += kBT) {
+            const int j = j0 + q;
+            const int f0 = A.fmt[j];
+            c_fmt[q] = f0;
+            c_fix[q] = A.fixb[j];
+            c_pt[q] = A.ptype[j];
+            c_cp[q] = A.col_ptr[j];
+            c_vp[q] = A.val_ptr[j];
+            const bool dn = (f0 == CYC_DENSE || f0 == CYC_INTERCEPT);
+            c_e0[q] = dn ? r0 : A.split[j * (C + 1) + rank];
+            c_e1[q] = dn ? r1 : A.split[j * (C + 1) + rank + 1];
+        }
+        for (int q = threadIdx.x; q < jn * G; q += kBT) {
+            const int ff = q / jn, jj = q % jn;
+            const size_t o = (size_t)(fg + ff) * A.J + j0 + jj;
+            c_beta[jj][ff] = A.beta[o];
+            c_hd[jj][ff] = A.hdelta[o];
+            c_xjy[jj][ff] = A.xjy[o];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int off = 0, ns = 0;
+            for (int qq = 0; qq < jn; ++qq) {
+                const int n = c_e1[qq] - c_e0[qq];
+                const bool dn = (c_fmt[qq] == CYC_DENSE || c_fmt[qq] == CYC_INTERCEPT);
+                if (!grouped && !c_fix[qq] && !dn && n > 0 && n <= kRegItems * NS && off + n <= kStage) {
+                    c_off[qq] = off;
+                    c_sq[ns] = qq;
+                    c_soff[ns] = off;
+                    ++ns;
+                    off += n;
+                } else {
+                    c_off[qq] = -1;
+                }
+            }
+            c_soff[ns] = off;
+            c_ns = ns;
+        }
+        __syncthreads();
+        {
+            const int ns = c_ns, total = c_soff[ns];
+            for (int t = threadIdx.x; t < total; t += kBT) {
+                int lo = 0, hi = ns - 1;                 // last staged column with offset <= t
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (c_soff[mid] <= t) lo = mid;
+                    else hi = mid - 1;
+                }
+                const int qq = c_sq[lo];
+                const long long e = c_e0[qq] + (t - c_soff[lo]);
+                s_sidx[t] = __ldg(A.idx + c_cp[qq] + e);
+                s_sx[t] = (c_fmt[qq] == CYC_SPARSE) ? (T)__ldg(A.val + c_vp[qq] + e) : T(1);
+            }
+        }
+        __syncthreads();
+        for (int q = 0; q < jn; ++q) {
+            const int j = j0 + q;
+            if (c_fix[q]) continue;
+            const int fmt = c_fmt[q];
             const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
             const bool ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
-            const int* cidx = A.idx + A.col_ptr[j];
-            const double* cval = A.val + A.val_ptr[j];
-            int e0, e1;
-            if (dense) { e0 = r0; e1 = r1; }
-            else { e0 = A.split[j * (C + 1) + rank]; e1 = A.split[j * (C + 1) + rank + 1]; }
-            // step inputs, read before the barrier (rank 0 rewrites them after it)
+            const int* cidx = A.idx + c_cp[q];
+            const double* cval = A.val + c_vp[q];
+            const int e0 = c_e0[q], e1 = c_e1[q];
             double b_f = 0.0, hd_f = 0.0, xjy_f = 0.0, var_f = 1.0;
             int done_f = 1;
             if (threadIdx.x < G) {
-                const int f = fg + threadIdx.x;
-                b_f = A.beta[(size_t)f * A.J + j];
-                hd_f = A.hdelta[(size_t)f * A.J + j];
-                xjy_f = A.xjy[(size_t)f * A.J + j];
-                var_f = A.variance[f];
+                b_f = c_beta[q][threadIdx.x];
+                hd_f = c_hd[q][threadIdx.x];
+                xjy_f = c_xjy[q][threadIdx.x];
+                var_f = var_l;
                 done_f = s_done[threadIdx.x];
             }
+            const bool regpath = !grouped && (e1 - e0) <= kRegItems * NS;
             // ---- gradient and Hessian of my rows (computeGradientAndHessianImpl)
             Kahan<T> ag, ah;
-            if (!grouped) {
-                for (int e = e0 + slot; e < e1; e += nslots) {
-                    const int k = dense ? e : __ldg(cidx + e);
-                    const T x = ind ? T(1) : (T)__ldg(cval + e);
-                    const T v = xbg[(size_t)k * G + fl];
-                    const T wt = wg[(size_t)k * G + fl];
-                    const T ex = fexp(v);
-                    if (MODEL == CYC_LR) {                // Logistic::incrementGradientAndHessian
-                        const T p = ex / (T(1) + ex);
-                        const T gi = p * x;
-                        ag.add(wt * gi);
-                        ah.add(wt * (ind ? gi * (T(1) - gi) : x * x * p * (T(1) - p)));
-                    } else {                              // PoissonRegression::incrementGradientAndHessian
-                        const T n1 = ex * x;
-                        ag.add(wt * n1);
-                        ah.add(wt * (ind ? n1 : n1 * x));
+            int kk[kRegItems];
+            T vv[kRegItems], xx[kRegItems];
+            if (regpath) {
+                // every load of this coordinate issued before any is used
+                const int so = c_off[q];
+                if (so >= 0) {
+                    #pragma unroll
+                    for (int r = 0; r < kRegItems; ++r) {
+                        const int e = slot + r * NS;            // relative to e0
+                        kk[r] = (e < e1 - e0 && !done_l) ? s_sidx[so + e] : -1;
+                        xx[r] = (e < e1 - e0 && !ind) ? s_sx[so + e] : T(1);
+                    }
+                } else {
+                    #pragma unroll
+                    for (int r = 0; r < kRegItems; ++r) {
+                        const int e = e0 + slot + r * NS;
+                        kk[r] = (e < e1 && !done_l) ? (dense ? e : __ldg(cidx + e)) : -1;
+                        xx[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
+                    }
+                }
+                T ww[kRegItems];
+                #pragma unroll
+                for (int r = 0; r < kRegItems; ++r) {
+                    if (kk[r] >= 0) {
+                        vv[r] = xbg[(size_t)kk[r] * G + fl];
+                        ww[r] = row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl);
+                    } else {
+                        vv[r] = T(0);
+                        ww[r] = T(0);
+                    }
+                }
+                #pragma unroll
+                for (int r = 0; r < kRegItems; ++r)
+                    if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+            } else if (!grouped) {
+                if (!done_l) {
+                    // long column: batches of kRegItems entries per thread, loads first
+                    for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
+                        int k2[kRegItems];
+                        T x2[kRegItems], v2[kRegItems], w2[kRegItems];
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r) {
+                            const int e = base + r * NS;
+                            k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
+                            x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
+                        }
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r) {
+                            v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
+                            w2[r] = k2[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, k2[r], G, fl) : T(0);
+                        }
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r)
+                            if (k2[r] >= 0) row_gh<T, MODEL>(v2[r], x2[r], w2[r], ind, ag, ah);
                     }
                 }
             } else {
-                for (int e = e0 + slot; e < e1; e += nslots) {
+                for (int e = e0 + slot; e < e1; e += NS) {
                     const int k = dense ? e : __ldg(cidx + e);
                     const int s = A.strat[k];
                     if (e > e0) {
@@ -280,14 +435,14 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
                 }
             }
             block_reduce_lanes<G>(ag.value(), ah.value(), s_red, s_scr);
-            if (threadIdx.x < G) s_part[par][threadIdx.x] = s_red[threadIdx.x];
-            cluster.sync();
+            if (threadIdx.x < G)
+                for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][threadIdx.x], r) = s_red[threadIdx.x];
+            if (C > 1) cluster.sync(); else __syncthreads();
             // ---- coordinate step, identical in every CTA of the cluster
             if (threadIdx.x < G) {
-                const int f = fg + threadIdx.x;
                 double g = 0.0, h = 0.0;
                 for (int r = 0; r < C; ++r) {
-                    const double2 p = *cluster.map_shared_rank(&s_part[par][threadIdx.x], r);
+                    const double2 p = s_part[par][r][threadIdx.x];
                     g += p.x;
                     h += p.y;
                 }
@@ -295,50 +450,52 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
                 double delta = 0.0;
                 if (!done_f) {
                     if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
-                    delta = prior_delta(A.ptype[j], var_f, b_f, g, h);
+                    delta = prior_delta(c_pt[q], var_f, b_f, g, h);
                     delta = apply_bounds(&hd_f, delta);
-                    if (rank == 0) {
-                        A.hdelta[(size_t)f * A.J + j] = hd_f;
-                        if (delta != 0.0) A.beta[(size_t)f * A.J + j] = b_f + delta;
-                    }
+                    c_hd[q][threadIdx.x] = hd_f;
+                    if (delta != 0.0) c_beta[q][threadIdx.x] = b_f + delta;
                 }
                 s_delta[threadIdx.x] = delta;
             }
             __syncthreads();
-            if (threadIdx.x == 0) {
-                int any = 0;
-                for (int q = 0; q < G; ++q) any |= (s_delta[q] != 0.0);
-                s_any = any;
-                if (rank == 0) {
-                    int act = 0, upd = 0;
-                    for (int q = 0; q < G; ++q) { act += !s_done[q]; upd += (s_delta[q] != 0.0); }
-                    const long long n = A.col_ptr[j + 1] - A.col_ptr[j];
-                    const long long nn = dense ? A.K : n;
-                    n_grad += (unsigned long long)(act * nn);
-                    n_upd += (unsigned long long)(upd * nn);
-                    n_steps += act;
-                    // the column streamed by this group: row ids (not for dense) and
-                    // values (sparse, dense), once for the gradient, again for an update
-                    const long long cb = nn * ((dense ? 0 : 4) + (ind ? 0 : 8));
-                    n_idx += (unsigned long long)(cb * (1 + (any ? 1 : 0)));
-                }
+            const double dl = s_delta[fl];
+            if (rank == 0 && threadIdx.x == 0) {
+                int act = 0, upd = 0;
+                for (int q = 0; q < G; ++q) { act += !s_done[q]; upd += (s_delta[q] != 0.0); }
+                const long long nn = dense ? A.K : A.col_ptr[j + 1] - A.col_ptr[j];
+                n_grad += (unsigned long long)(act * nn);
+                n_upd += (unsigned long long)(upd * nn);
+                n_steps += act;
+                // the column streamed by this group: row ids (not for dense) and
+                // values (sparse, dense), once for the gradient, again for an update
+                const long long cb = nn * ((dense ? 0 : 4) + (ind ? 0 : 8));
+                n_idx += (unsigned long long)(cb * (1 + (upd ? 1 : 0)));
             }
-            __syncthreads();
             // ---- updateXBeta for my rows
-            if (s_any) {
-                const double dl = s_delta[fl];
+            if (dl != 0.0) {
                 const T d = (T)dl;
-                if (!grouped) {
-                    if (dl != 0.0) {
-                        for (int e = e0 + slot; e < e1; e += nslots) {
-                            const int k = dense ? e : __ldg(cidx + e);
-                            const T x = ind ? T(1) : (T)__ldg(cval + e);
-                            T* p = xbg + (size_t)k * G + fl;
-                            *p = *p + d * x;
+                if (regpath) {
+                    #pragma unroll
+                    for (int r = 0; r < kRegItems; ++r)
+                        if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
+                } else if (!grouped) {
+                    for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
+                        int k2[kRegItems];
+                        T x2[kRegItems], v2[kRegItems];
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r) {
+                            const int e = base + r * NS;
+                            k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
+                            x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
                         }
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r) v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
+                        #pragma unroll
+                        for (int r = 0; r < kRegItems; ++r)
+                            if (k2[r] >= 0) xbg[(size_t)k2[r] * G + fl] = v2[r] + d * x2[r];
                     }
-                } else if (dl != 0.0) {
-                    for (int e = e0 + slot; e < e1; e += nslots) {
+                } else {
+                    for (int e = e0 + slot; e < e1; e += NS) {
                         const int k = dense ? e : __ldg(cidx + e);
                         const int s = A.strat[k];
                         if (e > e0) {
@@ -366,15 +523,26 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
             __syncthreads();
             par ^= 1;
         }
+        // chunk done: rank 0 writes the group's beta and trust regions back
+        if (rank == 0)
+            for (int q = threadIdx.x; q < jn * G; q += kBT) {
+                const int ff = q / jn, jj = q % jn;
+                const size_t o = (size_t)(fg + ff) * A.J + j0 + jj;
+                A.beta[o] = c_beta[jj][ff];
+                A.hdelta[o] = c_hd[jj][ff];
+            }
+        __syncthreads();
+      }
         // ---- convergence test (performCheckConvergence)
-        const double p = objective_partial<T, MODEL, G>(A, grp, r0, r1, s0, s1, xbg, wg, fl, use_ll);
+        const double p = objective_partial<T, MODEL, G, WM>(A, grp, r0, r1, s0, s1, xbg, wg, fitfold, fl, use_ll);
         block_reduce_lanes<G>(p, 0.0, s_red, s_scr);
-        if (threadIdx.x < G) s_obj[opar][threadIdx.x] = s_red[threadIdx.x].x;
-        cluster.sync();
+        if (threadIdx.x < G)
+            for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_obj[opar][rank][threadIdx.x], r) = s_red[threadIdx.x].x;
+        if (C > 1) cluster.sync(); else __syncthreads();
         if (threadIdx.x < G) {
             const int f = fg + threadIdx.x;
             double o = 0.0;
-            for (int r = 0; r < C; ++r) o += *cluster.map_shared_rank(&s_obj[opar][threadIdx.x], r);
+            for (int r = 0; r < C; ++r) o += s_obj[opar][r][threadIdx.x];
             if (use_ll && (MODEL == CYC_PR || MODEL == CYC_CPR)) o += A.llfixed[f];
             if (A.conv == CYC_CONV_LANGE) {
                 const double* bf = A.beta + (size_t)f * A.J;
@@ -404,9 +572,10 @@ __global__ void __launch_bounds__(kBT) k_batch(const BatchArgs A) {
             s_all_done = all;
         }
         __syncthreads();
+        done_l = s_done[fl] != 0;
         if (s_all_done) break;
     }
-    cluster.sync();   // no CTA leaves while others may still read its shared memory
+    if (C > 1) cluster.sync();   // no CTA leaves while others may still read its shared memory
     if (rank == 0 && threadIdx.x < G) {
         const int f = fg + threadIdx.x;
         A.out_iter[f] = s_iter[threadIdx.x];
@@ -448,6 +617,10 @@ __global__ void k_scatter_weights(int K, int G, int f, const double* __restrict_
     const int grp = f / G, lane = f % G;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x)
         w[((size_t)grp * K + k) * G + lane] = src ? (T)src[k] : T(1);
+}
+
+__global__ void k_fold_to_i8(int K, const int* __restrict__ fold, signed char* __restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) out[k] = (signed char)fold[k];
 }
 
 // CV grid weights: fit f trains on the rows outside its fold (padding fits: none)
@@ -593,12 +766,14 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
 
 }  // namespace
 
-template <class T, int MODEL, int G>
+template <class T, int MODEL, int G, int WM>
 static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
-    cfg.dynamicSmemBytes = 0;
+    const size_t dyn = kStage * (sizeof(int) + sizeof(T));
+    CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+    cfg.dynamicSmemBytes = dyn;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -607,17 +782,18 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CYC_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_batch<T, MODEL, G>, a));
+    CYC_CHECK_CUDA(cudaLaunchKernelEx(&cfg, k_batch<T, MODEL, G, WM>, a));
     count_launch();
 }
 
 template <class T, int G>
 static void launch_model(const BatchArgs& a, int ngroups, cudaStream_t stream) {
+    const bool cv = a.fold != nullptr;
     switch (a.model) {
-    case CYC_LR: launch_batch<T, CYC_LR, G>(a, ngroups, stream); break;
-    case CYC_PR: launch_batch<T, CYC_PR, G>(a, ngroups, stream); break;
-    case CYC_CLR: launch_batch<T, CYC_CLR, G>(a, ngroups, stream); break;
-    case CYC_CPR: launch_batch<T, CYC_CPR, G>(a, ngroups, stream); break;
+    case CYC_LR: cv ? launch_batch<T, CYC_LR, G, 1>(a, ngroups, stream) : launch_batch<T, CYC_LR, G, 0>(a, ngroups, stream); break;
+    case CYC_PR: cv ? launch_batch<T, CYC_PR, G, 1>(a, ngroups, stream) : launch_batch<T, CYC_PR, G, 0>(a, ngroups, stream); break;
+    case CYC_CLR: cv ? launch_batch<T, CYC_CLR, G, 1>(a, ngroups, stream) : launch_batch<T, CYC_CLR, G, 0>(a, ngroups, stream); break;
+    case CYC_CPR: cv ? launch_batch<T, CYC_CPR, G, 1>(a, ngroups, stream) : launch_batch<T, CYC_CPR, G, 0>(a, ngroups, stream); break;
     default: throw Error{CYC_ERR_UNSUPPORTED, "batched fits support lr, pr, clr, cpr"};
     }
 }
@@ -640,6 +816,7 @@ struct BatchRunner {
         Fp = ngroups * G;
         const int K = ds.K;
         C = std::max(1, std::min(kMaxC, (K + 16383) / 16384));
+        if (const char* e = std::getenv("CYC_BATCH_CLUSTER")) C = std::max(1, std::min(kMaxC, std::atoi(e)));
         // row partition, aligned to strata for grouped models
         rpart.assign(C + 1, K);
         for (int r = 0; r < C; ++r) {
@@ -659,8 +836,12 @@ struct BatchRunner {
     const int* d_fold = nullptr;
     DevBuf<int> d_fitfold;
 
+    DevBuf<signed char> d_fold8;
+
     void set_folds(const int* d_fold_of_row, const std::vector<int>& fit_fold) {
         d_fold = d_fold_of_row;
+        d_fold8.alloc(ds.K);
+        launch(k_fold_to_i8, grid_for(ds.K, 1), 256, 0, stream, ds.K, d_fold, d_fold8.get());
         std::vector<int> ff(Fp, -2);
         std::copy(fit_fold.begin(), fit_fold.end(), ff.begin());
         d_fitfold.alloc(Fp);
@@ -757,6 +938,8 @@ struct BatchRunner {
         a.fixb = d_fixb.get(); a.ptype = d_ptype.get(); a.xb = d_xb.get(); a.w = d_w.get();
         a.denom = d_denom.get(); a.nw = d_nw.get(); a.xjy = d_xjy.get(); a.beta = d_beta.get();
         a.hdelta = d_hdelta.get(); a.variance = d_var.get(); a.llfixed = d_llfixed.get(); a.active = d_active.get();
+        a.fold = d_fold ? d_fold8.get() : nullptr;
+        a.fitfold = d_fold ? d_fitfold.get() : nullptr;
         a.conv = ctl.convergence_type; a.tol = tol; a.max_iter = ctl.max_iterations;
         a.out_iter = d_iter.get(); a.out_flag = d_flag.get(); a.out_obj = d_obj.get(); a.counters = d_counters.get();
         cudaEvent_t e0, e1;
@@ -925,6 +1108,7 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
     return guarded([&] {
         CYC_REQUIRE(dsh && prior && fold_of_row && variances && ctl && out && n_folds > 1 && n_var > 0,
                     CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(n_folds <= 127, CYC_ERR_ARGUMENT, "at most 127 folds");
         Dataset& ds = dsh->ds;
         for (int k = 0; k < ds.K; ++k)
             CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
