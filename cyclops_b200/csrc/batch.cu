@@ -68,6 +68,7 @@ struct BatchArgs {
     const int* active;            // [F] 0 for padding fits
     const signed char* fold;      // K fold id per row (CV grid) or null
     const int* fitfold;           // [F] held-out fold of each fit (CV grid)
+    const int* run_len;           // J: columns in the run starting here (1 = alone), 0 inside a run
     int conv;
     double tol;
     int max_iter;
@@ -186,6 +187,18 @@ constexpr int kChunk = 128;
 // row ids of short columns staged per chunk (dynamic shared memory)
 constexpr int kStage = 4096;
 
+// Columns processed together: consecutive short columns whose rows are
+// pairwise disjoint (planned on the host, ConflictFreeRuns) form a run of at
+// most kRunMax columns.  For independent-rows models the gradient of a column
+// depends only on the linear predictor of its own rows, so the columns of a
+// run see exactly the state the serial coordinate loop would show them, and
+// their updates touch disjoint rows: the run gives the serial CCD result while
+// paying for one load round trip and one cluster barrier.  Warp w of every
+// CTA takes column w of the run.
+constexpr int kRunMax = kBT / 32;
+// entries per slot of a run column (a warp has 32/G slots)
+constexpr int kRunItems = 8;
+
 template <class T, int MODEL, int G, int WM>
 __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     cg::cluster_group cluster = cg::this_cluster();
@@ -204,35 +217,40 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     const int fl = threadIdx.x % G;
     const int slot = threadIdx.x / G;
     constexpr int NS = kBT / G;
+    constexpr int WS = 32 / G;                // slots per warp
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wslot = lane / G;
     const int fg = grp * G;                   // first fit of the group
     const int fitfold = (WM == 1) ? A.fitfold[fg + fl] : 0;
 
-    // every CTA's (g, h) partial for every fit lane, pushed into each CTA of the
-    // cluster before the barrier (double buffered by coordinate parity)
-    __shared__ double2 s_part[2][kMaxC][G];
-    // the current chunk of coordinates: column metadata and this group's
-    // beta / trust region / XjY, kept identical in every CTA of the cluster
-    __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk];
-    __shared__ long long c_cp[kChunk], c_vp[kChunk];
-    __shared__ double c_beta[kChunk][G], c_hd[kChunk][G], c_xjy[kChunk][G];
-    // row ids (and values) of the chunk's short columns, staged in one
-    // coalesced pass so a coordinate's critical path starts at the state load
-    __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
-    __shared__ int c_sq[kChunk + 1];       // staged coordinates in order
-    __shared__ int c_soff[kChunk + 1];     // their offsets (prefix sums)
-    __shared__ int c_ns;                   // how many coordinates are staged
-    extern __shared__ __align__(16) unsigned char dyn_smem[];
-    int* s_sidx = reinterpret_cast<int*>(dyn_smem);
-    T* s_sx = reinterpret_cast<T*>(dyn_smem + kStage * sizeof(int));
+    // every CTA's (g, h) partials, pushed into each CTA of the cluster before
+    // the barrier (double buffered by parity; one slot per column of a run)
+    __shared__ double2 s_part[2][kMaxC][kRunMax][G];
     __shared__ double2 s_scr[kBT / 32][G];
     __shared__ double2 s_red[G];
     __shared__ double s_obj[2][kMaxC][G];
     __shared__ double s_delta[G];
+    __shared__ double s_dr[kRunMax][G];
     __shared__ double s_last[G];
     __shared__ int s_done[G];
     __shared__ int s_flag[G];
     __shared__ int s_iter[G];
-    __shared__ int s_any, s_all_done;
+    __shared__ int s_all_done;
+    // the current chunk of coordinates
+    __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk], c_run[kChunk];
+    __shared__ long long c_cp[kChunk], c_vp[kChunk];
+    __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
+    __shared__ int c_sq[kChunk + 1];       // staged coordinates in order
+    __shared__ int c_soff[kChunk + 1];     // their offsets (prefix sums)
+    __shared__ int c_ns;
+    // dynamic: this group's beta / trust region / XjY for the chunk (kept
+    // identical in every CTA of the cluster), then the staged row ids / values
+    extern __shared__ __align__(16) unsigned char dyn_smem[];
+    double (*c_beta)[G] = reinterpret_cast<double (*)[G]>(dyn_smem);
+    double (*c_hd)[G] = reinterpret_cast<double (*)[G]>(dyn_smem + kChunk * G * sizeof(double));
+    double (*c_xjy)[G] = reinterpret_cast<double (*)[G]>(dyn_smem + 2 * kChunk * G * sizeof(double));
+    int* s_sidx = reinterpret_cast<int*>(dyn_smem + 3 * kChunk * G * sizeof(double));
+    T* s_sx = reinterpret_cast<T*>(dyn_smem + 3 * kChunk * G * sizeof(double) + kStage * sizeof(int));
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
     if (threadIdx.x < G) {
@@ -273,13 +291,14 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     for (int it = 1; it <= A.max_iter; ++it) {
       for (int j0 = 0; j0 < A.J; j0 += kChunk) {
         const int jn = min(kChunk, A.J - j0);
-        // stage the chunk (coalesced), then run its coordinates from shared memory
+        // ---- stage the chunk (coalesced)
         for (int q = threadIdx.x; q < jn; q += kBT) {
             const int j = j0 + q;
             const int f0 = A.fmt[j];
             c_fmt[q] = f0;
             c_fix[q] = A.fixb[j];
             c_pt[q] = A.ptype[j];
+            c_run[q] = A.run_len[j];
             c_cp[q] = A.col_ptr[j];
             c_vp[q] = A.val_ptr[j];
             const bool dn = (f0 == CYC_DENSE || f0 == CYC_INTERCEPT);
@@ -329,57 +348,122 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             }
         }
         __syncthreads();
-        for (int q = 0; q < jn; ++q) {
-            const int j = j0 + q;
-            if (c_fix[q]) continue;
+        int q = 0;
+        while (q < jn) {
+            const int L = c_run[q];
+            if (c_fix[q] || L <= 0) { ++q; continue; }
+            if (L > 1) {
+                // ---- a run of L conflict-free short columns: warp w takes column q + w
+                const int qq = q + warp;
+                int kk[kRunItems];
+                T vv[kRunItems], xx[kRunItems];
+                bool ind = true;
+                if (warp < L) {
+                    const int fmt = c_fmt[qq];
+                    ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
+                    const int e0 = c_e0[qq], n = c_e1[qq] - e0, so = c_off[qq];
+                    const int* cidx = A.idx + c_cp[qq];
+                    const double* cval = A.val + c_vp[qq];
+                    #pragma unroll
+                    for (int r = 0; r < kRunItems; ++r) {
+                        const int e = wslot + r * WS;
+                        const bool ok = e < n && !done_l;
+                        kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : __ldg(cidx + e0 + e));
+                        xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
+                    }
+                    T ww[kRunItems];
+                    #pragma unroll
+                    for (int r = 0; r < kRunItems; ++r) {
+                        vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
+                        ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
+                    }
+                    Kahan<T> ag, ah;
+                    #pragma unroll
+                    for (int r = 0; r < kRunItems; ++r)
+                        if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+                    double g = ag.value(), h = ah.value();
+                    for (int o = G; o < 32; o <<= 1) {
+                        g += __shfl_xor_sync(0xffffffffu, g, o);
+                        h += __shfl_xor_sync(0xffffffffu, h, o);
+                    }
+                    if (lane < G)
+                        for (int r = 0; r < C; ++r)
+                            *cluster.map_shared_rank(&s_part[par][rank][warp][lane], r) = make_double2(g, h);
+                }
+                if (C > 1) cluster.sync(); else __syncthreads();
+                double dl = 0.0;
+                if (warp < L) {
+                    if (lane < G) {
+                        double g = 0.0, h = 0.0;
+                        for (int r = 0; r < C; ++r) {
+                            const double2 pp = s_part[par][r][warp][lane];
+                            g += pp.x;
+                            h += pp.y;
+                        }
+                        g -= c_xjy[qq][lane];                     // :1181-1183
+                        if (!s_done[lane]) {
+                            if (h < 0.0) { g = 0.0; h = 0.0; }    // ccdUpdateBeta :1407-1410
+                            const double b = c_beta[qq][lane];
+                            double hd = c_hd[qq][lane];
+                            dl = prior_delta(c_pt[qq], var_l, b, g, h);
+                            dl = apply_bounds(&hd, dl);
+                            c_hd[qq][lane] = hd;
+                            if (dl != 0.0) c_beta[qq][lane] = b + dl;
+                        }
+                        s_dr[warp][lane] = dl;
+                    }
+                    dl = __shfl_sync(0xffffffffu, dl, fl);
+                    if (dl != 0.0) {
+                        const T d = (T)dl;
+                        #pragma unroll
+                        for (int r = 0; r < kRunItems; ++r)
+                            if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
+                    }
+                }
+                __syncthreads();
+                if (rank == 0 && threadIdx.x == 0) {
+                    int act = 0;
+                    for (int f = 0; f < G; ++f) act += !s_done[f];
+                    for (int w = 0; w < L; ++w) {
+                        int upd = 0;
+                        for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
+                        const long long nn = A.col_ptr[j0 + q + w + 1] - A.col_ptr[j0 + q + w];
+                        const bool in = (c_fmt[q + w] == CYC_INDICATOR);
+                        n_grad += (unsigned long long)(act * nn);
+                        n_upd += (unsigned long long)(upd * nn);
+                        n_steps += act;
+                        n_idx += (unsigned long long)(nn * (4 + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
+                    }
+                }
+                par ^= 1;
+                q += L;
+                continue;
+            }
+            // ---- a single column
             const int fmt = c_fmt[q];
             const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
             const bool ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
             const int* cidx = A.idx + c_cp[q];
             const double* cval = A.val + c_vp[q];
             const int e0 = c_e0[q], e1 = c_e1[q];
-            double b_f = 0.0, hd_f = 0.0, xjy_f = 0.0, var_f = 1.0;
-            int done_f = 1;
-            if (threadIdx.x < G) {
-                b_f = c_beta[q][threadIdx.x];
-                hd_f = c_hd[q][threadIdx.x];
-                xjy_f = c_xjy[q][threadIdx.x];
-                var_f = var_l;
-                done_f = s_done[threadIdx.x];
-            }
             const bool regpath = !grouped && (e1 - e0) <= kRegItems * NS;
-            // ---- gradient and Hessian of my rows (computeGradientAndHessianImpl)
             Kahan<T> ag, ah;
             int kk[kRegItems];
             T vv[kRegItems], xx[kRegItems];
             if (regpath) {
-                // every load of this coordinate issued before any is used
                 const int so = c_off[q];
-                if (so >= 0) {
-                    #pragma unroll
-                    for (int r = 0; r < kRegItems; ++r) {
-                        const int e = slot + r * NS;            // relative to e0
-                        kk[r] = (e < e1 - e0 && !done_l) ? s_sidx[so + e] : -1;
-                        xx[r] = (e < e1 - e0 && !ind) ? s_sx[so + e] : T(1);
-                    }
-                } else {
-                    #pragma unroll
-                    for (int r = 0; r < kRegItems; ++r) {
-                        const int e = e0 + slot + r * NS;
-                        kk[r] = (e < e1 && !done_l) ? (dense ? e : __ldg(cidx + e)) : -1;
-                        xx[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
-                    }
+                #pragma unroll
+                for (int r = 0; r < kRegItems; ++r) {
+                    const int e = slot + r * NS;                 // relative to e0
+                    const bool ok = e < e1 - e0 && !done_l;
+                    kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : (dense ? e0 + e : __ldg(cidx + e0 + e)));
+                    xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
                 }
                 T ww[kRegItems];
                 #pragma unroll
                 for (int r = 0; r < kRegItems; ++r) {
-                    if (kk[r] >= 0) {
-                        vv[r] = xbg[(size_t)kk[r] * G + fl];
-                        ww[r] = row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl);
-                    } else {
-                        vv[r] = T(0);
-                        ww[r] = T(0);
-                    }
+                    vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
+                    ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
                 }
                 #pragma unroll
                 for (int r = 0; r < kRegItems; ++r)
@@ -415,16 +499,16 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         if (A.strat[kp] == s) continue;
                     }
                     T n1 = 0, n2 = 0;
-                    int q = e;
+                    int qe = e;
                     int kq = k;
                     do {                                  // the run of stratum s in this column
-                        const T x = ind ? T(1) : (T)__ldg(cval + q);
+                        const T x = ind ? T(1) : (T)__ldg(cval + qe);
                         const T ex = fexp(xbg[(size_t)kq * G + fl]);
                         n1 += ex * x;
                         if (!ind) n2 += ex * x * x;
-                        ++q;
-                        if (q >= e1) break;
-                        kq = dense ? q : __ldg(cidx + q);
+                        ++qe;
+                        if (qe >= e1) break;
+                        kq = dense ? qe : __ldg(cidx + qe);
                     } while (A.strat[kq] == s);
                     const double d = dg[(size_t)s * G + fl];
                     const double nwv = ng[(size_t)s * G + fl];
@@ -436,24 +520,26 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             }
             block_reduce_lanes<G>(ag.value(), ah.value(), s_red, s_scr);
             if (threadIdx.x < G)
-                for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][threadIdx.x], r) = s_red[threadIdx.x];
+                for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
             if (C > 1) cluster.sync(); else __syncthreads();
             // ---- coordinate step, identical in every CTA of the cluster
             if (threadIdx.x < G) {
                 double g = 0.0, h = 0.0;
                 for (int r = 0; r < C; ++r) {
-                    const double2 p = s_part[par][r][threadIdx.x];
-                    g += p.x;
-                    h += p.y;
+                    const double2 pp = s_part[par][r][0][threadIdx.x];
+                    g += pp.x;
+                    h += pp.y;
                 }
-                g -= xjy_f;                                     // :1181-1183
+                g -= c_xjy[q][threadIdx.x];                    // :1181-1183
                 double delta = 0.0;
-                if (!done_f) {
+                if (!s_done[threadIdx.x]) {
                     if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
-                    delta = prior_delta(c_pt[q], var_f, b_f, g, h);
-                    delta = apply_bounds(&hd_f, delta);
-                    c_hd[q][threadIdx.x] = hd_f;
-                    if (delta != 0.0) c_beta[q][threadIdx.x] = b_f + delta;
+                    const double b = c_beta[q][threadIdx.x];
+                    double hd = c_hd[q][threadIdx.x];
+                    delta = prior_delta(c_pt[q], var_l, b, g, h);
+                    delta = apply_bounds(&hd, delta);
+                    c_hd[q][threadIdx.x] = hd;
+                    if (delta != 0.0) c_beta[q][threadIdx.x] = b + delta;
                 }
                 s_delta[threadIdx.x] = delta;
             }
@@ -461,14 +547,16 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             const double dl = s_delta[fl];
             if (rank == 0 && threadIdx.x == 0) {
                 int act = 0, upd = 0;
-                for (int q = 0; q < G; ++q) { act += !s_done[q]; upd += (s_delta[q] != 0.0); }
-                const long long nn = dense ? A.K : A.col_ptr[j + 1] - A.col_ptr[j];
-                n_grad += (unsigned long long)(act * nn);
-                n_upd += (unsigned long long)(upd * nn);
+                for (int f = 0; f < G; ++f) { act += !s_done[f]; upd += (s_delta[f] != 0.0); }
+                const long long nn = dense ? A.K : c_cp[q + 1 < jn ? q + 1 : q] - c_cp[q];
+                const long long nnc = dense ? A.K : A.col_ptr[j0 + q + 1] - A.col_ptr[j0 + q];
+                (void)nn;
+                n_grad += (unsigned long long)(act * nnc);
+                n_upd += (unsigned long long)(upd * nnc);
                 n_steps += act;
                 // the column streamed by this group: row ids (not for dense) and
                 // values (sparse, dense), once for the gradient, again for an update
-                const long long cb = nn * ((dense ? 0 : 4) + (ind ? 0 : 8));
+                const long long cb = nnc * ((dense ? 0 : 4) + (ind ? 0 : 8));
                 n_idx += (unsigned long long)(cb * (1 + (upd ? 1 : 0)));
             }
             // ---- updateXBeta for my rows
@@ -503,18 +591,18 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                             if (A.strat[kp] == s) continue;
                         }
                         double acc = dg[(size_t)s * G + fl];
-                        int q = e;
+                        int qe = e;
                         int kq = k;
                         do {
-                            const T x = ind ? T(1) : (T)__ldg(cval + q);
-                            T* p = xbg + (size_t)kq * G + fl;
-                            const T old = *p;
+                            const T x = ind ? T(1) : (T)__ldg(cval + qe);
+                            T* pp = xbg + (size_t)kq * G + fl;
+                            const T old = *pp;
                             const T nv = old + d * x;
-                            *p = nv;
+                            *pp = nv;
                             acc += (double)fexp(nv) - (double)fexp(old);
-                            ++q;
-                            if (q >= e1) break;
-                            kq = dense ? q : __ldg(cidx + q);
+                            ++qe;
+                            if (qe >= e1) break;
+                            kq = dense ? qe : __ldg(cidx + qe);
                         } while (A.strat[kq] == s);
                         dg[(size_t)s * G + fl] = acc;
                     }
@@ -522,11 +610,12 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             }
             __syncthreads();
             par ^= 1;
+            ++q;
         }
         // chunk done: rank 0 writes the group's beta and trust regions back
         if (rank == 0)
-            for (int q = threadIdx.x; q < jn * G; q += kBT) {
-                const int ff = q / jn, jj = q % jn;
+            for (int qq = threadIdx.x; qq < jn * G; qq += kBT) {
+                const int ff = qq / jn, jj = qq % jn;
                 const size_t o = (size_t)(fg + ff) * A.J + j0 + jj;
                 A.beta[o] = c_beta[jj][ff];
                 A.hdelta[o] = c_hd[jj][ff];
@@ -568,7 +657,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         __syncthreads();
         if (threadIdx.x == 0) {
             int all = 1;
-            for (int q = 0; q < G; ++q) all &= s_done[q];
+            for (int f = 0; f < G; ++f) all &= s_done[f];
             s_all_done = all;
         }
         __syncthreads();
@@ -766,12 +855,66 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
 
 }  // namespace
 
+
+// Conflict-free runs (see k_batch): walk the columns in order and open a new
+// run whenever the next short column shares a row with the open run, the run
+// is full, a chunk boundary is reached, or the column is not short (dense,
+// fixed, or more than `cap` entries in some CTA's rows).  run_len[j] is the
+// run's length at its first column, 0 inside a run, 1 for a column alone.
+static std::vector<int> plan_runs(const Dataset& ds, const std::vector<int>& rpart, const std::vector<int>& fixb,
+                                  int cap, bool allow) {
+    const int J = ds.J, C = (int)rpart.size() - 1;
+    std::vector<int> run_len(J, 1);
+    if (!allow) return run_len;
+    std::vector<int> stamp(ds.K, -1);
+    int run_id = -1, start = -1, len = 0;
+    auto close = [&] {
+        if (start >= 0) run_len[start] = len;
+        start = -1;
+        len = 0;
+    };
+    std::vector<int> cnt(C);
+    for (int j = 0; j < J; ++j) {
+        if (j % kChunk == 0) close();
+        const int f = ds.fmt[j];
+        bool small = (f == CYC_SPARSE || f == CYC_INDICATOR) && !fixb[j];
+        const int* rows = ds.h_idx.data() + ds.col_ptr[j];
+        const long long n = ds.col_ptr[j + 1] - ds.col_ptr[j];
+        if (small) {
+            std::fill(cnt.begin(), cnt.end(), 0);
+            int r = 0;
+            for (long long e = 0; e < n && small; ++e) {
+                while (r < C - 1 && rows[e] >= rpart[r + 1]) ++r;
+                if (++cnt[r] > cap) small = false;
+            }
+        }
+        if (!small) {
+            close();
+            run_len[j] = 1;
+            continue;
+        }
+        bool conflict = false;
+        if (start >= 0)
+            for (long long e = 0; e < n && !conflict; ++e) conflict = (stamp[rows[e]] == run_id);
+        if (start < 0 || conflict || len == kRunMax) {
+            close();
+            start = j;
+            ++run_id;
+        }
+        for (long long e = 0; e < n; ++e) stamp[rows[e]] = run_id;
+        run_len[j] = 0;
+        ++len;
+    }
+    close();
+    return run_len;
+}
+
 template <class T, int MODEL, int G, int WM>
 static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
-    const size_t dyn = kStage * (sizeof(int) + sizeof(T));
+    const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * (sizeof(int) + sizeof(T));
     CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     cfg.dynamicSmemBytes = dyn;
     cfg.stream = stream;
@@ -806,7 +949,7 @@ struct BatchRunner {
     cudaStream_t stream;
     int F, G, ngroups, Fp, C;
     std::vector<int> rpart;
-    DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag;
+    DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag, d_runlen;
     DevBuf<T> d_xb, d_w;
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
@@ -864,6 +1007,20 @@ struct BatchRunner {
         std::vector<double> var(Fp, 1.0);
         for (int f = 0; f < F; ++f) var[f] = specs[f].variance;
         d_fixb.alloc(J); d_ptype.alloc(J); d_active.alloc(Fp); d_var.alloc(Fp);
+        {
+            const std::pair<int, int> key(C, G);
+            const std::vector<int>* plan = nullptr;
+            for (auto& kv : ds.run_plans)
+                if (kv.first == key) plan = &kv.second;
+            if (!plan) {
+                ds.run_plans.emplace_back(key, plan_runs(ds, rpart, fixb, (32 / G) * kRunItems,
+                                                         model_independent(ds.model)));
+                plan = &ds.run_plans.back().second;
+            }
+            d_runlen.alloc(J);
+            CYC_CHECK_CUDA(cudaMemcpyAsync(d_runlen.get(), plan->data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
+            CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+        }
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixb.get(), fixb.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_ptype.get(), pt.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_active.get(), act.data(), Fp * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -940,6 +1097,7 @@ struct BatchRunner {
         a.hdelta = d_hdelta.get(); a.variance = d_var.get(); a.llfixed = d_llfixed.get(); a.active = d_active.get();
         a.fold = d_fold ? d_fold8.get() : nullptr;
         a.fitfold = d_fold ? d_fitfold.get() : nullptr;
+        a.run_len = d_runlen.get();
         a.conv = ctl.convergence_type; a.tol = tol; a.max_iter = ctl.max_iterations;
         a.out_iter = d_iter.get(); a.out_flag = d_flag.get(); a.out_obj = d_obj.get(); a.counters = d_counters.get();
         cudaEvent_t e0, e1;

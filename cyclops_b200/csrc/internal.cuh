@@ -169,6 +169,9 @@ struct Dataset {
     DevBuf<int> d_row_col;
     DevBuf<double> d_row_val;
 
+    // conflict-free column runs of the batched solver, cached per (cluster size, fits per group)
+    std::vector<std::pair<std::pair<int, int>, std::vector<int>>> run_plans;
+
     long long col_len(int j) const {
         return (fmt[j] == CYC_DENSE || fmt[j] == CYC_INTERCEPT) ? K : col_ptr[j + 1] - col_ptr[j];
     }
