@@ -68,7 +68,14 @@ struct BatchArgs {
     const int* active;            // [F] 0 for padding fits
     const signed char* fold;      // K fold id per row (CV grid) or null
     const int* fitfold;           // [F] held-out fold of each fit (CV grid)
-    const int* run_len;           // J: columns in the run starting here (1 = alone), 0 inside a run
+    const int* run_len;           // J: columns in the batch starting here (1 = alone), 0 inside a batch
+    const int* run_lvl;           // J: level of the column within its batch
+    const int* run_dr0;           // J: first shared row of the batch starting here (into drow)
+    const int* run_nd;            // J: shared rows of that batch
+    const int* drow;              // shared row ids
+    const int* de_ptr;            // J+1: entries of column j on shared rows
+    const int* de_d;              // shared-row slot | (column within the batch << 8)
+    const int* de_e;              // entry position within the column
     int conv;
     double tol;
     int max_iter;
@@ -164,16 +171,227 @@ __device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp,
 // ModelSpecifics.h:540-568, 1508-1543); the logistic probability is formed as
 // 1 / (1 + exp(-xb)), which equals exb / (1 + exb) without overflowing
 template <class T, int MODEL>
-__device__ __forceinline__ void row_gh(T v, T x, T wt, bool ind, Kahan<T>& ag, Kahan<T>& ah) {
+__device__ __forceinline__ void row_terms(T v, T x, T wt, bool ind, T& gi, T& hi) {
     if (MODEL == CYC_LR) {
         const T p = T(1) / (T(1) + fexp(-v));
-        const T gi = p * x;
-        ag.add(wt * gi);
-        ah.add(wt * (ind ? gi * (T(1) - gi) : x * x * p * (T(1) - p)));
+        const T g1 = p * x;
+        gi = wt * g1;
+        hi = wt * (ind ? g1 * (T(1) - g1) : x * x * p * (T(1) - p));
     } else {
         const T n1 = fexp(v) * x;
-        ag.add(wt * n1);
-        ah.add(wt * (ind ? n1 : n1 * x));
+        gi = wt * n1;
+        hi = wt * (ind ? n1 : n1 * x);
+    }
+}
+
+template <class T, int MODEL>
+__device__ __forceinline__ void row_gh(T v, T x, T wt, bool ind, Kahan<T>& ag, Kahan<T>& ah) {
+    T gi, hi;
+    row_terms<T, MODEL>(v, x, wt, ind, gi, hi);
+    ag.add(gi);
+    ah.add(hi);
+}
+
+// xb + delta * x as one fused multiply-add, the same wherever a batch
+// replays an update (the owning CTA and every CTA's copy of a shared row)
+__device__ __forceinline__ float upd_fma(float d, float x, float v) { return __fmaf_rn(d, x, v); }
+__device__ __forceinline__ double upd_fma(double d, double x, double v) { return __fma_rn(d, x, v); }
+
+// N consecutive values of one row of the [K][G] layout (16-byte aligned
+// when N * sizeof(T) is a multiple of 16)
+template <class T, int N>
+__device__ __forceinline__ void load_row(const T* p, T (&v)[N]) {
+    if constexpr (sizeof(T) == 4 && N % 4 == 0) {
+        #pragma unroll
+        for (int i = 0; i < N / 4; ++i) {
+            const float4 q = reinterpret_cast<const float4*>(p)[i];
+            v[4 * i] = q.x; v[4 * i + 1] = q.y; v[4 * i + 2] = q.z; v[4 * i + 3] = q.w;
+        }
+    } else if constexpr (sizeof(T) == 8 && N % 2 == 0) {
+        #pragma unroll
+        for (int i = 0; i < N / 2; ++i) {
+            const double2 q = reinterpret_cast<const double2*>(p)[i];
+            v[2 * i] = q.x; v[2 * i + 1] = q.y;
+        }
+    } else {
+        #pragma unroll
+        for (int i = 0; i < N; ++i) v[i] = p[i];
+    }
+}
+
+template <class T, int N>
+__device__ __forceinline__ void store_row(T* p, const T (&v)[N]) {
+    if constexpr (sizeof(T) == 4 && N % 4 == 0) {
+        #pragma unroll
+        for (int i = 0; i < N / 4; ++i)
+            reinterpret_cast<float4*>(p)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    } else if constexpr (sizeof(T) == 8 && N % 2 == 0) {
+        #pragma unroll
+        for (int i = 0; i < N / 2; ++i) reinterpret_cast<double2*>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    } else {
+        #pragma unroll
+        for (int i = 0; i < N; ++i) p[i] = v[i];
+    }
+}
+
+// Thread-per-row layout of one group's G fits: a row's linear predictors
+// are split into TPR parts of FPT fits (16 bytes in FP32, one 32-byte sector
+// in FP64), and each thread holds R rows' parts at a time.
+template <class T, int G, int WM>
+struct RowLayout {
+    static constexpr int FPT = (G % 4 == 0) ? 4 : G;
+    static constexpr int TPR = G / FPT;
+    static constexpr int R = 2;
+};
+
+// Warp sum of per-lane (g[f], h[f]), f < FPT (the lane's part lane % TPR of
+// the fits), by a butterfly reduce-scatter: each level halves the values a
+// lane carries (2 FPT values: FPT + FPT/2 + ... + 1 shuffles per lane, then
+// one more).  Returns the sum of this lane's value and sets `fit` (within the
+// group) and `is_h`; `holder` marks one of the two lanes that hold it.
+// Fixed order: deterministic.
+template <int FPT, int TPR>
+__device__ __forceinline__ double warp_reduce_rows(const double (&g)[FPT], const double (&h)[FPT], int& fit,
+                                                   bool& is_h, bool& holder) {
+    constexpr unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    double v[2 * FPT];
+    #pragma unroll
+    for (int f = 0; f < FPT; ++f) { v[f] = g[f]; v[FPT + f] = h[f]; }
+    int vi = 0;
+    #pragma unroll
+    for (int half = FPT, off = 16; half >= 1; half >>= 1, off >>= 1) {
+        const bool up = (lane & off) != 0;
+        #pragma unroll
+        for (int i = 0; i < half; ++i) {
+            const double send = up ? v[i] : v[i + half];
+            const double keep = up ? v[i + half] : v[i];
+            v[i] = keep + __shfl_xor_sync(full, send, off);
+        }
+        vi += up ? half : 0;
+    }
+    v[0] += __shfl_xor_sync(full, v[0], TPR);
+    fit = (lane % TPR) * FPT + (vi % FPT);
+    is_h = vi >= FPT;
+    holder = (lane & TPR) == 0;
+    return v[0];
+}
+
+// Block sum of per-thread (g, h) parts into out[f] = (g, h): warp sums, then
+// the warps' sums in warp order.  Deterministic.
+template <int G, int FPT, int TPR>
+__device__ __forceinline__ void block_reduce_rows(const double (&g)[FPT], const double (&h)[FPT], double2* out,
+                                                  double* scr /* [kBT/32][2G] */) {
+    const int wid = threadIdx.x >> 5;
+    int fit;
+    bool is_h, holder;
+    const double v = warp_reduce_rows<FPT, TPR>(g, h, fit, is_h, holder);
+    if (holder) scr[wid * 2 * G + (is_h ? G : 0) + fit] = v;
+    __syncthreads();
+    if (threadIdx.x < 2 * G) {
+        double s = 0.0;
+        for (int q = 0; q < kBT / 32; ++q) s += scr[q * 2 * G + threadIdx.x];
+        if (threadIdx.x < G) out[threadIdx.x].x = s;
+        else out[threadIdx.x - G].y = s;
+    }
+    __syncthreads();
+}
+
+// Where the entries of one column in this CTA's rows come from: positions
+// [e0, e1) of the column (row ids `cidx`, values `cval`), or, when staged in
+// shared memory, sidx / sx [0, e1 - e0).
+template <class T>
+struct ColRows {
+    const int* cidx;
+    const double* cval;
+    const int* sidx;
+    const T* sx;
+    int e0, e1;
+    bool dense, ind;
+    __device__ __forceinline__ void get(int e, int& k, T& x) const {
+        if (e >= e1) { k = -1; x = T(1); return; }
+        if (sidx) {
+            k = sidx[e - e0];
+            x = ind ? T(1) : sx[e - e0];
+        } else {
+            k = dense ? e : __ldg(cidx + e);
+            x = ind ? T(1) : (T)__ldg(cval + e);
+        }
+    }
+};
+
+// Gradient and Hessian terms of the group's fits over the entries of a column
+// (an independent-rows model), by the STRIDE threads t0 = 0 .. STRIDE-1:
+// thread t takes rows t / TPR, t / TPR + STRIDE / TPR, ... and fits part
+// t % TPR of each, loaded as one vector.  `wmask[fold]` holds the fits that
+// train on rows of that fold (CV grid); `done` the fits that have converged
+// (skipped).
+template <class T, int MODEL, int G, int WM, int STRIDE>
+__device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xbg, const T* wg,
+                                        const signed char* fold, const unsigned char* wmask, unsigned done,
+                                        double (&g)[RowLayout<T, G, WM>::FPT], double (&h)[RowLayout<T, G, WM>::FPT]) {
+    using Lay = RowLayout<T, G, WM>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
+    const int f0 = (t0 % TPR) * FPT;
+    const unsigned dn = done >> f0;
+    Kahan<T> ag[FPT], ah[FPT];
+    for (int base = c.e0 + t0 / TPR; base < c.e1; base += R * RS) {
+        int k[R];
+        T x[R];
+        #pragma unroll
+        for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+        T v[R][FPT], w[R][FPT];
+        unsigned wm[R];
+        #pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (k[r] >= 0) {
+                load_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
+                if (WM == 0) load_row<T, FPT>(wg + (size_t)k[r] * G + f0, w[r]);
+                else wm[r] = (unsigned)wmask[(int)__ldg(fold + k[r])] >> f0;
+            } else {
+                wm[r] = 0u;
+                #pragma unroll
+                for (int f = 0; f < FPT; ++f) { v[r][f] = T(0); w[r][f] = T(0); }
+            }
+        }
+        #pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (k[r] < 0) continue;
+            #pragma unroll
+            for (int f = 0; f < FPT; ++f) {
+                if ((dn >> f) & 1u) continue;
+                const T wt = (WM == 1) ? (((wm[r] >> f) & 1u) ? T(1) : T(0)) : w[r][f];
+                row_gh<T, MODEL>(v[r][f], x[r], wt, c.ind, ag[f], ah[f]);
+            }
+        }
+    }
+    #pragma unroll
+    for (int f = 0; f < FPT; ++f) { g[f] = ag[f].value(); h[f] = ah[f].value(); }
+}
+
+// updateXBeta over the entries of a column by the STRIDE threads t0 (same
+// split as rows_gh)
+template <class T, int G, int WM, int STRIDE>
+__device__ __forceinline__ void rows_update(const ColRows<T>& c, int t0, T* xbg, const T (&d)[G]) {
+    using Lay = RowLayout<T, G, WM>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
+    const int f0 = (t0 % TPR) * FPT;
+    for (int base = c.e0 + t0 / TPR; base < c.e1; base += R * RS) {
+        int k[R];
+        T x[R];
+        #pragma unroll
+        for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+        T v[R][FPT];
+        #pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (k[r] >= 0) load_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
+        #pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (k[r] < 0) continue;
+            #pragma unroll
+            for (int f = 0; f < FPT; ++f) v[r][f] = upd_fma(d[f0 + f], x[r], v[r][f]);
+            store_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
+        }
     }
 }
 
@@ -198,6 +416,11 @@ constexpr int kStage = 4096;
 constexpr int kRunMax = kBT / 32;
 // entries per slot of a run column (a warp has 32/G slots)
 constexpr int kRunItems = 8;
+// With G = 8 fits per group (independent-rows models) a batch may share rows
+// between its columns: at most kDirtyMax such rows, replayed serially (see
+// k_batch).  Columns of at most kBatchCap entries in every CTA's rows join.
+constexpr int kDirtyMax = 32;
+constexpr int kBatchCap = 256;
 
 template <class T, int MODEL, int G, int WM>
 __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
@@ -207,6 +430,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     const int grp = blockIdx.x / C;
     const int r0 = A.rpart[rank], r1 = A.rpart[rank + 1];
     const bool grouped = (MODEL == CYC_CLR || MODEL == CYC_CPR);
+    // independent rows, 8 fits per group: columns stream thread per row (all
+    // fits of a row by vector loads) and short columns go in batches
+    constexpr bool kRowStream = (G == 8) && !(MODEL == CYC_CLR || MODEL == CYC_CPR);
+    using Lay = RowLayout<T, G, WM>;
     // strata of my rows (partition boundaries are stratum starts); none if my range is empty
     const int s0 = (grouped && r0 < r1) ? A.strat[r0] : 0;
     const int s1 = (grouped && r0 < r1) ? (r1 >= A.K ? A.S : A.strat[r1]) : 0;
@@ -236,8 +463,17 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     __shared__ int s_flag[G];
     __shared__ int s_iter[G];
     __shared__ int s_all_done;
+    // CV grid: the fits of the group that train on rows of fold v (bit f)
+    __shared__ unsigned char s_wmask[128];
+    // the open batch: its entries on shared rows (slot, value) per column, and
+    // the shared rows' fold masks
+    __shared__ int s_bde_ptr[kRunMax + 1];
+    __shared__ int s_bde_d[kRunMax * kDirtyMax];
+    __shared__ double s_bde_x[kRunMax * kDirtyMax];
+    __shared__ unsigned char s_dwm[kDirtyMax];
     // the current chunk of coordinates
     __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk], c_run[kChunk];
+    __shared__ int c_lvl[kChunk];
     __shared__ long long c_cp[kChunk], c_vp[kChunk];
     __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
     __shared__ int c_sq[kChunk + 1];       // staged coordinates in order
@@ -251,6 +487,11 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     double (*c_xjy)[G] = reinterpret_cast<double (*)[G]>(dyn_smem + 2 * kChunk * G * sizeof(double));
     int* s_sidx = reinterpret_cast<int*>(dyn_smem + 3 * kChunk * G * sizeof(double));
     T* s_sx = reinterpret_cast<T*>(dyn_smem + 3 * kChunk * G * sizeof(double) + kStage * sizeof(int));
+    // shared rows of the open batch: as pushed by their owners (by parity),
+    // the working copy of the serial replay, and their weights
+    T (*s_dst)[kDirtyMax][G] = reinterpret_cast<T (*)[kDirtyMax][G]>(s_sx + kStage);
+    T (*s_dcur)[G] = reinterpret_cast<T (*)[G]>(s_sx + kStage + 2 * kDirtyMax * G);
+    T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_sx + kStage + 3 * kDirtyMax * G);
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
     if (threadIdx.x < G) {
@@ -258,6 +499,14 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         s_done[threadIdx.x] = A.active[f] ? 0 : 1;
         s_flag[threadIdx.x] = CYC_SUCCESS;
         s_iter[threadIdx.x] = 0;
+    }
+    if (WM == 1 && threadIdx.x < 128) {
+        unsigned m = 0;
+        for (int f = 0; f < G; ++f) {
+            const int ff = A.fitfold[fg + f];
+            if (ff >= -1 && ff != (int)threadIdx.x) m |= 1u << f;
+        }
+        s_wmask[threadIdx.x] = (unsigned char)m;
     }
     __syncthreads();
 
@@ -284,6 +533,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     }
     __syncthreads();
     bool done_l = s_done[fl] != 0;   // this thread's fit lane has converged
+    unsigned done_m = 0;             // all converged fits of the group (bit f)
+    for (int f = 0; f < G; ++f) done_m |= (s_done[f] ? 1u : 0u) << f;
     const double var_l = A.variance[fg + fl];
 
     unsigned long long n_grad = 0, n_upd = 0, n_steps = 0, n_idx = 0;
@@ -291,6 +542,37 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     for (int it = 1; it <= A.max_iter; ++it) {
       for (int j0 = 0; j0 < A.J; j0 += kChunk) {
         const int jn = min(kChunk, A.J - j0);
+        // ccdUpdateBeta for fit f of chunk coordinate qq from its (g, h) summed
+        // over the cluster; called by the thread whose fit lane is f
+        auto coord_step = [&](int qq, int f, double g, double h) -> double {
+            g -= c_xjy[qq][f];                             // :1181-1183
+            if (s_done[f]) return 0.0;
+            if (h < 0.0) { g = 0.0; h = 0.0; }             // :1407-1410
+            const double b = c_beta[qq][f];
+            double hd = c_hd[qq][f];
+            double dl = prior_delta(c_pt[qq], var_l, b, g, h);
+            dl = apply_bounds(&hd, dl);
+            c_hd[qq][f] = hd;
+            if (dl != 0.0) c_beta[qq][f] = b + dl;
+            return dl;
+        };
+        // work counters of L columns from chunk coordinate q0 (deltas in s_dr)
+        auto count_run = [&](int q0, int L) {
+            int act = 0;
+            for (int f = 0; f < G; ++f) act += !s_done[f];
+            for (int w = 0; w < L; ++w) {
+                int upd = 0;
+                for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
+                const int j = j0 + q0 + w, fm = c_fmt[q0 + w];
+                const bool dn = (fm == CYC_DENSE || fm == CYC_INTERCEPT);
+                const bool in = (fm == CYC_INDICATOR || fm == CYC_INTERCEPT);
+                const long long nn = dn ? A.K : A.col_ptr[j + 1] - A.col_ptr[j];
+                n_grad += (unsigned long long)(act * nn);
+                n_upd += (unsigned long long)(upd * nn);
+                n_steps += act;
+                n_idx += (unsigned long long)(nn * ((dn ? 0 : 4) + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
+            }
+        };
         // ---- stage the chunk (coalesced)
         for (int q = threadIdx.x; q < jn; q += kBT) {
             const int j = j0 + q;
@@ -299,6 +581,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             c_fix[q] = A.fixb[j];
             c_pt[q] = A.ptype[j];
             c_run[q] = A.run_len[j];
+            c_lvl[q] = A.run_lvl[j];
             c_cp[q] = A.col_ptr[j];
             c_vp[q] = A.val_ptr[j];
             const bool dn = (f0 == CYC_DENSE || f0 == CYC_INTERCEPT);
@@ -352,265 +635,419 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         while (q < jn) {
             const int L = c_run[q];
             if (c_fix[q] || L <= 0) { ++q; continue; }
+            if constexpr (kRowStream) {
             if (L > 1) {
-                // ---- a run of L conflict-free short columns: warp w takes column q + w
-                const int qq = q + warp;
-                int kk[kRunItems];
-                T vv[kRunItems], xx[kRunItems];
-                bool ind = true;
+                // ---- a batch of L short columns (planned: plan_runs); warp w takes column q + w
+                const int jb = j0 + q;
+                const int nd = A.run_nd[jb], dr0 = A.run_dr0[jb];
+                const int de0 = A.de_ptr[jb], nde = A.de_ptr[jb + L] - de0;
+                // rows shared inside the batch: their owners push them (all G fits)
+                // into every CTA; the weights of those rows are kept locally
+                for (int t = threadIdx.x; t < nd * G; t += kBT) {
+                    const int d = t / G, f = t % G;
+                    const int k = __ldg(A.drow + dr0 + d);
+                    if (k >= r0 && k < r1) {
+                        const T v = xbg[(size_t)k * G + f];
+                        for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_dst[par][d][f], r) = v;
+                    }
+                    if (WM == 1) {
+                        if (f == 0) s_dwm[d] = s_wmask[(int)__ldg(A.fold + k)];
+                    } else {
+                        s_dw[d][f] = wg[(size_t)k * G + f];
+                    }
+                }
+                if (threadIdx.x <= L) s_bde_ptr[threadIdx.x] = A.de_ptr[jb + threadIdx.x] - de0;
+                for (int t = threadIdx.x; t < nde; t += kBT) {
+                    const int dd = __ldg(A.de_d + de0 + t);
+                    const int qw = q + (dd >> 8);
+                    s_bde_d[t] = dd & 0xff;
+                    s_bde_x[t] = (c_fmt[qw] == CYC_SPARSE) ? __ldg(A.val + c_vp[qw] + __ldg(A.de_e + de0 + t)) : 1.0;
+                }
+                // gradient partials of every column from the state at the batch's start
                 if (warp < L) {
-                    const int fmt = c_fmt[qq];
-                    ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
-                    const int e0 = c_e0[qq], n = c_e1[qq] - e0, so = c_off[qq];
-                    const int* cidx = A.idx + c_cp[qq];
-                    const double* cval = A.val + c_vp[qq];
-                    #pragma unroll
-                    for (int r = 0; r < kRunItems; ++r) {
-                        const int e = wslot + r * WS;
-                        const bool ok = e < n && !done_l;
-                        kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : __ldg(cidx + e0 + e));
-                        xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
+                    const int qq = q + warp, so = c_off[qq];
+                    const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
+                                        so >= 0 ? s_sx + so : nullptr, c_e0[qq], c_e1[qq], false,
+                                        c_fmt[qq] == CYC_INDICATOR};
+                    double g[Lay::FPT], h[Lay::FPT];
+                    rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, g, h);
+                    int fit;
+                    bool is_h, holder;
+                    const double v = warp_reduce_rows<Lay::FPT, Lay::TPR>(g, h, fit, is_h, holder);
+                    if (holder) {
+                        double* dst = is_h ? &s_part[par][rank][warp][fit].y : &s_part[par][rank][warp][fit].x;
+                        for (int r = 0; r < C; ++r) *cluster.map_shared_rank(dst, r) = v;
                     }
-                    T ww[kRunItems];
-                    #pragma unroll
-                    for (int r = 0; r < kRunItems; ++r) {
-                        vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
-                        ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
-                    }
-                    Kahan<T> ag, ah;
-                    #pragma unroll
-                    for (int r = 0; r < kRunItems; ++r)
-                        if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
-                    double g = ag.value(), h = ah.value();
-                    for (int o = G; o < 32; o <<= 1) {
-                        g += __shfl_xor_sync(0xffffffffu, g, o);
-                        h += __shfl_xor_sync(0xffffffffu, h, o);
-                    }
-                    if (lane < G)
-                        for (int r = 0; r < C; ++r)
-                            *cluster.map_shared_rank(&s_part[par][rank][warp][lane], r) = make_double2(g, h);
                 }
                 if (C > 1) cluster.sync(); else __syncthreads();
-                double dl = 0.0;
-                if (warp < L) {
-                    if (lane < G) {
-                        double g = 0.0, h = 0.0;
-                        for (int r = 0; r < C; ++r) {
-                            const double2 pp = s_part[par][r][warp][lane];
-                            g += pp.x;
-                            h += pp.y;
-                        }
-                        g -= c_xjy[qq][lane];                     // :1181-1183
-                        if (!s_done[lane]) {
-                            if (h < 0.0) { g = 0.0; h = 0.0; }    // ccdUpdateBeta :1407-1410
-                            const double b = c_beta[qq][lane];
-                            double hd = c_hd[qq][lane];
-                            dl = prior_delta(c_pt[qq], var_l, b, g, h);
-                            dl = apply_bounds(&hd, dl);
-                            c_hd[qq][lane] = hd;
-                            if (dl != 0.0) c_beta[qq][lane] = b + dl;
-                        }
-                        s_dr[warp][lane] = dl;
-                    }
-                    dl = __shfl_sync(0xffffffffu, dl, fl);
-                    if (dl != 0.0) {
-                        const T d = (T)dl;
-                        #pragma unroll
-                        for (int r = 0; r < kRunItems; ++r)
-                            if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
-                    }
-                }
+                // the serial steps, replayed identically in every CTA: level by
+                // level, a column's (g, h) is its partials plus, for each of its
+                // entries on a shared row, the change of that row's terms since
+                // the batch's start (zero unless an earlier column moved it)
+                for (int t = threadIdx.x; t < nd * G; t += kBT) s_dcur[t / G][t % G] = s_dst[par][t / G][t % G];
                 __syncthreads();
-                if (rank == 0 && threadIdx.x == 0) {
-                    int act = 0;
-                    for (int f = 0; f < G; ++f) act += !s_done[f];
-                    for (int w = 0; w < L; ++w) {
-                        int upd = 0;
-                        for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
-                        const long long nn = A.col_ptr[j0 + q + w + 1] - A.col_ptr[j0 + q + w];
-                        const bool in = (c_fmt[q + w] == CYC_INDICATOR);
-                        n_grad += (unsigned long long)(act * nn);
-                        n_upd += (unsigned long long)(upd * nn);
-                        n_steps += act;
-                        n_idx += (unsigned long long)(nn * (4 + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
+                int nlev = 1;
+                for (int w = 0; w < L; ++w) nlev = max(nlev, c_lvl[q + w]);
+                const int fw = lane % G, sl = lane / G;    // (fit, entry slot) inside a warp
+                for (int lv = 1; lv <= nlev; ++lv) {
+                    if (warp < L && c_lvl[q + warp] == lv) {
+                        const int qq = q + warp;
+                        const bool ind = c_fmt[qq] == CYC_INDICATOR;
+                        const int i0 = s_bde_ptr[warp], i1 = s_bde_ptr[warp + 1];
+                        double gc = 0.0, hc = 0.0;
+                        if (!((done_m >> fw) & 1u))
+                            for (int i = i0 + sl; i < i1; i += 32 / G) {
+                                const int d = s_bde_d[i];
+                                const T x = (T)s_bde_x[i];
+                                const T wt = (WM == 1) ? (((s_dwm[d] >> fw) & 1u) ? T(1) : T(0)) : s_dw[d][fw];
+                                T g1, h1, g0, h0;
+                                row_terms<T, MODEL>(s_dcur[d][fw], x, wt, ind, g1, h1);
+                                row_terms<T, MODEL>(s_dst[par][d][fw], x, wt, ind, g0, h0);
+                                gc += (double)g1 - (double)g0;
+                                hc += (double)h1 - (double)h0;
+                            }
+                        for (int o = G; o < 32; o <<= 1) {
+                            gc += __shfl_xor_sync(0xffffffffu, gc, o);
+                            hc += __shfl_xor_sync(0xffffffffu, hc, o);
+                        }
+                        double dl = 0.0;
+                        if (lane < G) {
+                            double g = 0.0, h = 0.0;
+                            for (int r = 0; r < C; ++r) {
+                                const double2 pp = s_part[par][r][warp][lane];
+                                g += pp.x;
+                                h += pp.y;
+                            }
+                            g += gc;
+                            h += hc;
+                            dl = coord_step(qq, lane, g, h);
+                            s_dr[warp][lane] = dl;
+                        }
+                        dl = __shfl_sync(0xffffffffu, dl, fw);
+                        if (dl != 0.0)
+                            for (int i = i0 + sl; i < i1; i += 32 / G) {
+                                const int d = s_bde_d[i];
+                                s_dcur[d][fw] = upd_fma((T)dl, (T)s_bde_x[i], s_dcur[d][fw]);
+                            }
                     }
+                    __syncthreads();
                 }
+                // updateXBeta of my rows, level by level (columns of one level share no row)
+                for (int lv = 1; lv <= nlev; ++lv) {
+                    if (warp < L && c_lvl[q + warp] == lv) {
+                        const int qq = q + warp, so = c_off[qq];
+                        T dd[G];
+                        bool any = false;
+                        #pragma unroll
+                        for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[warp][f]; any |= (s_dr[warp][f] != 0.0); }
+                        if (any) {
+                            const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
+                                                so >= 0 ? s_sx + so : nullptr, c_e0[qq], c_e1[qq], false,
+                                                c_fmt[qq] == CYC_INDICATOR};
+                            rows_update<T, G, WM, 32>(cr, lane, xbg, dd);
+                        }
+                    }
+                    __syncthreads();
+                }
+                if (rank == 0 && threadIdx.x == 0) count_run(q, L);
                 par ^= 1;
                 q += L;
                 continue;
             }
-            // ---- a single column
-            const int fmt = c_fmt[q];
-            const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
-            const bool ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
-            const int* cidx = A.idx + c_cp[q];
-            const double* cval = A.val + c_vp[q];
-            const int e0 = c_e0[q], e1 = c_e1[q];
-            const bool regpath = !grouped && (e1 - e0) <= kRegItems * NS;
-            Kahan<T> ag, ah;
-            int kk[kRegItems];
-            T vv[kRegItems], xx[kRegItems];
-            if (regpath) {
-                const int so = c_off[q];
-                #pragma unroll
-                for (int r = 0; r < kRegItems; ++r) {
-                    const int e = slot + r * NS;                 // relative to e0
-                    const bool ok = e < e1 - e0 && !done_l;
-                    kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : (dense ? e0 + e : __ldg(cidx + e0 + e)));
-                    xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
-                }
-                T ww[kRegItems];
-                #pragma unroll
-                for (int r = 0; r < kRegItems; ++r) {
-                    vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
-                    ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
-                }
-                #pragma unroll
-                for (int r = 0; r < kRegItems; ++r)
-                    if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
-            } else if (!grouped) {
-                if (!done_l) {
-                    // long column: batches of kRegItems entries per thread, loads first
-                    for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
-                        int k2[kRegItems];
-                        T x2[kRegItems], v2[kRegItems], w2[kRegItems];
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r) {
-                            const int e = base + r * NS;
-                            k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
-                            x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
-                        }
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r) {
-                            v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
-                            w2[r] = k2[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, k2[r], G, fl) : T(0);
-                        }
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r)
-                            if (k2[r] >= 0) row_gh<T, MODEL>(v2[r], x2[r], w2[r], ind, ag, ah);
+            // ---- a single column, thread per row (all G fits)
+            {
+                const int fmt = c_fmt[q], so = c_off[q];
+                const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
+                const ColRows<T> cr{A.idx + c_cp[q], A.val + c_vp[q], so >= 0 ? s_sidx + so : nullptr,
+                                    so >= 0 ? s_sx + so : nullptr, c_e0[q], c_e1[q], dense,
+                                    fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT};
+                double g[Lay::FPT], h[Lay::FPT];
+                rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, g, h);
+                block_reduce_rows<G, Lay::FPT, Lay::TPR>(g, h, s_red, reinterpret_cast<double*>(s_scr));
+                if (threadIdx.x < G)
+                    for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
+                if (C > 1) cluster.sync(); else __syncthreads();
+                if (threadIdx.x < G) {
+                    double gs = 0.0, hs = 0.0;
+                    for (int r = 0; r < C; ++r) {
+                        const double2 pp = s_part[par][r][0][threadIdx.x];
+                        gs += pp.x;
+                        hs += pp.y;
                     }
+                    s_dr[0][threadIdx.x] = coord_step(q, threadIdx.x, gs, hs);
                 }
+                __syncthreads();
+                T dd[G];
+                bool any = false;
+                #pragma unroll
+                for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[0][f]; any |= (s_dr[0][f] != 0.0); }
+                if (rank == 0 && threadIdx.x == 0) count_run(q, 1);
+                if (any) rows_update<T, G, WM, kBT>(cr, threadIdx.x, xbg, dd);
+                __syncthreads();
+                par ^= 1;
+                ++q;
+            }
             } else {
-                for (int e = e0 + slot; e < e1; e += NS) {
-                    const int k = dense ? e : __ldg(cidx + e);
-                    const int s = A.strat[k];
-                    if (e > e0) {
-                        const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
-                        if (A.strat[kp] == s) continue;
-                    }
-                    T n1 = 0, n2 = 0;
-                    int qe = e;
-                    int kq = k;
-                    do {                                  // the run of stratum s in this column
-                        const T x = ind ? T(1) : (T)__ldg(cval + qe);
-                        const T ex = fexp(xbg[(size_t)kq * G + fl]);
-                        n1 += ex * x;
-                        if (!ind) n2 += ex * x * x;
-                        ++qe;
-                        if (qe >= e1) break;
-                        kq = dense ? qe : __ldg(cidx + qe);
-                    } while (A.strat[kq] == s);
-                    const double d = dg[(size_t)s * G + fl];
-                    const double nwv = ng[(size_t)s * G + fl];
-                    const double t = (double)n1 / d;        // ConditionalLogisticRegression::incrementGradientAndHessian
-                    const double gg = nwv * t;
-                    ag.add((T)gg);
-                    ah.add((T)(ind ? gg * (1.0 - t) : nwv * ((double)n2 / d - t * t)));
-                }
+              if (L > 1) {
+                  // ---- a run of L conflict-free short columns: warp w takes column q + w
+                  const int qq = q + warp;
+                  int kk[kRunItems];
+                  T vv[kRunItems], xx[kRunItems];
+                  bool ind = true;
+                  if (warp < L) {
+                      const int fmt = c_fmt[qq];
+                      ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
+                      const int e0 = c_e0[qq], n = c_e1[qq] - e0, so = c_off[qq];
+                      const int* cidx = A.idx + c_cp[qq];
+                      const double* cval = A.val + c_vp[qq];
+                      #pragma unroll
+                      for (int r = 0; r < kRunItems; ++r) {
+                          const int e = wslot + r * WS;
+                          const bool ok = e < n && !done_l;
+                          kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : __ldg(cidx + e0 + e));
+                          xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
+                      }
+                      T ww[kRunItems];
+                      #pragma unroll
+                      for (int r = 0; r < kRunItems; ++r) {
+                          vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
+                          ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
+                      }
+                      Kahan<T> ag, ah;
+                      #pragma unroll
+                      for (int r = 0; r < kRunItems; ++r)
+                          if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+                      double g = ag.value(), h = ah.value();
+                      for (int o = G; o < 32; o <<= 1) {
+                          g += __shfl_xor_sync(0xffffffffu, g, o);
+                          h += __shfl_xor_sync(0xffffffffu, h, o);
+                      }
+                      if (lane < G)
+                          for (int r = 0; r < C; ++r)
+                              *cluster.map_shared_rank(&s_part[par][rank][warp][lane], r) = make_double2(g, h);
+                  }
+                  if (C > 1) cluster.sync(); else __syncthreads();
+                  double dl = 0.0;
+                  if (warp < L) {
+                      if (lane < G) {
+                          double g = 0.0, h = 0.0;
+                          for (int r = 0; r < C; ++r) {
+                              const double2 pp = s_part[par][r][warp][lane];
+                              g += pp.x;
+                              h += pp.y;
+                          }
+                          g -= c_xjy[qq][lane];                     // :1181-1183
+                          if (!s_done[lane]) {
+                              if (h < 0.0) { g = 0.0; h = 0.0; }    // ccdUpdateBeta :1407-1410
+                              const double b = c_beta[qq][lane];
+                              double hd = c_hd[qq][lane];
+                              dl = prior_delta(c_pt[qq], var_l, b, g, h);
+                              dl = apply_bounds(&hd, dl);
+                              c_hd[qq][lane] = hd;
+                              if (dl != 0.0) c_beta[qq][lane] = b + dl;
+                          }
+                          s_dr[warp][lane] = dl;
+                      }
+                      dl = __shfl_sync(0xffffffffu, dl, fl);
+                      if (dl != 0.0) {
+                          const T d = (T)dl;
+                          #pragma unroll
+                          for (int r = 0; r < kRunItems; ++r)
+                              if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
+                      }
+                  }
+                  __syncthreads();
+                  if (rank == 0 && threadIdx.x == 0) {
+                      int act = 0;
+                      for (int f = 0; f < G; ++f) act += !s_done[f];
+                      for (int w = 0; w < L; ++w) {
+                          int upd = 0;
+                          for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
+                          const long long nn = A.col_ptr[j0 + q + w + 1] - A.col_ptr[j0 + q + w];
+                          const bool in = (c_fmt[q + w] == CYC_INDICATOR);
+                          n_grad += (unsigned long long)(act * nn);
+                          n_upd += (unsigned long long)(upd * nn);
+                          n_steps += act;
+                          n_idx += (unsigned long long)(nn * (4 + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
+                      }
+                  }
+                  par ^= 1;
+                  q += L;
+                  continue;
+              }
+              // ---- a single column
+              const int fmt = c_fmt[q];
+              const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
+              const bool ind = (fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT);
+              const int* cidx = A.idx + c_cp[q];
+              const double* cval = A.val + c_vp[q];
+              const int e0 = c_e0[q], e1 = c_e1[q];
+              const bool regpath = !grouped && (e1 - e0) <= kRegItems * NS;
+              Kahan<T> ag, ah;
+              int kk[kRegItems];
+              T vv[kRegItems], xx[kRegItems];
+              if (regpath) {
+                  const int so = c_off[q];
+                  #pragma unroll
+                  for (int r = 0; r < kRegItems; ++r) {
+                      const int e = slot + r * NS;                 // relative to e0
+                      const bool ok = e < e1 - e0 && !done_l;
+                      kk[r] = !ok ? -1 : (so >= 0 ? s_sidx[so + e] : (dense ? e0 + e : __ldg(cidx + e0 + e)));
+                      xx[r] = (!ok || ind) ? T(1) : (so >= 0 ? s_sx[so + e] : (T)__ldg(cval + e0 + e));
+                  }
+                  T ww[kRegItems];
+                  #pragma unroll
+                  for (int r = 0; r < kRegItems; ++r) {
+                      vv[r] = kk[r] >= 0 ? xbg[(size_t)kk[r] * G + fl] : T(0);
+                      ww[r] = kk[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, kk[r], G, fl) : T(0);
+                  }
+                  #pragma unroll
+                  for (int r = 0; r < kRegItems; ++r)
+                      if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+              } else if (!grouped) {
+                  if (!done_l) {
+                      // long column: batches of kRegItems entries per thread, loads first
+                      for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
+                          int k2[kRegItems];
+                          T x2[kRegItems], v2[kRegItems], w2[kRegItems];
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r) {
+                              const int e = base + r * NS;
+                              k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
+                              x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
+                          }
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r) {
+                              v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
+                              w2[r] = k2[r] >= 0 ? row_weight<T, WM>(wg, A.fold, fitfold, k2[r], G, fl) : T(0);
+                          }
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r)
+                              if (k2[r] >= 0) row_gh<T, MODEL>(v2[r], x2[r], w2[r], ind, ag, ah);
+                      }
+                  }
+              } else {
+                  for (int e = e0 + slot; e < e1; e += NS) {
+                      const int k = dense ? e : __ldg(cidx + e);
+                      const int s = A.strat[k];
+                      if (e > e0) {
+                          const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
+                          if (A.strat[kp] == s) continue;
+                      }
+                      T n1 = 0, n2 = 0;
+                      int qe = e;
+                      int kq = k;
+                      do {                                  // the run of stratum s in this column
+                          const T x = ind ? T(1) : (T)__ldg(cval + qe);
+                          const T ex = fexp(xbg[(size_t)kq * G + fl]);
+                          n1 += ex * x;
+                          if (!ind) n2 += ex * x * x;
+                          ++qe;
+                          if (qe >= e1) break;
+                          kq = dense ? qe : __ldg(cidx + qe);
+                      } while (A.strat[kq] == s);
+                      const double d = dg[(size_t)s * G + fl];
+                      const double nwv = ng[(size_t)s * G + fl];
+                      const double t = (double)n1 / d;        // ConditionalLogisticRegression::incrementGradientAndHessian
+                      const double gg = nwv * t;
+                      ag.add((T)gg);
+                      ah.add((T)(ind ? gg * (1.0 - t) : nwv * ((double)n2 / d - t * t)));
+                  }
+              }
+              block_reduce_lanes<G>(ag.value(), ah.value(), s_red, s_scr);
+              if (threadIdx.x < G)
+                  for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
+              if (C > 1) cluster.sync(); else __syncthreads();
+              // ---- coordinate step, identical in every CTA of the cluster
+              if (threadIdx.x < G) {
+                  double g = 0.0, h = 0.0;
+                  for (int r = 0; r < C; ++r) {
+                      const double2 pp = s_part[par][r][0][threadIdx.x];
+                      g += pp.x;
+                      h += pp.y;
+                  }
+                  g -= c_xjy[q][threadIdx.x];                    // :1181-1183
+                  double delta = 0.0;
+                  if (!s_done[threadIdx.x]) {
+                      if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
+                      const double b = c_beta[q][threadIdx.x];
+                      double hd = c_hd[q][threadIdx.x];
+                      delta = prior_delta(c_pt[q], var_l, b, g, h);
+                      delta = apply_bounds(&hd, delta);
+                      c_hd[q][threadIdx.x] = hd;
+                      if (delta != 0.0) c_beta[q][threadIdx.x] = b + delta;
+                  }
+                  s_delta[threadIdx.x] = delta;
+              }
+              __syncthreads();
+              const double dl = s_delta[fl];
+              if (rank == 0 && threadIdx.x == 0) {
+                  int act = 0, upd = 0;
+                  for (int f = 0; f < G; ++f) { act += !s_done[f]; upd += (s_delta[f] != 0.0); }
+                  const long long nn = dense ? A.K : c_cp[q + 1 < jn ? q + 1 : q] - c_cp[q];
+                  const long long nnc = dense ? A.K : A.col_ptr[j0 + q + 1] - A.col_ptr[j0 + q];
+                  (void)nn;
+                  n_grad += (unsigned long long)(act * nnc);
+                  n_upd += (unsigned long long)(upd * nnc);
+                  n_steps += act;
+                  // the column streamed by this group: row ids (not for dense) and
+                  // values (sparse, dense), once for the gradient, again for an update
+                  const long long cb = nnc * ((dense ? 0 : 4) + (ind ? 0 : 8));
+                  n_idx += (unsigned long long)(cb * (1 + (upd ? 1 : 0)));
+              }
+              // ---- updateXBeta for my rows
+              if (dl != 0.0) {
+                  const T d = (T)dl;
+                  if (regpath) {
+                      #pragma unroll
+                      for (int r = 0; r < kRegItems; ++r)
+                          if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
+                  } else if (!grouped) {
+                      for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
+                          int k2[kRegItems];
+                          T x2[kRegItems], v2[kRegItems];
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r) {
+                              const int e = base + r * NS;
+                              k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
+                              x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
+                          }
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r) v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
+                          #pragma unroll
+                          for (int r = 0; r < kRegItems; ++r)
+                              if (k2[r] >= 0) xbg[(size_t)k2[r] * G + fl] = v2[r] + d * x2[r];
+                      }
+                  } else {
+                      for (int e = e0 + slot; e < e1; e += NS) {
+                          const int k = dense ? e : __ldg(cidx + e);
+                          const int s = A.strat[k];
+                          if (e > e0) {
+                              const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
+                              if (A.strat[kp] == s) continue;
+                          }
+                          double acc = dg[(size_t)s * G + fl];
+                          int qe = e;
+                          int kq = k;
+                          do {
+                              const T x = ind ? T(1) : (T)__ldg(cval + qe);
+                              T* pp = xbg + (size_t)kq * G + fl;
+                              const T old = *pp;
+                              const T nv = old + d * x;
+                              *pp = nv;
+                              acc += (double)fexp(nv) - (double)fexp(old);
+                              ++qe;
+                              if (qe >= e1) break;
+                              kq = dense ? qe : __ldg(cidx + qe);
+                          } while (A.strat[kq] == s);
+                          dg[(size_t)s * G + fl] = acc;
+                      }
+                  }
+              }
+              __syncthreads();
+              par ^= 1;
+              ++q;
             }
-            block_reduce_lanes<G>(ag.value(), ah.value(), s_red, s_scr);
-            if (threadIdx.x < G)
-                for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
-            if (C > 1) cluster.sync(); else __syncthreads();
-            // ---- coordinate step, identical in every CTA of the cluster
-            if (threadIdx.x < G) {
-                double g = 0.0, h = 0.0;
-                for (int r = 0; r < C; ++r) {
-                    const double2 pp = s_part[par][r][0][threadIdx.x];
-                    g += pp.x;
-                    h += pp.y;
-                }
-                g -= c_xjy[q][threadIdx.x];                    // :1181-1183
-                double delta = 0.0;
-                if (!s_done[threadIdx.x]) {
-                    if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
-                    const double b = c_beta[q][threadIdx.x];
-                    double hd = c_hd[q][threadIdx.x];
-                    delta = prior_delta(c_pt[q], var_l, b, g, h);
-                    delta = apply_bounds(&hd, delta);
-                    c_hd[q][threadIdx.x] = hd;
-                    if (delta != 0.0) c_beta[q][threadIdx.x] = b + delta;
-                }
-                s_delta[threadIdx.x] = delta;
-            }
-            __syncthreads();
-            const double dl = s_delta[fl];
-            if (rank == 0 && threadIdx.x == 0) {
-                int act = 0, upd = 0;
-                for (int f = 0; f < G; ++f) { act += !s_done[f]; upd += (s_delta[f] != 0.0); }
-                const long long nn = dense ? A.K : c_cp[q + 1 < jn ? q + 1 : q] - c_cp[q];
-                const long long nnc = dense ? A.K : A.col_ptr[j0 + q + 1] - A.col_ptr[j0 + q];
-                (void)nn;
-                n_grad += (unsigned long long)(act * nnc);
-                n_upd += (unsigned long long)(upd * nnc);
-                n_steps += act;
-                // the column streamed by this group: row ids (not for dense) and
-                // values (sparse, dense), once for the gradient, again for an update
-                const long long cb = nnc * ((dense ? 0 : 4) + (ind ? 0 : 8));
-                n_idx += (unsigned long long)(cb * (1 + (upd ? 1 : 0)));
-            }
-            // ---- updateXBeta for my rows
-            if (dl != 0.0) {
-                const T d = (T)dl;
-                if (regpath) {
-                    #pragma unroll
-                    for (int r = 0; r < kRegItems; ++r)
-                        if (kk[r] >= 0) xbg[(size_t)kk[r] * G + fl] = vv[r] + d * xx[r];
-                } else if (!grouped) {
-                    for (int base = e0 + slot; base < e1; base += kRegItems * NS) {
-                        int k2[kRegItems];
-                        T x2[kRegItems], v2[kRegItems];
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r) {
-                            const int e = base + r * NS;
-                            k2[r] = (e < e1) ? (dense ? e : __ldg(cidx + e)) : -1;
-                            x2[r] = (e < e1 && !ind) ? (T)__ldg(cval + e) : T(1);
-                        }
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r) v2[r] = k2[r] >= 0 ? xbg[(size_t)k2[r] * G + fl] : T(0);
-                        #pragma unroll
-                        for (int r = 0; r < kRegItems; ++r)
-                            if (k2[r] >= 0) xbg[(size_t)k2[r] * G + fl] = v2[r] + d * x2[r];
-                    }
-                } else {
-                    for (int e = e0 + slot; e < e1; e += NS) {
-                        const int k = dense ? e : __ldg(cidx + e);
-                        const int s = A.strat[k];
-                        if (e > e0) {
-                            const int kp = dense ? e - 1 : __ldg(cidx + e - 1);
-                            if (A.strat[kp] == s) continue;
-                        }
-                        double acc = dg[(size_t)s * G + fl];
-                        int qe = e;
-                        int kq = k;
-                        do {
-                            const T x = ind ? T(1) : (T)__ldg(cval + qe);
-                            T* pp = xbg + (size_t)kq * G + fl;
-                            const T old = *pp;
-                            const T nv = old + d * x;
-                            *pp = nv;
-                            acc += (double)fexp(nv) - (double)fexp(old);
-                            ++qe;
-                            if (qe >= e1) break;
-                            kq = dense ? qe : __ldg(cidx + qe);
-                        } while (A.strat[kq] == s);
-                        dg[(size_t)s * G + fl] = acc;
-                    }
-                }
-            }
-            __syncthreads();
-            par ^= 1;
-            ++q;
         }
         // chunk done: rank 0 writes the group's beta and trust regions back
         if (rank == 0)
@@ -662,6 +1099,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         }
         __syncthreads();
         done_l = s_done[fl] != 0;
+        done_m = 0;
+        for (int f = 0; f < G; ++f) done_m |= (s_done[f] ? 1u : 0u) << f;
         if (s_all_done) break;
     }
     if (C > 1) cluster.sync();   // no CTA leaves while others may still read its shared memory
@@ -856,20 +1295,47 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
 }  // namespace
 
 
-// Conflict-free runs (see k_batch): walk the columns in order and open a new
-// run whenever the next short column shares a row with the open run, the run
-// is full, a chunk boundary is reached, or the column is not short (dense,
-// fixed, or more than `cap` entries in some CTA's rows).  run_len[j] is the
-// run's length at its first column, 0 inside a run, 1 for a column alone.
-static std::vector<int> plan_runs(const Dataset& ds, const std::vector<int>& rpart, const std::vector<int>& fixb,
-                                  int cap, bool allow) {
-    const int J = ds.J, C = (int)rpart.size() - 1;
-    std::vector<int> run_len(J, 1);
-    if (!allow) return run_len;
-    std::vector<int> stamp(ds.K, -1);
+// Column batches (see k_batch): walk the columns in order and extend the open
+// batch with the next short column (sparse or indicator, not fixed, at most
+// `cap` entries in every CTA's rows) while it holds fewer than kRunMax
+// columns, the chunk of kChunk coordinates goes on, and the rows shared
+// between its columns number at most `dmax`; otherwise close it and open a new
+// one.  A column's level is 1 + the highest level of the earlier columns of
+// its batch it shares a row with, so columns of one level touch disjoint
+// rows.  Each shared row gets a slot, and every entry on a shared row is
+// listed with (slot, column within the batch, position in the column).
+// dmax = 0 gives the conflict-free runs used with one fit per group.
+static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const std::vector<int>& fixb, int cap,
+                         bool allow, int dmax) {
+    const int J = ds.J, K = ds.K, C = (int)rpart.size() - 1;
+    RunPlan P;
+    P.len.assign(J, 1);
+    P.lvl.assign(J, 1);
+    P.dr0.assign(J, 0);
+    P.nd.assign(J, 0);
+    P.de_ptr.assign(J + 1, 0);
+    std::vector<int> stamp(K, -1), rlvl(K, 0), dslot(K, -1), first_w(K, 0), first_e(K, 0);
+    struct Ent { int w, d, e; };
+    std::vector<Ent> ents;
+    std::vector<int> shared;            // row ids in order of their slots
     int run_id = -1, start = -1, len = 0;
     auto close = [&] {
-        if (start >= 0) run_len[start] = len;
+        if (start < 0) return;
+        P.len[start] = len;
+        P.dr0[start] = (int)P.drow.size();
+        P.nd[start] = (int)shared.size();
+        P.drow.insert(P.drow.end(), shared.begin(), shared.end());
+        std::stable_sort(ents.begin(), ents.end(), [](const Ent& a, const Ent& b) { return a.w < b.w; });
+        size_t i = 0;
+        for (int w = 0; w < len; ++w) {
+            P.de_ptr[start + w] = (int)P.de_d.size();
+            for (; i < ents.size() && ents[i].w == w; ++i) {
+                P.de_d.push_back(ents[i].d | (w << 8));
+                P.de_e.push_back(ents[i].e);
+            }
+        }
+        ents.clear();
+        shared.clear();
         start = -1;
         len = 0;
     };
@@ -877,36 +1343,63 @@ static std::vector<int> plan_runs(const Dataset& ds, const std::vector<int>& rpa
     for (int j = 0; j < J; ++j) {
         if (j % kChunk == 0) close();
         const int f = ds.fmt[j];
-        bool small = (f == CYC_SPARSE || f == CYC_INDICATOR) && !fixb[j];
+        bool small = allow && (f == CYC_SPARSE || f == CYC_INDICATOR) && !fixb[j];
         const int* rows = ds.h_idx.data() + ds.col_ptr[j];
-        const long long n = ds.col_ptr[j + 1] - ds.col_ptr[j];
+        const int n = (int)(ds.col_ptr[j + 1] - ds.col_ptr[j]);
         if (small) {
             std::fill(cnt.begin(), cnt.end(), 0);
             int r = 0;
-            for (long long e = 0; e < n && small; ++e) {
+            for (int e = 0; e < n && small; ++e) {
                 while (r < C - 1 && rows[e] >= rpart[r + 1]) ++r;
                 if (++cnt[r] > cap) small = false;
             }
         }
         if (!small) {
             close();
-            run_len[j] = 1;
+            P.de_ptr[j] = (int)P.de_d.size();
             continue;
         }
-        bool conflict = false;
+        // rows shared with the open batch: how many become shared, and the level
+        int fresh = 0, level = 1;
         if (start >= 0)
-            for (long long e = 0; e < n && !conflict; ++e) conflict = (stamp[rows[e]] == run_id);
-        if (start < 0 || conflict || len == kRunMax) {
+            for (int e = 0; e < n; ++e)
+                if (stamp[rows[e]] == run_id) {
+                    fresh += dslot[rows[e]] < 0;
+                    level = std::max(level, rlvl[rows[e]] + 1);
+                }
+        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax)) {
             close();
+            level = 1;
+        }
+        if (start < 0) {
             start = j;
             ++run_id;
         }
-        for (long long e = 0; e < n; ++e) stamp[rows[e]] = run_id;
-        run_len[j] = 0;
+        const int w = len;
+        for (int e = 0; e < n; ++e) {
+            const int r = rows[e];
+            if (stamp[r] == run_id) {
+                if (dslot[r] < 0) {
+                    dslot[r] = (int)shared.size();
+                    shared.push_back(r);
+                    ents.push_back({first_w[r], dslot[r], first_e[r]});
+                }
+                ents.push_back({w, dslot[r], e});
+            } else {
+                stamp[r] = run_id;
+                dslot[r] = -1;
+                first_w[r] = w;
+                first_e[r] = e;
+            }
+            rlvl[r] = level;
+        }
+        P.len[j] = 0;
+        P.lvl[j] = level;
         ++len;
     }
     close();
-    return run_len;
+    P.de_ptr[J] = (int)P.de_d.size();
+    return P;
 }
 
 template <class T, int MODEL, int G, int WM>
@@ -914,7 +1407,8 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
-    const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * (sizeof(int) + sizeof(T));
+    const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * (sizeof(int) + sizeof(T)) +
+                       4 * kDirtyMax * G * sizeof(T);
     CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     cfg.dynamicSmemBytes = dyn;
     cfg.stream = stream;
@@ -949,7 +1443,8 @@ struct BatchRunner {
     cudaStream_t stream;
     int F, G, ngroups, Fp, C;
     std::vector<int> rpart;
-    DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag, d_runlen;
+    DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag;
+    DevBuf<int> d_runlen, d_runlvl, d_rundr0, d_runnd, d_drow, d_deptr, d_ded, d_dee;
     DevBuf<T> d_xb, d_w;
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
@@ -1008,17 +1503,31 @@ struct BatchRunner {
         for (int f = 0; f < F; ++f) var[f] = specs[f].variance;
         d_fixb.alloc(J); d_ptype.alloc(J); d_active.alloc(Fp); d_var.alloc(Fp);
         {
-            const std::pair<int, int> key(C, G);
-            const std::vector<int>* plan = nullptr;
-            for (auto& kv : ds.run_plans)
-                if (kv.first == key) plan = &kv.second;
+            const RunPlan* plan = nullptr;
+            for (auto& pl : ds.run_plans)
+                if (pl.C == C && pl.G == G) plan = &pl;
             if (!plan) {
-                ds.run_plans.emplace_back(key, plan_runs(ds, rpart, fixb, (32 / G) * kRunItems,
-                                                         model_independent(ds.model)));
-                plan = &ds.run_plans.back().second;
+                const bool rows8 = (G == 8) && model_independent(ds.model);
+                RunPlan pl = plan_runs(ds, rpart, fixb, rows8 ? kBatchCap : (32 / G) * kRunItems,
+                                       model_independent(ds.model), rows8 ? kDirtyMax : 0);
+                pl.C = C;
+                pl.G = G;
+                ds.run_plans.push_back(std::move(pl));
+                plan = &ds.run_plans.back();
             }
-            d_runlen.alloc(J);
-            CYC_CHECK_CUDA(cudaMemcpyAsync(d_runlen.get(), plan->data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
+            auto up = [&](DevBuf<int>& d, const std::vector<int>& h) {
+                d.alloc(std::max<size_t>(1, h.size()));
+                if (!h.empty())
+                    CYC_CHECK_CUDA(cudaMemcpyAsync(d.get(), h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+            };
+            up(d_runlen, plan->len);
+            up(d_runlvl, plan->lvl);
+            up(d_rundr0, plan->dr0);
+            up(d_runnd, plan->nd);
+            up(d_drow, plan->drow);
+            up(d_deptr, plan->de_ptr);
+            up(d_ded, plan->de_d);
+            up(d_dee, plan->de_e);
             CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
         }
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixb.get(), fixb.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -1098,6 +1607,13 @@ struct BatchRunner {
         a.fold = d_fold ? d_fold8.get() : nullptr;
         a.fitfold = d_fold ? d_fitfold.get() : nullptr;
         a.run_len = d_runlen.get();
+        a.run_lvl = d_runlvl.get();
+        a.run_dr0 = d_rundr0.get();
+        a.run_nd = d_runnd.get();
+        a.drow = d_drow.get();
+        a.de_ptr = d_deptr.get();
+        a.de_d = d_ded.get();
+        a.de_e = d_dee.get();
         a.conv = ctl.convergence_type; a.tol = tol; a.max_iter = ctl.max_iterations;
         a.out_iter = d_iter.get(); a.out_flag = d_flag.get(); a.out_obj = d_obj.get(); a.counters = d_counters.get();
         cudaEvent_t e0, e1;

@@ -140,6 +140,20 @@ struct ColView {
 };
 
 // ---------------------------------------------------------------------------
+// column batches of the batched solver (planned on the host, batch.cu)
+// ---------------------------------------------------------------------------
+struct RunPlan {
+    int C = 0, G = 0;
+    std::vector<int> len;       // J: columns in the batch starting here (1 = alone), 0 inside a batch
+    std::vector<int> lvl;       // J: level of the column in its batch (1 + max level of earlier sharers)
+    std::vector<int> dr0, nd;   // J (batch starts): its shared rows are drow[dr0, dr0 + nd)
+    std::vector<int> drow;      // row ids shared by two or more columns of a batch
+    std::vector<int> de_ptr;    // J+1: entries of column j on shared rows are de_*[de_ptr[j], de_ptr[j+1])
+    std::vector<int> de_d;      // shared-row slot | (column within the batch << 8)
+    std::vector<int> de_e;      // entry position within the column
+};
+
+// ---------------------------------------------------------------------------
 // dataset
 // ---------------------------------------------------------------------------
 struct Dataset {
@@ -169,8 +183,8 @@ struct Dataset {
     DevBuf<int> d_row_col;
     DevBuf<double> d_row_val;
 
-    // conflict-free column runs of the batched solver, cached per (cluster size, fits per group)
-    std::vector<std::pair<std::pair<int, int>, std::vector<int>>> run_plans;
+    // column batches of the batched solver, cached per (cluster size, fits per group)
+    std::vector<RunPlan> run_plans;
 
     long long col_len(int j) const {
         return (fmt[j] == CYC_DENSE || fmt[j] == CYC_INTERCEPT) ? K : col_ptr[j + 1] - col_ptr[j];

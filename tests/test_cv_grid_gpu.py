@@ -1,0 +1,112 @@
+"""Cross-validation grids on the device (cyc_cv_grid_fit): folds x prior
+variances as one batched solve.  Every fit equals the oracle's fit on the
+same training rows, its held-out predictive log likelihood is the oracle's
+for its coefficients, and both hold whatever number of CTAs splits the rows
+(the cluster size), so the cross-CTA exchange and the batches of short
+columns that share rows are covered.
+
+The data mixes an intercept, real-valued sparse columns drawn from a small
+pool of rows (so consecutive short columns share rows and batches replay
+them serially), and Zipf-sized indicator columns (long columns stream)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from cyclops_b200 import data as D
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed_data(model, K=40_000, n_sparse=120, n_ind=300, seed=5):
+    rng = np.random.default_rng(seed)
+    b = D.ColumnBuilder(K).intercept()
+    eta = np.full(K, -1.0 if model == D.LR else -2.0)
+    pool = rng.choice(K, size=4_000, replace=False)         # rows the sparse columns share
+    for c in range(n_sparse):
+        n = int(rng.integers(5, 400))
+        rows = rng.choice(pool, size=n, replace=False)
+        vals = rng.normal(0.0, 1.0, size=n)
+        b.sparse(rows, vals)
+        if c % 3 == 0:
+            eta[rows] += 0.5 * vals
+    counts = np.maximum(1, (K * 0.5 * np.arange(1, n_ind + 1) ** -0.9)).astype(int)
+    for c in range(n_ind):
+        rows = rng.choice(K, size=min(K, counts[c]), replace=False)
+        b.indicator(rows)
+        if c % 4 == 0:
+            eta[rows] += rng.normal(0.0, 0.5)
+    if model == D.LR:
+        y = (rng.random(K) < 1.0 / (1.0 + np.exp(-eta))).astype(float)
+    else:
+        y = rng.poisson(np.exp(np.minimum(eta, 5.0))).astype(float)
+    return b.build(model, y, has_intercept=True)
+
+
+def _oracle_fit(data, variance, weights, tol):
+    from oracle import oracle as O
+    return O.port().fit(data, D.PRIOR_LAPLACE, variance,
+                        control=O.make_control(tolerance=tol, convergence_type=D.CONV_GRADIENT), exclude=[0],
+                        weights=weights)
+
+
+@pytest.fixture
+def cluster_size():
+    old = os.environ.get("CYC_BATCH_CLUSTER")
+    yield lambda c: os.environ.__setitem__("CYC_BATCH_CLUSTER", str(c))
+    if old is None:
+        os.environ.pop("CYC_BATCH_CLUSTER", None)
+    else:
+        os.environ["CYC_BATCH_CLUSTER"] = old
+
+
+@pytest.mark.parametrize("model", [D.LR, D.PR])
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("clusters", [1, 3, 8])
+def test_cv_grid_matches_oracle(cuda_lib, cluster_size, model, precision, clusters):
+    from cyclops_b200 import api
+    from oracle import oracle as O
+    cluster_size(clusters)
+    data = _mixed_data(model)
+    n_folds = 5
+    masks = api.cv_fold_weights(data.K, n_folds, 31)
+    folds = api.fold_ids_from_weights(masks)
+    variances = [D.laplace_variance(lam) for lam in (1.0, 10.0)]
+    tol = 1e-7
+    prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, [0])
+    ctl = api.create_control(tolerance=tol, precision=precision, polish_tolerance=1e-5)
+    res = api.cv_grid_fit(data, prior, folds, n_folds, variances, ctl)
+    lib = O.port()
+    for i, fit in enumerate(res.fits):
+        v, f = variances[i // n_folds], i % n_folds
+        ref = _oracle_fit(data, v, masks[f], tol)
+        assert fit.return_flag == ref.return_flag == 0
+        np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
+        err = np.abs(fit.beta - ref.beta) / np.maximum(np.abs(ref.beta), 1.0)
+        assert err.max() < 1e-4, (i, err.max())
+        if precision == "fp64":   # mixed precision reports the cycles of its FP64 phase
+            assert abs(fit.iterations - ref.iterations) <= 2, (i, fit.iterations, ref.iterations)
+        held = (masks[f] == 0).astype(float)
+        pll = lib.predictive_loglik(data, fit.beta, held)
+        assert rel_err(res.pred_loglik[i], pll) < 1e-9, (i, res.pred_loglik[i], pll)
+    for v in range(len(variances)):
+        assert rel_err(res.grid_mean[v], np.mean(res.pred_loglik[v * n_folds:(v + 1) * n_folds])) < 1e-12
+
+
+def test_cluster_sizes_agree(cuda_lib, cluster_size):
+    """The same grid split over 1, 2, 5 and 8 CTAs: only the order of the
+    cross-CTA sums differs, so the fits agree far inside the tolerance."""
+    from cyclops_b200 import api
+    data = _mixed_data(D.LR, seed=9)
+    masks = api.cv_fold_weights(data.K, 4, 3)
+    folds = api.fold_ids_from_weights(masks)
+    prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, [0])
+    ctl = api.create_control(tolerance=1e-8)
+    variances = [D.laplace_variance(10.0)] * 2
+    out = {}
+    for c in (1, 2, 5, 8):
+        cluster_size(c)
+        out[c] = np.array([f.beta for f in api.cv_grid_fit(data, prior, folds, 4, variances, ctl).fits])
+    for c in (2, 5, 8):
+        assert np.max(np.abs(out[c] - out[1]) / np.maximum(np.abs(out[1]), 1.0)) < 1e-6, c
