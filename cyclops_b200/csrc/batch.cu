@@ -75,14 +75,15 @@ struct BatchArgs {
     const int* drow;              // shared row ids
     const int* de_ptr;            // J+1: entries of column j on shared rows
     const int* de_d;              // shared-row slot | (column within the batch << 8)
-    const int* de_e;              // entry position within the column
+    const double* de_x;           // the entry's value (1 for indicator columns)
     int conv;
     double tol;
     int max_iter;
     int* out_iter;                // [F]
     int* out_flag;                // [F]
     double* out_obj;              // [F]
-    unsigned long long* counters; // [4] grad fit-entries, update fit-entries, steps, index entries
+    unsigned long long* counters; // [3 + groups]: grad fit-entries, update fit-entries, steps, then
+                                  // per group the bytes of row ids / values it streamed
 };
 
 template <class T>
@@ -235,11 +236,15 @@ __device__ __forceinline__ void store_row(T* p, const T (&v)[N]) {
 }
 
 // Thread-per-row layout of one group's G fits: a row's linear predictors
-// are split into TPR parts of FPT fits (16 bytes in FP32, one 32-byte sector
-// in FP64), and each thread holds R rows' parts at a time.
-template <class T, int G, int WM>
+// are split into TPR parts of FPT = 4 fits (16 bytes in FP32, one 32-byte
+// sector in FP64), and each thread holds R = 2 rows' parts at a time.  The
+// layout is a parameter of the caller (a CTA streaming one long column,
+// BLOCK, or a warp taking one short column of a batch); wider parts or more
+// rows per thread measured slower on B200 here: the registers they take make
+// the rest of the persistent kernel spill.
+template <class T, int G, bool BLOCK>
 struct RowLayout {
-    static constexpr int FPT = (G % 4 == 0) ? 4 : G;
+    static constexpr int FPT = (G % 4 != 0) ? G : 4;
     static constexpr int TPR = G / FPT;
     static constexpr int R = 2;
 };
@@ -329,17 +334,19 @@ struct ColRows {
 template <class T, int MODEL, int G, int WM, int STRIDE>
 __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xbg, const T* wg,
                                         const signed char* fold, const unsigned char* wmask, unsigned done,
-                                        double (&g)[RowLayout<T, G, WM>::FPT], double (&h)[RowLayout<T, G, WM>::FPT]) {
-    using Lay = RowLayout<T, G, WM>;
+                                        double (&g)[RowLayout<T, G, STRIDE == kBT>::FPT],
+                                        double (&h)[RowLayout<T, G, STRIDE == kBT>::FPT]) {
+    using Lay = RowLayout<T, G, STRIDE == kBT>;
     constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
     const int f0 = (t0 % TPR) * FPT;
     const unsigned dn = done >> f0;
     Kahan<T> ag[FPT], ah[FPT];
-    for (int base = c.e0 + t0 / TPR; base < c.e1; base += R * RS) {
-        int k[R];
-        T x[R];
-        #pragma unroll
-        for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+    int base = c.e0 + t0 / TPR;
+    int k[R];
+    T x[R];
+    #pragma unroll
+    for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+    for (; base < c.e1; base += R * RS) {
         T v[R][FPT], w[R][FPT];
         unsigned wm[R];
         #pragma unroll
@@ -354,6 +361,11 @@ __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xb
                 for (int f = 0; f < FPT; ++f) { v[r][f] = T(0); w[r][f] = T(0); }
             }
         }
+        // the next rows' ids load while these rows' values arrive
+        int kn[R];
+        T xn[R];
+        #pragma unroll
+        for (int r = 0; r < R; ++r) c.get(base + (R + r) * RS, kn[r], xn[r]);
         #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (k[r] < 0) continue;
@@ -364,6 +376,8 @@ __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xb
                 row_gh<T, MODEL>(v[r][f], x[r], wt, c.ind, ag[f], ah[f]);
             }
         }
+        #pragma unroll
+        for (int r = 0; r < R; ++r) { k[r] = kn[r]; x[r] = xn[r]; }
     }
     #pragma unroll
     for (int f = 0; f < FPT; ++f) { g[f] = ag[f].value(); h[f] = ah[f].value(); }
@@ -371,26 +385,100 @@ __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xb
 
 // updateXBeta over the entries of a column by the STRIDE threads t0 (same
 // split as rows_gh)
-template <class T, int G, int WM, int STRIDE>
+template <class T, int G, int STRIDE>
 __device__ __forceinline__ void rows_update(const ColRows<T>& c, int t0, T* xbg, const T (&d)[G]) {
-    using Lay = RowLayout<T, G, WM>;
+    using Lay = RowLayout<T, G, STRIDE == kBT>;
     constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
     const int f0 = (t0 % TPR) * FPT;
-    for (int base = c.e0 + t0 / TPR; base < c.e1; base += R * RS) {
-        int k[R];
-        T x[R];
-        #pragma unroll
-        for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+    bool moved = false;                     // a part whose fits all kept their coefficients stays
+    #pragma unroll
+    for (int f = 0; f < FPT; ++f) moved |= (d[f0 + f] != T(0));
+    if (!moved) return;
+    int base = c.e0 + t0 / TPR;
+    int k[R];
+    T x[R];
+    #pragma unroll
+    for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
+    for (; base < c.e1; base += R * RS) {
         T v[R][FPT];
         #pragma unroll
         for (int r = 0; r < R; ++r)
             if (k[r] >= 0) load_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
+        int kn[R];
+        T xn[R];
+        #pragma unroll
+        for (int r = 0; r < R; ++r) c.get(base + (R + r) * RS, kn[r], xn[r]);
         #pragma unroll
         for (int r = 0; r < R; ++r) {
             if (k[r] < 0) continue;
             #pragma unroll
             for (int f = 0; f < FPT; ++f) v[r][f] = upd_fma(d[f0 + f], x[r], v[r][f]);
             store_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
+        }
+        #pragma unroll
+        for (int r = 0; r < R; ++r) { k[r] = kn[r]; x[r] = xn[r]; }
+    }
+}
+
+// updateXBeta of a batch's columns over this CTA's rows, flat: item i is part
+// i % TPR of entry i / TPR of the concatenated columns (offsets `boff`, empty
+// for columns without a step), U items per thread in flight.  Entries on the
+// batch's shared rows (`drow`, nd of them) are left to their owner.  No two
+// items touch the same (row, part): a row outside `drow` is in one column.
+template <class T, int G>
+__device__ __forceinline__ void batch_update(T* xbg, const int* idx, const double* val, const int* sidx, const T* sx,
+                                             const long long* cp, const long long* vp, const int* e0, const int* off,
+                                             const int* fmt, int q, int L, const int* boff,
+                                             const double (*dr)[G], const int* drow, int nd) {
+    using Lay = RowLayout<T, G, false>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, U = 4;
+    unsigned bloom = 0;
+    for (int d = 0; d < nd; ++d) bloom |= 1u << (drow[d] & 31);
+    const int items = boff[L] * TPR;
+    for (int i0 = threadIdx.x; i0 < items; i0 += U * kBT) {
+        int k[U], w[U];
+        T x[U];
+        #pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int i = i0 + u * kBT;
+            k[u] = -1;
+            w[u] = 0;
+            x[u] = T(1);
+            if (i >= items) continue;
+            const int it = i / TPR;
+            int c = 0;
+            while (it >= boff[c + 1]) ++c;
+            const int qq = q + c, e = it - boff[c];
+            w[u] = c;
+            if (off[qq] >= 0) {
+                k[u] = sidx[off[qq] + e];
+                if (fmt[qq] == CYC_SPARSE) x[u] = sx[off[qq] + e];
+            } else {
+                k[u] = __ldg(idx + cp[qq] + e0[qq] + e);
+                if (fmt[qq] == CYC_SPARSE) x[u] = (T)__ldg(val + vp[qq] + e0[qq] + e);
+            }
+            if ((bloom >> (k[u] & 31)) & 1u) {
+                bool sh = false;
+                for (int d = 0; d < nd; ++d) sh |= (drow[d] == k[u]);
+                if (sh) k[u] = -1;
+            }
+            bool moved = false;             // a part whose fits all kept their coefficients stays
+            const int f0 = (i % TPR) * FPT;
+            #pragma unroll
+            for (int f = 0; f < FPT; ++f) moved |= (dr[c][f0 + f] != 0.0);
+            if (!moved) k[u] = -1;
+        }
+        T v[U][FPT];
+        #pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (k[u] >= 0) load_row<T, FPT>(xbg + (size_t)k[u] * G + ((i0 + u * kBT) % TPR) * FPT, v[u]);
+        #pragma unroll
+        for (int u = 0; u < U; ++u) {
+            if (k[u] < 0) continue;
+            const int f0 = ((i0 + u * kBT) % TPR) * FPT;
+            #pragma unroll
+            for (int f = 0; f < FPT; ++f) v[u][f] = upd_fma((T)dr[w[u]][f0 + f], x[u], v[u][f]);
+            store_row<T, FPT>(xbg + (size_t)k[u] * G + f0, v[u]);
         }
     }
 }
@@ -433,7 +521,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     // independent rows, 8 fits per group: columns stream thread per row (all
     // fits of a row by vector loads) and short columns go in batches
     constexpr bool kRowStream = (G == 8) && !(MODEL == CYC_CLR || MODEL == CYC_CPR);
-    using Lay = RowLayout<T, G, WM>;
+    using LayW = RowLayout<T, G, false>;   // a warp per column (batches)
+    using LayB = RowLayout<T, G, true>;    // the CTA per column (single columns)
     // strata of my rows (partition boundaries are stratum starts); none if my range is empty
     const int s0 = (grouped && r0 < r1) ? A.strat[r0] : 0;
     const int s1 = (grouped && r0 < r1) ? (r1 >= A.K ? A.S : A.strat[r1]) : 0;
@@ -471,9 +560,11 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     __shared__ int s_bde_d[kRunMax * kDirtyMax];
     __shared__ double s_bde_x[kRunMax * kDirtyMax];
     __shared__ unsigned char s_dwm[kDirtyMax];
+    __shared__ int s_drow[kDirtyMax];
+    __shared__ int s_boff[kRunMax + 1];
     // the current chunk of coordinates
     __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk], c_run[kChunk];
-    __shared__ int c_lvl[kChunk];
+    __shared__ int c_lvl[kChunk], c_nd[kChunk], c_dr0[kChunk], c_de0[kChunk + 1];
     __shared__ long long c_cp[kChunk], c_vp[kChunk];
     __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
     __shared__ int c_sq[kChunk + 1];       // staged coordinates in order
@@ -536,6 +627,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     unsigned done_m = 0;             // all converged fits of the group (bit f)
     for (int f = 0; f < G; ++f) done_m |= (s_done[f] ? 1u : 0u) << f;
     const double var_l = A.variance[fg + fl];
+    const double lam_l = sqrt(2.0 / var_l);      // LaplacePrior rate, :282-292
 
     unsigned long long n_grad = 0, n_upd = 0, n_steps = 0, n_idx = 0;
     int par = 0;
@@ -550,7 +642,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             if (h < 0.0) { g = 0.0; h = 0.0; }             // :1407-1410
             const double b = c_beta[qq][f];
             double hd = c_hd[qq][f];
-            double dl = prior_delta(c_pt[qq], var_l, b, g, h);
+            double dl = prior_delta_rate(c_pt[qq], var_l, lam_l, b, g, h);
             dl = apply_bounds(&hd, dl);
             c_hd[qq][f] = hd;
             if (dl != 0.0) c_beta[qq][f] = b + dl;
@@ -582,6 +674,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             c_pt[q] = A.ptype[j];
             c_run[q] = A.run_len[j];
             c_lvl[q] = A.run_lvl[j];
+            c_nd[q] = A.run_nd[j];
+            c_dr0[q] = A.run_dr0[j];
+            c_de0[q] = A.de_ptr[j];
+            if (q == jn - 1) c_de0[jn] = A.de_ptr[j + 1];
             c_cp[q] = A.col_ptr[j];
             c_vp[q] = A.val_ptr[j];
             const bool dn = (f0 == CYC_DENSE || f0 == CYC_INTERCEPT);
@@ -638,9 +734,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             if constexpr (kRowStream) {
             if (L > 1) {
                 // ---- a batch of L short columns (planned: plan_runs); warp w takes column q + w
-                const int jb = j0 + q;
-                const int nd = A.run_nd[jb], dr0 = A.run_dr0[jb];
-                const int de0 = A.de_ptr[jb], nde = A.de_ptr[jb + L] - de0;
+                const int nd = c_nd[q], dr0 = c_dr0[q];
+                const int de0 = c_de0[q], nde = c_de0[q + L] - de0;
                 // rows shared inside the batch: their owners push them (all G fits)
                 // into every CTA; the weights of those rows are kept locally
                 for (int t = threadIdx.x; t < nd * G; t += kBT) {
@@ -650,18 +745,17 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         const T v = xbg[(size_t)k * G + f];
                         for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_dst[par][d][f], r) = v;
                     }
+                    if (f == 0) s_drow[d] = k;
                     if (WM == 1) {
                         if (f == 0) s_dwm[d] = s_wmask[(int)__ldg(A.fold + k)];
                     } else {
                         s_dw[d][f] = wg[(size_t)k * G + f];
                     }
                 }
-                if (threadIdx.x <= L) s_bde_ptr[threadIdx.x] = A.de_ptr[jb + threadIdx.x] - de0;
+                if (threadIdx.x <= L) s_bde_ptr[threadIdx.x] = c_de0[q + threadIdx.x] - de0;
                 for (int t = threadIdx.x; t < nde; t += kBT) {
-                    const int dd = __ldg(A.de_d + de0 + t);
-                    const int qw = q + (dd >> 8);
-                    s_bde_d[t] = dd & 0xff;
-                    s_bde_x[t] = (c_fmt[qw] == CYC_SPARSE) ? __ldg(A.val + c_vp[qw] + __ldg(A.de_e + de0 + t)) : 1.0;
+                    s_bde_d[t] = __ldg(A.de_d + de0 + t) & 0xff;
+                    s_bde_x[t] = __ldg(A.de_x + de0 + t);
                 }
                 // gradient partials of every column from the state at the batch's start
                 if (warp < L) {
@@ -669,11 +763,11 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                     const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
                                         so >= 0 ? s_sx + so : nullptr, c_e0[qq], c_e1[qq], false,
                                         c_fmt[qq] == CYC_INDICATOR};
-                    double g[Lay::FPT], h[Lay::FPT];
+                    double g[LayW::FPT], h[LayW::FPT];
                     rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, g, h);
                     int fit;
                     bool is_h, holder;
-                    const double v = warp_reduce_rows<Lay::FPT, Lay::TPR>(g, h, fit, is_h, holder);
+                    const double v = warp_reduce_rows<LayW::FPT, LayW::TPR>(g, h, fit, is_h, holder);
                     if (holder) {
                         double* dst = is_h ? &s_part[par][rank][warp][fit].y : &s_part[par][rank][warp][fit].x;
                         for (int r = 0; r < C; ++r) *cluster.map_shared_rank(dst, r) = v;
@@ -684,8 +778,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 // level, a column's (g, h) is its partials plus, for each of its
                 // entries on a shared row, the change of that row's terms since
                 // the batch's start (zero unless an earlier column moved it)
-                for (int t = threadIdx.x; t < nd * G; t += kBT) s_dcur[t / G][t % G] = s_dst[par][t / G][t % G];
-                __syncthreads();
+                if (nd > 0) {
+                    for (int t = threadIdx.x; t < nd * G; t += kBT) s_dcur[t / G][t % G] = s_dst[par][t / G][t % G];
+                    __syncthreads();
+                }
                 int nlev = 1;
                 for (int w = 0; w < L; ++w) nlev = max(nlev, c_lvl[q + w]);
                 const int fw = lane % G, sl = lane / G;    // (fit, entry slot) inside a warp
@@ -732,23 +828,29 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                     }
                     __syncthreads();
                 }
-                // updateXBeta of my rows, level by level (columns of one level share no row)
-                for (int lv = 1; lv <= nlev; ++lv) {
-                    if (warp < L && c_lvl[q + warp] == lv) {
-                        const int qq = q + warp, so = c_off[qq];
-                        T dd[G];
+                // updateXBeta of my rows in one pass over the batch's entries (all
+                // threads, flat): a row that one column of the batch touches gets
+                // that column's step; a row the batch shares gets its replayed
+                // value, written by its owner.  Columns whose fits all kept their
+                // coefficients are skipped.
+                if (threadIdx.x == 0) {
+                    int o = 0;
+                    for (int w = 0; w < L; ++w) {
+                        s_boff[w] = o;
                         bool any = false;
-                        #pragma unroll
-                        for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[warp][f]; any |= (s_dr[warp][f] != 0.0); }
-                        if (any) {
-                            const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
-                                                so >= 0 ? s_sx + so : nullptr, c_e0[qq], c_e1[qq], false,
-                                                c_fmt[qq] == CYC_INDICATOR};
-                            rows_update<T, G, WM, 32>(cr, lane, xbg, dd);
-                        }
+                        for (int f = 0; f < G; ++f) any |= (s_dr[w][f] != 0.0);
+                        if (any) o += c_e1[q + w] - c_e0[q + w];
                     }
-                    __syncthreads();
+                    s_boff[L] = o;
                 }
+                __syncthreads();
+                batch_update<T, G>(xbg, A.idx, A.val, s_sidx, s_sx, c_cp, c_vp, c_e0, c_off, c_fmt, q, L, s_boff,
+                                   s_dr, s_drow, nd);
+                for (int t = threadIdx.x; t < nd * G; t += kBT) {
+                    const int d = t / G, k = s_drow[d];
+                    if (k >= r0 && k < r1) xbg[(size_t)k * G + t % G] = s_dcur[d][t % G];
+                }
+                __syncthreads();
                 if (rank == 0 && threadIdx.x == 0) count_run(q, L);
                 par ^= 1;
                 q += L;
@@ -761,9 +863,9 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 const ColRows<T> cr{A.idx + c_cp[q], A.val + c_vp[q], so >= 0 ? s_sidx + so : nullptr,
                                     so >= 0 ? s_sx + so : nullptr, c_e0[q], c_e1[q], dense,
                                     fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT};
-                double g[Lay::FPT], h[Lay::FPT];
+                double g[LayB::FPT], h[LayB::FPT];
                 rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, g, h);
-                block_reduce_rows<G, Lay::FPT, Lay::TPR>(g, h, s_red, reinterpret_cast<double*>(s_scr));
+                block_reduce_rows<G, LayB::FPT, LayB::TPR>(g, h, s_red, reinterpret_cast<double*>(s_scr));
                 if (threadIdx.x < G)
                     for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
                 if (C > 1) cluster.sync(); else __syncthreads();
@@ -782,7 +884,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 #pragma unroll
                 for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[0][f]; any |= (s_dr[0][f] != 0.0); }
                 if (rank == 0 && threadIdx.x == 0) count_run(q, 1);
-                if (any) rows_update<T, G, WM, kBT>(cr, threadIdx.x, xbg, dd);
+                if (any) rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd);
                 __syncthreads();
                 par ^= 1;
                 ++q;
@@ -1114,7 +1216,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         atomicAdd(A.counters + 0, n_grad);
         atomicAdd(A.counters + 1, n_upd);
         atomicAdd(A.counters + 2, n_steps);
-        atomicAdd(A.counters + 3, n_idx);
+        atomicAdd(A.counters + 3 + grp, n_idx);
     }
 }
 
@@ -1147,21 +1249,15 @@ __global__ void k_scatter_weights(int K, int G, int f, const double* __restrict_
         w[((size_t)grp * K + k) * G + lane] = src ? (T)src[k] : T(1);
 }
 
-__global__ void k_fold_to_i8(int K, const int* __restrict__ fold, signed char* __restrict__ out) {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) out[k] = (signed char)fold[k];
+// values of the entries a batch shares (index into the value array, -1 for 1)
+__global__ void k_gather_values(int n, const int* __restrict__ vi, const double* __restrict__ val,
+                                double* __restrict__ out) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x)
+        out[t] = vi[t] >= 0 ? val[vi[t]] : 1.0;
 }
 
-// CV grid weights: fit f trains on the rows outside its fold (padding fits: none)
-template <class T>
-__global__ void k_fold_weights(int K, int G, int Fp, const int* __restrict__ fold, const int* __restrict__ fitfold,
-                               T* __restrict__ w) {
-    const long long total = (long long)K * Fp;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
-        const int f = (int)(t % Fp);
-        const int k = (int)(t / Fp);
-        const int ff = fitfold[f];
-        w[((size_t)(f / G) * K + k) * G + (f % G)] = (ff >= -1 && fold[k] != ff) ? T(1) : T(0);
-    }
+__global__ void k_fold_to_i8(int K, const int* __restrict__ fold, signed char* __restrict__ out) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) out[k] = (signed char)fold[k];
 }
 
 // per fit: log likelihood under its training weights (getLogLikelihood,
@@ -1181,7 +1277,8 @@ __global__ void k_batch_final(int model, int K, int S, int G, int F, const doubl
     double a = 0.0, p = 0.0;
     for (int k = threadIdx.x; k < K; k += blockDim.x) {
         const size_t o = ((size_t)grp * K + k) * G + lane;
-        const double v = xb[o], wt = w[o], yk = y[k];
+        const double v = xb[o], yk = y[k];
+        const double wt = w ? w[o] : ((fitfold[f] >= -1 && fold[k] != fitfold[f]) ? 1.0 : 0.0);
         const int yi = (int)yk;
         a += yi * v * wt;
         if (model == CYC_LR) a -= wt * log(1.0 + exp(v));
@@ -1260,10 +1357,59 @@ __global__ void k_batch_xjy(int J, int K, int G, int ngroups, const int* fmt, co
     }
 }
 
+// CV grid XjY (computeXjY, ModelSpecifics.hpp:486-524, with 0/1 fold
+// weights): per column, the sums of x*y over its entries in each fold, 16
+// folds per pass, each thread summing its own entries, then the threads'
+// sums in thread order (deterministic).  out[j][v], v < n_folds.
+__global__ void k_fold_xy(int J, int K, int n_folds, const int* fmt, const long long* col_ptr,
+                          const long long* val_ptr, const int* idx, const double* val, const double* y,
+                          const signed char* fold, double* out) {
+    __shared__ double part[16][kBT];
+    for (int j = blockIdx.x; j < J; j += gridDim.x) {
+        const int f = fmt[j];
+        const bool dense = (f == CYC_DENSE || f == CYC_INTERCEPT);
+        const bool hasx = (f == CYC_SPARSE || f == CYC_DENSE);
+        const long long n = dense ? K : col_ptr[j + 1] - col_ptr[j];
+        const int* c = idx + col_ptr[j];
+        const double* v = val + val_ptr[j];
+        for (int v0 = 0; v0 < n_folds; v0 += 16) {
+            for (int q = 0; q < 16; ++q) part[q][threadIdx.x] = 0.0;
+            for (long long e = threadIdx.x; e < n; e += kBT) {
+                const int k = dense ? (int)e : c[e];
+                const int q = (int)fold[k] - v0;
+                if (q >= 0 && q < 16) part[q][threadIdx.x] += (hasx ? v[e] : 1.0) * y[k];
+            }
+            __syncthreads();
+            if (threadIdx.x < 16 && v0 + (int)threadIdx.x < n_folds) {
+                double sum = 0.0;
+                for (int t = 0; t < kBT; ++t) sum += part[threadIdx.x][t];
+                out[(size_t)j * n_folds + v0 + threadIdx.x] = sum;
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// every fit's XjY from the fold sums: fit f trains on the folds other than
+// fitfold[f] (all of them for -1, none for padding fits)
+__global__ void k_cv_xjy(int J, int Fp, int n_folds, const double* __restrict__ fs, const int* __restrict__ fitfold,
+                         double* __restrict__ xjy) {
+    const long long total = (long long)Fp * J;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int f = (int)(t / J), j = (int)(t % J);
+        const int ff = fitfold[f];
+        double sum = 0.0;
+        if (ff >= -1)
+            for (int v = 0; v < n_folds; ++v)
+                if (v != ff) sum += fs[(size_t)j * n_folds + v];
+        xjy[(size_t)f * J + j] = sum;
+    }
+}
+
 // grouped models: per (stratum, fit) events sum(y*w) and denominator sum(exp(xb))
 template <class T>
 __global__ void k_batch_strata(int S, int K, int G, int ngroups, const int* strat_ptr, const double* y, const T* w,
-                               const T* xb, double* nw, double* denom) {
+                               const signed char* fold, const int* fitfold, const T* xb, double* nw, double* denom) {
     const long long total = (long long)S * G * ngroups;
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
         const int lane = (int)(t % G);
@@ -1272,7 +1418,8 @@ __global__ void k_batch_strata(int S, int K, int G, int ngroups, const int* stra
         double a = 0.0, d = 0.0;
         for (int k = strat_ptr[s]; k < strat_ptr[s + 1]; ++k) {
             const size_t o = ((size_t)grp * K + k) * G + lane;
-            a += y[k] * (double)w[o];
+            const int ff = w ? 0 : fitfold[grp * G + lane];
+            a += y[k] * (w ? (double)w[o] : ((ff >= -1 && fold[k] != ff) ? 1.0 : 0.0));
             d += exp((double)xb[o]);
         }
         nw[((size_t)grp * S + s) * G + lane] = a;
@@ -1282,12 +1429,15 @@ __global__ void k_batch_strata(int S, int K, int G, int ngroups, const int* stra
 
 // fixed likelihood terms per fit: sum_k w_fk * c_k with c_k = -log(y_k!)
 template <class T>
-__global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w, double* out) {
+__global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w, const signed char* fold,
+                                const int* fitfold, double* out) {
     const int f = blockIdx.x;
     if (f >= F) return;
     const int grp = f / G, lane = f % G;
+    const int ff = w ? 0 : fitfold[f];
     double a = 0.0, dummy = 0.0;
-    for (int k = threadIdx.x; k < K; k += blockDim.x) a += c[k] * (double)w[((size_t)grp * K + k) * G + lane];
+    for (int k = threadIdx.x; k < K; k += blockDim.x)
+        a += c[k] * (w ? (double)w[((size_t)grp * K + k) * G + lane] : ((ff >= -1 && fold[k] != ff) ? 1.0 : 0.0));
     block_sum2(a, dummy);
     if (threadIdx.x == 0) out[f] = a;
 }
@@ -1331,7 +1481,7 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
             P.de_ptr[start + w] = (int)P.de_d.size();
             for (; i < ents.size() && ents[i].w == w; ++i) {
                 P.de_d.push_back(ents[i].d | (w << 8));
-                P.de_e.push_back(ents[i].e);
+                P.de_e.push_back(ds.fmt[start + w] == CYC_SPARSE ? (int)(ds.val_ptr[start + w] + ents[i].e) : -1);
             }
         }
         ents.clear();
@@ -1446,6 +1596,7 @@ struct BatchRunner {
     DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag;
     DevBuf<int> d_runlen, d_runlvl, d_rundr0, d_runnd, d_drow, d_deptr, d_ded, d_dee;
     DevBuf<T> d_xb, d_w;
+    DevBuf<double> d_dex;
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
 
@@ -1476,8 +1627,11 @@ struct BatchRunner {
 
     DevBuf<signed char> d_fold8;
 
-    void set_folds(const int* d_fold_of_row, const std::vector<int>& fit_fold) {
+    int n_folds = 0;
+
+    void set_folds(const int* d_fold_of_row, int folds, const std::vector<int>& fit_fold) {
         d_fold = d_fold_of_row;
+        n_folds = folds;
         d_fold8.alloc(ds.K);
         launch(k_fold_to_i8, grid_for(ds.K, 1), 256, 0, stream, ds.K, d_fold, d_fold8.get());
         std::vector<int> ff(Fp, -2);
@@ -1528,18 +1682,20 @@ struct BatchRunner {
             up(d_deptr, plan->de_ptr);
             up(d_ded, plan->de_d);
             up(d_dee, plan->de_e);
+            d_dex.alloc(std::max<size_t>(1, plan->de_e.size()));
+            if (!plan->de_e.empty())
+                launch(k_gather_values, grid_for((long long)plan->de_e.size(), 4), 256, 0, stream,
+                       (int)plan->de_e.size(), (const int*)d_dee.get(), (const double*)ds.d_val.get(), d_dex.get());
             CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
         }
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixb.get(), fixb.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_ptype.get(), pt.data(), J * sizeof(int), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_active.get(), act.data(), Fp * sizeof(int), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_var.get(), var.data(), Fp * sizeof(double), cudaMemcpyHostToDevice, stream));
-        // weights
-        d_w.alloc((size_t)ngroups * K * G);
-        if (d_fold) {
-            launch(k_fold_weights<T>, grid_for((long long)K * Fp, 1), 256, 0, stream, K, G, Fp, d_fold,
-                   (const int*)d_fitfold.get(), d_w.get());
-        } else {
+        // weights: per-fit vectors in the [group][K][G] layout; a CV grid's
+        // weights are its fold ids (no array)
+        if (!d_fold) {
+          d_w.alloc((size_t)ngroups * K * G);
           d_stage.alloc(K);
           for (int f = 0; f < Fp; ++f) {
             const double* src = nullptr;
@@ -1568,15 +1724,27 @@ struct BatchRunner {
         CYC_CHECK_LAUNCH();
         // fixed gradient terms
         d_xjy.alloc((size_t)Fp * J);
-        launch(k_batch_xjy<T>, std::min(J, 148 * 8), kBT, 0, stream, J, K, G, ngroups, ds.d_fmt.get(), ds.d_col_ptr.get(),
-                                                                 ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(),
-                                                                 ds.d_y.get(), d_w.get(), d_xjy.get());
-        CYC_CHECK_LAUNCH();
+        if (d_fold) {
+            DevBuf<double> fs;
+            fs.alloc((size_t)J * n_folds);
+            launch(k_fold_xy, std::min(J, 148 * 8), kBT, 0, stream, J, K, n_folds, ds.d_fmt.get(), ds.d_col_ptr.get(),
+                   ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(), ds.d_y.get(), (const signed char*)d_fold8.get(),
+                   fs.get());
+            launch(k_cv_xjy, grid_for((long long)Fp * J, 4), 256, 0, stream, J, Fp, n_folds, (const double*)fs.get(),
+                   (const int*)d_fitfold.get(), d_xjy.get());
+            CYC_CHECK_CUDA(cudaStreamSynchronize(stream));   // before fs is freed
+        } else {
+            launch(k_batch_xjy<T>, std::min(J, 148 * 8), kBT, 0, stream, J, K, G, ngroups, ds.d_fmt.get(),
+                   ds.d_col_ptr.get(), ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(), ds.d_y.get(),
+                   (const T*)d_w.get(), d_xjy.get());
+        }
         if (model_grouped(ds.model)) {
             d_nw.alloc((size_t)ngroups * ds.S * G);
             d_denom.alloc((size_t)ngroups * ds.S * G);
             launch(k_batch_strata<T>, grid_for((long long)ds.S * Fp, 1), 256, 0, stream, 
-                ds.S, K, G, ngroups, ds.d_strat_ptr.get(), ds.d_y.get(), d_w.get(), d_xb.get(), d_nw.get(), d_denom.get());
+                ds.S, K, G, ngroups, ds.d_strat_ptr.get(), ds.d_y.get(), (const T*)d_w.get(),
+                (const signed char*)d_fold8.get(), (const int*)d_fitfold.get(), (const T*)d_xb.get(), d_nw.get(),
+                d_denom.get());
             CYC_CHECK_LAUNCH();
         }
         d_llfixed.alloc(Fp);
@@ -1587,12 +1755,13 @@ struct BatchRunner {
                 for (int i = 2; i <= (int)ds.y[k]; ++i) c[k] -= std::log((double)i);
             d_fixedc.alloc(K);
             CYC_CHECK_CUDA(cudaMemcpyAsync(d_fixedc.get(), c.data(), K * sizeof(double), cudaMemcpyHostToDevice, stream));
-            launch(k_batch_llfixed<T>, Fp, 256, 0, stream, K, G, Fp, d_fixedc.get(), d_w.get(), d_llfixed.get());
+            launch(k_batch_llfixed<T>, Fp, 256, 0, stream, K, G, Fp, (const double*)d_fixedc.get(), (const T*)d_w.get(),
+                   (const signed char*)d_fold8.get(), (const int*)d_fitfold.get(), d_llfixed.get());
             CYC_CHECK_LAUNCH();
             CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
         }
-        d_iter.alloc(Fp); d_flag.alloc(Fp); d_obj.alloc(Fp); d_counters.alloc(4);
-        CYC_CHECK_CUDA(cudaMemsetAsync(d_counters.get(), 0, 4 * sizeof(unsigned long long), stream));
+        d_iter.alloc(Fp); d_flag.alloc(Fp); d_obj.alloc(Fp); d_counters.alloc(3 + ngroups);
+        CYC_CHECK_CUDA(cudaMemsetAsync(d_counters.get(), 0, (3 + ngroups) * sizeof(unsigned long long), stream));
     }
 
     void run(const cyc_control& ctl, double tol, float* ms) {
@@ -1613,7 +1782,7 @@ struct BatchRunner {
         a.drow = d_drow.get();
         a.de_ptr = d_deptr.get();
         a.de_d = d_ded.get();
-        a.de_e = d_dee.get();
+        a.de_x = d_dex.get();
         a.conv = ctl.convergence_type; a.tol = tol; a.max_iter = ctl.max_iterations;
         a.out_iter = d_iter.get(); a.out_flag = d_flag.get(); a.out_obj = d_obj.get(); a.counters = d_counters.get();
         cudaEvent_t e0, e1;
@@ -1648,7 +1817,7 @@ struct BatchRunner {
     }
 
     void results(std::vector<double>& beta, std::vector<double>& hd, std::vector<int>& iters, std::vector<int>& flags,
-                 unsigned long long* counters) {
+                 std::vector<unsigned long long>& counters) {
         const int J = ds.J;
         beta.resize((size_t)F * J);
         hd.resize((size_t)F * J);
@@ -1658,7 +1827,9 @@ struct BatchRunner {
         CYC_CHECK_CUDA(cudaMemcpyAsync(hd.data(), d_hdelta.get(), hd.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(iters.data(), d_iter.get(), F * sizeof(int), cudaMemcpyDeviceToHost, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(flags.data(), d_flag.get(), F * sizeof(int), cudaMemcpyDeviceToHost, stream));
-        CYC_CHECK_CUDA(cudaMemcpyAsync(counters, d_counters.get(), 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream));
+        counters.assign(3 + ngroups, 0ull);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(counters.data(), d_counters.get(), counters.size() * sizeof(unsigned long long),
+                                       cudaMemcpyDeviceToHost, stream));
         CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
     }
 };
@@ -1669,10 +1840,12 @@ using namespace cyc;
 
 namespace {
 
-// The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` /
-// `fit_fold` select the CV-grid weights; otherwise `specs[f].weights`.
+// The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` (fold id
+// per row, `n_folds` of them) and `fit_fold` (the held-out fold of each fit)
+// select the CV-grid weights; otherwise `specs[f].weights`.
 void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F, const cyc_control* ctl,
-               cyc_fit_result* out, const int* d_fold, const std::vector<int>* fit_fold, std::vector<double>* pll) {
+               cyc_fit_result* out, const int* d_fold, int n_folds, const std::vector<int>* fit_fold,
+               std::vector<double>* pll) {
     CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
                 "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
     CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
@@ -1699,22 +1872,32 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     }
     const int G = F >= 4 ? 8 : 1;
     std::vector<int> iters, flags;
-    unsigned long long ctr[4] = {0, 0, 0, 0};
+    std::vector<unsigned long long> ctr;
     cyc_run_stats st{};
-    // algorithmic bytes of one phase: the columns each group streams, the
-    // (xb, weight) pair of every active fit per gradient entry, the xb
-    // read + write per updated entry, and the convergence passes over
-    // (xb, weight) per fit plus y once per group
+    // Algorithmic bytes of one phase (the bytes the algorithm must move, not
+    // what this kernel's layout re-reads): per cycle and column, the column's
+    // row ids and values once (every group streams them, the fits share
+    // them: the slowest group's count stands for all), per gradient visit of
+    // a fit its linear predictor and weight (a CV grid's weight is one fold
+    // byte per row shared by the group's G fits: 1/G B), per updated entry of
+    // a fit its linear predictor read and written, and per convergence check
+    // (linear predictor, weight) per fit plus y once.
     auto account = [&](int phase, float ms, const std::vector<int>& it, int s) {
         const double K = ds.K;
+        const double wb = d_fold ? 1.0 / G : (double)s;
         double conv = 0.0;
-        for (int f = 0; f < F; ++f) conv += (it[f] + 1) * K * 2.0 * s;
-        for (int g0 = 0; g0 < F; g0 += G) {
-            int mx = 0;
-            for (int f = g0; f < std::min(F, g0 + G); ++f) mx = std::max(mx, it[f]);
-            conv += (mx + 1) * K * 8.0;
+        int mx = 0;
+        for (int f = 0; f < F; ++f) {
+            conv += (it[f] + 1) * K * (s + wb);
+            mx = std::max(mx, it[f]);
         }
-        const double bytes = (double)ctr[3] + ((double)ctr[0] + (double)ctr[1]) * 2.0 * s + conv;
+        conv += (mx + 1) * K * 8.0;
+        double idx_once = 0.0, idx_all = 0.0;
+        for (size_t g = 3; g < ctr.size(); ++g) {
+            idx_once = std::max(idx_once, (double)ctr[g]);
+            idx_all += (double)ctr[g];
+        }
+        const double bytes = idx_once + (double)ctr[0] * (s + wb) + (double)ctr[1] * 2.0 * s + conv;
         st.phase_ms[phase] = ms;
         st.phase_bytes[phase] = bytes;
         st.phase_state_bytes[phase] = s;
@@ -1723,7 +1906,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         st.gradient_entries += (double)ctr[0];
         st.update_entries += (double)ctr[1];
         st.coordinate_steps += (double)ctr[2];
-        st.index_entries += (double)ctr[3];
+        st.index_entries += idx_all;
         for (int f = 0; f < F; ++f) st.cycles += it[f];
         st.launches += 1;
         st.phases = phase + 1;
@@ -1732,7 +1915,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     if (ctl->precision == CYC_MIXED) {
         // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
         BatchRunner<float> r32(ds, stream, F, G);
-        if (d_fold) r32.set_folds(d_fold, *fit_fold);
+        if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
         r32.setup(*prior, specs, beta, hd);
         float ms = 0.f;
         r32.run(*ctl, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
@@ -1742,7 +1925,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         std::fill(hd.begin(), hd.end(), ctl->initial_bound);
     }
     BatchRunner<double> r64(ds, stream, F, G);
-    if (d_fold) r64.set_folds(d_fold, *fit_fold);
+    if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
     r64.setup(*prior, specs, beta, hd);
     float ms = 0.f;
     r64.run(*ctl, ctl->tolerance, &ms);
@@ -1772,7 +1955,7 @@ extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc
                              const cyc_control* ctl, cyc_fit_result* out) {
     return guarded([&] {
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
-        run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, nullptr, nullptr);
+        run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, 0, nullptr, nullptr);
     });
 }
 
@@ -1800,7 +1983,7 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
         d_fold.alloc(ds.K);
         CYC_CHECK_CUDA(cudaMemcpy(d_fold.get(), fold_of_row, ds.K * sizeof(int), cudaMemcpyHostToDevice));
         std::vector<double> pll;
-        run_batch(ds, prior, specs.data(), F, ctl, out, d_fold.get(), &fit_fold, &pll);
+        run_batch(ds, prior, specs.data(), F, ctl, out, d_fold.get(), n_folds, &fit_fold, &pll);
         // AbstractCrossValidationDriver: NaN for fits that did not converge;
         // the grid point's estimate is the mean over folds ignoring NaN
         // (computePointEstimate, AbstractCrossValidationDriver.cpp:252-264)

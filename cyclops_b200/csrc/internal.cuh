@@ -150,7 +150,7 @@ struct RunPlan {
     std::vector<int> drow;      // row ids shared by two or more columns of a batch
     std::vector<int> de_ptr;    // J+1: entries of column j on shared rows are de_*[de_ptr[j], de_ptr[j+1])
     std::vector<int> de_d;      // shared-row slot | (column within the batch << 8)
-    std::vector<int> de_e;      // entry position within the column
+    std::vector<int> de_e;      // index of the entry's value (sparse columns), -1 for indicators
 };
 
 // ---------------------------------------------------------------------------

@@ -22,10 +22,11 @@ __host__ __device__ inline double std_max(double a, double b) { return (a < b) ?
 // getDelta: NoPrior (src/cyclops/priors/CovariatePrior.h:186-188),
 // LaplacePrior (:240-273, lambda = sqrt(2/variance), :282-292),
 // NormalPrior (:410-415)
-__host__ __device__ inline double prior_delta(int type, double variance, double beta, double g, double h) {
+// ... with the Laplace rate lambda = sqrt(2 / variance) given by the caller
+__host__ __device__ inline double prior_delta_rate(int type, double variance, double lambda, double beta, double g,
+                                                   double h) {
     if (type == CYC_PRIOR_NONE) return -(g / h);
     if (type == CYC_PRIOR_NORMAL) return -(g + (beta / variance)) / (h + (1.0 / variance));
-    const double lambda = sqrt(2.0 / variance);
     const double neg = -(g - lambda) / h;
     const double pos = -(g + lambda) / h;
     const int s = sgn(beta);
@@ -39,6 +40,10 @@ __host__ __device__ inline double prior_delta(int type, double variance, double 
         if (sgn(beta + delta) != s) delta = -beta;
     }
     return delta;
+}
+
+__host__ __device__ inline double prior_delta(int type, double variance, double beta, double g, double h) {
+    return prior_delta_rate(type, variance, type == CYC_PRIOR_LAPLACE ? sqrt(2.0 / variance) : 0.0, beta, g, h);
 }
 
 // applyBounds (src/cyclops/CyclicCoordinateDescent.cpp:1503-1520)

@@ -231,7 +231,7 @@ typedef struct {
     double gradient_entries;    /* sum over (fit, coordinate) of nnz_j */
     double update_entries;      /* sum over (fit, coordinate) with delta != 0 of nnz_j */
     double coordinate_steps;    /* (fit, coordinate) steps taken */
-    double index_entries;       /* column entries streamed per fit group */
+    double index_entries;       /* bytes of row ids / values streamed, summed over fit groups */
     double cycles;              /* sum over fits of CCD cycles */
     int launches;               /* solver kernel launches */
     int phases;                 /* 1 (FP64) or 2 (FP32, then FP64 polish) */
