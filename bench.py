@@ -142,6 +142,61 @@ def traffic_record(workload_name):
 
 
 # --------------------------------------------------------------------------
+# replicas: one process per GPU, independent grids, no data-path collective
+# --------------------------------------------------------------------------
+
+class Replicas:
+    """torchrun plumbing of the N > 1 path: each rank solves its own grid (its
+    own fold seed); the process group serves only the barriers around the
+    timed region and the max over ranks of the device times.  `backend` is
+    "nccl" on GPUs, "gloo" in the CPU tests."""
+
+    def __init__(self, backend="nccl", timeout_s=600):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend
+        self.dist = None
+        if self.world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+            self.dist = dist
+
+    def fold_seed(self, base):
+        return base + self.rank
+
+    def barrier(self):
+        if self.backend == "nccl":
+            import torch
+            torch.cuda.synchronize(self.local)
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, x):
+        if not self.dist:
+            return x
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def total_rate(self, units_per_rank, steps, ms):
+        """whole-job rate: the units all ranks processed / the slowest rank's time"""
+        return units_per_rank * self.world * steps / (ms / 1000.0)
+
+    def close(self):
+        if self.dist:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
+# --------------------------------------------------------------------------
 # CPU legs (reference engine; port if the reference was not built)
 # --------------------------------------------------------------------------
 
@@ -212,22 +267,13 @@ def run_reference(args):
 
 def run_ours(args):
     import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist_
-        dist = dist_
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    device = local
+    rep = Replicas("nccl")
+    world, rank, device = rep.world, rep.rank, rep.local
 
     from cyclops_b200 import api, build as B
     B.build()
     data, lambdas, variances, desc, gen_s = workload(args.quick)
-    folds = fold_ids(data.K, FOLD_SEED + rank)     # independent replicas per rank
+    folds = fold_ids(data.K, rep.fold_seed(FOLD_SEED))     # independent replicas per rank
     prior = api.PriorSpec(D.PRIOR_LAPLACE, 1.0, [0])
     control = api.create_control(tolerance=1e-6, precision=args.precision, polish_tolerance=1e-4,
                                  max_iterations=args.max_iterations)
@@ -238,17 +284,8 @@ def run_ours(args):
     def step():
         return api.cv_grid_fit(ds, prior, folds, N_FOLDS, variances, control)
 
-    def barrier():
-        torch.cuda.synchronize(device)
-        if dist:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if not dist:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     for _ in range(args.warmup):
         step()
@@ -274,7 +311,7 @@ def run_ours(args):
     barrier()
     launches = api.launch_count() - launches0
     ms = max_over_ranks(ev0.elapsed_time(ev1))
-    value = F * world * args.steps / (ms / 1000.0)
+    value = rep.total_rate(F, args.steps, ms)
     clocks = clk.summary()
 
     # end to end: upload from pinned host memory + solve + read back, every step
@@ -285,8 +322,7 @@ def run_ours(args):
                 "phase_ms": phase_ms, "phase_bytes": phase_bytes}
         if rank == 0:
             print(json.dumps(line))
-        if dist:
-            dist.destroy_process_group()
+        rep.close()
         return 0
     pinned = {}
     for name in ("y", "col_format", "col_ptr", "col_idx", "val_ptr", "col_val"):
@@ -312,7 +348,7 @@ def run_ours(args):
     barrier()
     ms_e2e = max_over_ranks(e0.elapsed_time(e1))
     d2h = F * data.J * 8 + F * (8 * 4)
-    e2e = F * world * args.steps / (ms_e2e / 1000.0)
+    e2e = rep.total_rate(F, args.steps, ms_e2e)
 
     line = None
     if rank == 0:
@@ -342,8 +378,7 @@ def run_ours(args):
             "cv": {"best_lambda": float(lambdas[res.best]) if res.best >= 0 else None,
                    "grid_mean_pred_loglik": [float(x) for x in res.grid_mean]},
         }
-    if dist:
-        dist.barrier()
+    rep.barrier()
     if rank == 0 and world == 1 and not args.no_baselines:
         # plain FP64 single-fit GPU CCD (host-driven loop): 2 cycles of one fit
         i0 = sample_ids(1)[0]
@@ -370,9 +405,7 @@ def run_ours(args):
         line["check"] = {"fits_compared": len(ids), "max_rel_err_beta_vs_cpu": err}
     if rank == 0:
         print(json.dumps(line))
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
