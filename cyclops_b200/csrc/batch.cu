@@ -41,6 +41,8 @@ namespace {
 
 constexpr int kBT = 256;          // threads per CTA
 constexpr int kMaxC = 8;          // CTAs per cluster (portable limit)
+// shared memory per CTA for rows arriving by cp.async (8-fit groups)
+constexpr int kAsyncBytes = 32768;
 
 struct BatchArgs {
     int model, K, J, S, C;
@@ -247,7 +249,30 @@ struct RowLayout {
     static constexpr int FPT = (G % 4 != 0) ? G : 4;
     static constexpr int TPR = G / FPT;
     static constexpr int R = 2;
+    // row parts in flight per thread when rows arrive by cp.async (their
+    // slots fit in kAsyncBytes per CTA)
+    static constexpr int D = 4;
+    static_assert(kBT * D * FPT * sizeof(T) <= kAsyncBytes, "cp.async slots exceed their shared memory");
 };
+
+// 16-byte asynchronous copies global -> shared (L2 only), one group per row
+// slot; a thread waits for its own copies only.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// one row part (FPT values, a multiple of 16 bytes) into a slot
+template <class T, int FPT>
+__device__ __forceinline__ void issue_part(T* slot, const T* src) {
+    static_assert((FPT * sizeof(T)) % 16 == 0, "row parts are whole 16-byte pieces");
+    #pragma unroll
+    for (int i = 0; i < (int)(FPT * sizeof(T)) / 16; ++i)
+        cp_async16(reinterpret_cast<char*>(slot) + 16 * i, reinterpret_cast<const char*>(src) + 16 * i);
+}
 
 // Warp sum of per-lane (g[f], h[f]), f < FPT (the lane's part lane % TPR of
 // the fits), by a butterfly reduce-scatter: each level halves the values a
@@ -304,7 +329,7 @@ __device__ __forceinline__ void block_reduce_rows(const double (&g)[FPT], const 
 
 // Where the entries of one column in this CTA's rows come from: positions
 // [e0, e1) of the column (row ids `cidx`, values `cval`), or, when staged in
-// shared memory, sidx / sx [0, e1 - e0).
+// shared memory, sidx / sx [0, e1 - e0) (values from `cval` when sx is null).
 template <class T>
 struct ColRows {
     const int* cidx;
@@ -317,7 +342,7 @@ struct ColRows {
         if (e >= e1) { k = -1; x = T(1); return; }
         if (sidx) {
             k = sidx[e - e0];
-            x = ind ? T(1) : sx[e - e0];
+            x = ind ? T(1) : (sx ? sx[e - e0] : (T)__ldg(cval + e));
         } else {
             k = dense ? e : __ldg(cidx + e);
             x = ind ? T(1) : (T)__ldg(cval + e);
@@ -328,96 +353,113 @@ struct ColRows {
 // Gradient and Hessian terms of the group's fits over the entries of a column
 // (an independent-rows model), by the STRIDE threads t0 = 0 .. STRIDE-1:
 // thread t takes rows t / TPR, t / TPR + STRIDE / TPR, ... and fits part
-// t % TPR of each, loaded as one vector.  `wmask[fold]` holds the fits that
-// train on rows of that fold (CV grid); `done` the fits that have converged
-// (skipped).
+// t % TPR of each.  Two-stage pipeline per thread: a row's id (and value,
+// fold id) loads 2D rows ahead; its part of the linear predictors arrives by
+// cp.async into the thread's D slots (`abuf`) D rows ahead of the one being
+// summed.  `wmask[fold]` holds the fits that train on rows of that fold (CV
+// grid); `done` the fits that have converged (skipped).
 template <class T, int MODEL, int G, int WM, int STRIDE>
 __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xbg, const T* wg,
-                                        const signed char* fold, const unsigned char* wmask, unsigned done,
+                                        const signed char* fold, const unsigned char* wmask, unsigned done, T* abuf,
                                         double (&g)[RowLayout<T, G, STRIDE == kBT>::FPT],
                                         double (&h)[RowLayout<T, G, STRIDE == kBT>::FPT]) {
     using Lay = RowLayout<T, G, STRIDE == kBT>;
-    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, D = Lay::D, RS = STRIDE / TPR;
     const int f0 = (t0 % TPR) * FPT;
     const unsigned dn = done >> f0;
     Kahan<T> ag[FPT], ah[FPT];
     int base = c.e0 + t0 / TPR;
-    int k[R];
-    T x[R];
+    int k[D], kn[D], fd[D];                  // rows in the slots, and the rows after them
+    T x[D], xn[D];
+    T w[D][FPT];
+    auto fetch = [&](int s, int e) { c.get(e, kn[s], xn[s]); };   // stage 1: id and value
+    auto issue = [&](int s) {                // stage 2: the row part into slot s, its fold id
+        k[s] = kn[s];
+        x[s] = xn[s];
+        fd[s] = 0;
+        if (k[s] >= 0) {
+            issue_part<T, FPT>(abuf + s * FPT, xbg + (size_t)k[s] * G + f0);
+            if (WM == 0) load_row<T, FPT>(wg + (size_t)k[s] * G + f0, w[s]);
+            else fd[s] = (int)__ldg(fold + k[s]);
+        }
+        cp_async_commit();
+    };
     #pragma unroll
-    for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
-    for (; base < c.e1; base += R * RS) {
-        T v[R][FPT], w[R][FPT];
-        unsigned wm[R];
-        #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (k[r] >= 0) {
-                load_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
-                if (WM == 0) load_row<T, FPT>(wg + (size_t)k[r] * G + f0, w[r]);
-                else wm[r] = (unsigned)wmask[(int)__ldg(fold + k[r])] >> f0;
-            } else {
-                wm[r] = 0u;
-                #pragma unroll
-                for (int f = 0; f < FPT; ++f) { v[r][f] = T(0); w[r][f] = T(0); }
-            }
-        }
-        // the next rows' ids load while these rows' values arrive
-        int kn[R];
-        T xn[R];
-        #pragma unroll
-        for (int r = 0; r < R; ++r) c.get(base + (R + r) * RS, kn[r], xn[r]);
-        #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (k[r] < 0) continue;
-            #pragma unroll
-            for (int f = 0; f < FPT; ++f) {
-                if ((dn >> f) & 1u) continue;
-                const T wt = (WM == 1) ? (((wm[r] >> f) & 1u) ? T(1) : T(0)) : w[r][f];
-                row_gh<T, MODEL>(v[r][f], x[r], wt, c.ind, ag[f], ah[f]);
-            }
-        }
-        #pragma unroll
-        for (int r = 0; r < R; ++r) { k[r] = kn[r]; x[r] = xn[r]; }
+    for (int s = 0; s < D; ++s) fetch(s, base + s * RS);
+    #pragma unroll
+    for (int s = 0; s < D; ++s) {
+        issue(s);
+        fetch(s, base + (D + s) * RS);
     }
+    for (; base < c.e1; base += D * RS) {
+        #pragma unroll
+        for (int s = 0; s < D; ++s) {
+            cp_async_wait<D - 1>();
+            if (k[s] >= 0) {
+                T v[FPT];
+                load_row<T, FPT>(abuf + s * FPT, v);
+                const unsigned wm = (WM == 1) ? (unsigned)wmask[fd[s]] >> f0 : 0u;
+                #pragma unroll
+                for (int f = 0; f < FPT; ++f) {
+                    if ((dn >> f) & 1u) continue;
+                    const T wt = (WM == 1) ? (((wm >> f) & 1u) ? T(1) : T(0)) : w[s][f];
+                    row_gh<T, MODEL>(v[f], x[s], wt, c.ind, ag[f], ah[f]);
+                }
+            }
+            issue(s);
+            fetch(s, base + (2 * D + s) * RS);
+        }
+    }
+    cp_async_wait<0>();
     #pragma unroll
     for (int f = 0; f < FPT; ++f) { g[f] = ag[f].value(); h[f] = ah[f].value(); }
 }
 
 // updateXBeta over the entries of a column by the STRIDE threads t0 (same
-// split as rows_gh)
+// split and the same two-stage pipeline as rows_gh; the new values are stored
+// from registers)
 template <class T, int G, int STRIDE>
-__device__ __forceinline__ void rows_update(const ColRows<T>& c, int t0, T* xbg, const T (&d)[G]) {
+__device__ __forceinline__ void rows_update(const ColRows<T>& c, int t0, T* xbg, const T (&d)[G], T* abuf) {
     using Lay = RowLayout<T, G, STRIDE == kBT>;
-    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, R = Lay::R, RS = STRIDE / TPR;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, D = Lay::D, RS = STRIDE / TPR;
     const int f0 = (t0 % TPR) * FPT;
     bool moved = false;                     // a part whose fits all kept their coefficients stays
     #pragma unroll
     for (int f = 0; f < FPT; ++f) moved |= (d[f0 + f] != T(0));
     if (!moved) return;
     int base = c.e0 + t0 / TPR;
-    int k[R];
-    T x[R];
+    int k[D], kn[D];
+    T x[D], xn[D];
+    auto fetch = [&](int s, int e) { c.get(e, kn[s], xn[s]); };
+    auto issue = [&](int s) {
+        k[s] = kn[s];
+        x[s] = xn[s];
+        if (k[s] >= 0) issue_part<T, FPT>(abuf + s * FPT, xbg + (size_t)k[s] * G + f0);
+        cp_async_commit();
+    };
     #pragma unroll
-    for (int r = 0; r < R; ++r) c.get(base + r * RS, k[r], x[r]);
-    for (; base < c.e1; base += R * RS) {
-        T v[R][FPT];
-        #pragma unroll
-        for (int r = 0; r < R; ++r)
-            if (k[r] >= 0) load_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
-        int kn[R];
-        T xn[R];
-        #pragma unroll
-        for (int r = 0; r < R; ++r) c.get(base + (R + r) * RS, kn[r], xn[r]);
-        #pragma unroll
-        for (int r = 0; r < R; ++r) {
-            if (k[r] < 0) continue;
-            #pragma unroll
-            for (int f = 0; f < FPT; ++f) v[r][f] = upd_fma(d[f0 + f], x[r], v[r][f]);
-            store_row<T, FPT>(xbg + (size_t)k[r] * G + f0, v[r]);
-        }
-        #pragma unroll
-        for (int r = 0; r < R; ++r) { k[r] = kn[r]; x[r] = xn[r]; }
+    for (int s = 0; s < D; ++s) fetch(s, base + s * RS);
+    #pragma unroll
+    for (int s = 0; s < D; ++s) {
+        issue(s);
+        fetch(s, base + (D + s) * RS);
     }
+    for (; base < c.e1; base += D * RS) {
+        #pragma unroll
+        for (int s = 0; s < D; ++s) {
+            cp_async_wait<D - 1>();
+            if (k[s] >= 0) {
+                T v[FPT];
+                load_row<T, FPT>(abuf + s * FPT, v);
+                #pragma unroll
+                for (int f = 0; f < FPT; ++f) v[f] = upd_fma(d[f0 + f], x[s], v[f]);
+                store_row<T, FPT>(xbg + (size_t)k[s] * G + f0, v);
+            }
+            issue(s);
+            fetch(s, base + (2 * D + s) * RS);
+        }
+    }
+    cp_async_wait<0>();
 }
 
 // updateXBeta of a batch's columns over this CTA's rows, flat: item i is part
@@ -452,7 +494,7 @@ __device__ __forceinline__ void batch_update(T* xbg, const int* idx, const doubl
             w[u] = c;
             if (off[qq] >= 0) {
                 k[u] = sidx[off[qq] + e];
-                if (fmt[qq] == CYC_SPARSE) x[u] = sx[off[qq] + e];
+                if (fmt[qq] == CYC_SPARSE) x[u] = sx ? sx[off[qq] + e] : (T)__ldg(val + vp[qq] + e0[qq] + e);
             } else {
                 k[u] = __ldg(idx + cp[qq] + e0[qq] + e);
                 if (fmt[qq] == CYC_SPARSE) x[u] = (T)__ldg(val + vp[qq] + e0[qq] + e);
@@ -510,6 +552,14 @@ constexpr int kRunItems = 8;
 constexpr int kDirtyMax = 32;
 constexpr int kBatchCap = 256;
 
+// 8-fit groups of independent-rows models take the thread-per-row paths
+template <int MODEL, int G>
+constexpr bool row_stream() { return G == 8 && MODEL != CYC_CLR && MODEL != CYC_CPR; }
+
+// bytes after the staged row ids: staged values, or the cp.async row slots
+template <class T, int MODEL, int G>
+constexpr size_t staged_value_bytes() { return row_stream<MODEL, G>() ? (size_t)kAsyncBytes : kStage * sizeof(T); }
+
 template <class T, int MODEL, int G, int WM>
 __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     cg::cluster_group cluster = cg::this_cluster();
@@ -520,7 +570,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     const bool grouped = (MODEL == CYC_CLR || MODEL == CYC_CPR);
     // independent rows, 8 fits per group: columns stream thread per row (all
     // fits of a row by vector loads) and short columns go in batches
-    constexpr bool kRowStream = (G == 8) && !(MODEL == CYC_CLR || MODEL == CYC_CPR);
+    constexpr bool kRowStream = row_stream<MODEL, G>();
     using LayW = RowLayout<T, G, false>;   // a warp per column (batches)
     using LayB = RowLayout<T, G, true>;    // the CTA per column (single columns)
     // strata of my rows (partition boundaries are stratum starts); none if my range is empty
@@ -577,12 +627,16 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     double (*c_hd)[G] = reinterpret_cast<double (*)[G]>(dyn_smem + kChunk * G * sizeof(double));
     double (*c_xjy)[G] = reinterpret_cast<double (*)[G]>(dyn_smem + 2 * kChunk * G * sizeof(double));
     int* s_sidx = reinterpret_cast<int*>(dyn_smem + 3 * kChunk * G * sizeof(double));
+    // staged values of short sparse columns (per-lane paths), or, for 8-fit
+    // groups of independent-rows models, each thread's cp.async row slots
     T* s_sx = reinterpret_cast<T*>(dyn_smem + 3 * kChunk * G * sizeof(double) + kStage * sizeof(int));
+    T* s_abuf = s_sx + (size_t)threadIdx.x * LayB::D * LayB::FPT;
     // shared rows of the open batch: as pushed by their owners (by parity),
     // the working copy of the serial replay, and their weights
-    T (*s_dst)[kDirtyMax][G] = reinterpret_cast<T (*)[kDirtyMax][G]>(s_sx + kStage);
-    T (*s_dcur)[G] = reinterpret_cast<T (*)[G]>(s_sx + kStage + 2 * kDirtyMax * G);
-    T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_sx + kStage + 3 * kDirtyMax * G);
+    T* s_dirty = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(s_sx) + staged_value_bytes<T, MODEL, G>());
+    T (*s_dst)[kDirtyMax][G] = reinterpret_cast<T (*)[kDirtyMax][G]>(s_dirty);
+    T (*s_dcur)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 2 * kDirtyMax * G);
+    T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 3 * kDirtyMax * G);
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
     if (threadIdx.x < G) {
@@ -723,7 +777,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 const int qq = c_sq[lo];
                 const long long e = c_e0[qq] + (t - c_soff[lo]);
                 s_sidx[t] = __ldg(A.idx + c_cp[qq] + e);
-                s_sx[t] = (c_fmt[qq] == CYC_SPARSE) ? (T)__ldg(A.val + c_vp[qq] + e) : T(1);
+                if constexpr (!kRowStream) s_sx[t] = (c_fmt[qq] == CYC_SPARSE) ? (T)__ldg(A.val + c_vp[qq] + e) : T(1);
             }
         }
         __syncthreads();
@@ -761,10 +815,9 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 if (warp < L) {
                     const int qq = q + warp, so = c_off[qq];
                     const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
-                                        so >= 0 ? s_sx + so : nullptr, c_e0[qq], c_e1[qq], false,
-                                        c_fmt[qq] == CYC_INDICATOR};
+                                        nullptr, c_e0[qq], c_e1[qq], false, c_fmt[qq] == CYC_INDICATOR};
                     double g[LayW::FPT], h[LayW::FPT];
-                    rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, g, h);
+                    rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
                     int fit;
                     bool is_h, holder;
                     const double v = warp_reduce_rows<LayW::FPT, LayW::TPR>(g, h, fit, is_h, holder);
@@ -794,11 +847,13 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         if (!((done_m >> fw) & 1u))
                             for (int i = i0 + sl; i < i1; i += 32 / G) {
                                 const int d = s_bde_d[i];
+                                const T vc = s_dcur[d][fw], vs = s_dst[par][d][fw];
+                                if (vc == vs) continue;        // not moved yet: the change is exactly zero
                                 const T x = (T)s_bde_x[i];
                                 const T wt = (WM == 1) ? (((s_dwm[d] >> fw) & 1u) ? T(1) : T(0)) : s_dw[d][fw];
                                 T g1, h1, g0, h0;
-                                row_terms<T, MODEL>(s_dcur[d][fw], x, wt, ind, g1, h1);
-                                row_terms<T, MODEL>(s_dst[par][d][fw], x, wt, ind, g0, h0);
+                                row_terms<T, MODEL>(vc, x, wt, ind, g1, h1);
+                                row_terms<T, MODEL>(vs, x, wt, ind, g0, h0);
                                 gc += (double)g1 - (double)g0;
                                 hc += (double)h1 - (double)h0;
                             }
@@ -844,7 +899,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                     s_boff[L] = o;
                 }
                 __syncthreads();
-                batch_update<T, G>(xbg, A.idx, A.val, s_sidx, s_sx, c_cp, c_vp, c_e0, c_off, c_fmt, q, L, s_boff,
+                batch_update<T, G>(xbg, A.idx, A.val, s_sidx, nullptr, c_cp, c_vp, c_e0, c_off, c_fmt, q, L, s_boff,
                                    s_dr, s_drow, nd);
                 for (int t = threadIdx.x; t < nd * G; t += kBT) {
                     const int d = t / G, k = s_drow[d];
@@ -860,11 +915,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             {
                 const int fmt = c_fmt[q], so = c_off[q];
                 const bool dense = (fmt == CYC_DENSE || fmt == CYC_INTERCEPT);
-                const ColRows<T> cr{A.idx + c_cp[q], A.val + c_vp[q], so >= 0 ? s_sidx + so : nullptr,
-                                    so >= 0 ? s_sx + so : nullptr, c_e0[q], c_e1[q], dense,
-                                    fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT};
+                const ColRows<T> cr{A.idx + c_cp[q], A.val + c_vp[q], so >= 0 ? s_sidx + so : nullptr, nullptr,
+                                    c_e0[q], c_e1[q], dense, fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT};
                 double g[LayB::FPT], h[LayB::FPT];
-                rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, g, h);
+                rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
                 block_reduce_rows<G, LayB::FPT, LayB::TPR>(g, h, s_red, reinterpret_cast<double*>(s_scr));
                 if (threadIdx.x < G)
                     for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
@@ -884,7 +938,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 #pragma unroll
                 for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[0][f]; any |= (s_dr[0][f] != 0.0); }
                 if (rank == 0 && threadIdx.x == 0) count_run(q, 1);
-                if (any) rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd);
+                if (any) rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd, s_abuf);
                 __syncthreads();
                 par ^= 1;
                 ++q;
@@ -1557,7 +1611,7 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
-    const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * (sizeof(int) + sizeof(T)) +
+    const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * sizeof(int) + staged_value_bytes<T, MODEL, G>() +
                        4 * kDirtyMax * G * sizeof(T);
     CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     cfg.dynamicSmemBytes = dyn;
