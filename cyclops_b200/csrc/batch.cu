@@ -1918,6 +1918,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     cudaStream_t stream;
     CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{stream};
+    StreamScope scope(stream);   // every buffer of this solve lives on `stream`
     const int J = ds.J;
     std::vector<double> beta((size_t)F * J, 0.0), hd((size_t)F * J, ctl->initial_bound);
     for (int f = 0; f < F; ++f) {
@@ -2033,9 +2034,11 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
             specs[i].start_beta = nullptr;
             fit_fold[i] = i % n_folds;
         }
+        StreamScope scope(ds.stream);
         DevBuf<int> d_fold;
         d_fold.alloc(ds.K);
-        CYC_CHECK_CUDA(cudaMemcpy(d_fold.get(), fold_of_row, ds.K * sizeof(int), cudaMemcpyHostToDevice));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_fold.get(), fold_of_row, ds.K * sizeof(int), cudaMemcpyHostToDevice, ds.stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(ds.stream));
         std::vector<double> pll;
         run_batch(ds, prior, specs.data(), F, ctl, out, d_fold.get(), n_folds, &fit_fold, &pll);
         // AbstractCrossValidationDriver: NaN for fits that did not converge;

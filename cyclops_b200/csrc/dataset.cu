@@ -30,20 +30,70 @@ void set_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
+namespace {
+std::mutex g_pinned_mutex;
+std::vector<void*>& pinned_free() {
+    static std::vector<void*>* v = new std::vector<void*>();   // lives to process exit
+    return *v;
+}
+}  // namespace
+
+void* pinned_block() {
+    std::lock_guard<std::mutex> lk(g_pinned_mutex);
+    auto& fl = pinned_free();
+    if (fl.empty()) {
+        char* chunk = nullptr;
+        CYC_CHECK_CUDA(cudaMallocHost(reinterpret_cast<void**>(&chunk), 64 * 512));
+        for (int i = 511; i >= 0; --i) fl.push_back(chunk + 64 * i);
+    }
+    void* p = fl.back();
+    fl.pop_back();
+    return p;
+}
+
+void release_pinned_block(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pinned_mutex);
+    pinned_free().push_back(p);
+}
+
+cudaStream_t& alloc_stream() {
+    static thread_local cudaStream_t s = nullptr;
+    return s;
+}
+
+// freed memory stays in the device's default pool for the next allocation
+// instead of going back to the driver at every synchronisation (a setting of
+// this process's pool, not of the GPU)
+void prepare_pool(int device) {
+    static std::mutex m;
+    static std::vector<int> done;
+    std::lock_guard<std::mutex> lk(m);
+    for (int d : done)
+        if (d == device) return;
+    cudaMemPool_t pool;
+    CYC_CHECK_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+    unsigned long long keep = ~0ull;
+    CYC_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    done.push_back(device);
+}
+
 size_t Dataset::device_bytes() const {
     return d_fmt.bytes() + d_col_ptr.bytes() + d_val_ptr.bytes() + d_idx.bytes() + d_val.bytes() +
            d_y.bytes() + d_time.bytes() + d_strat.bytes() + d_strat_ptr.bytes() + d_row_ptr.bytes() +
            d_row_col.bytes() + d_row_val.bytes();
 }
 
+// on the calling thread's allocation stream (the dataset's, during uploads)
 template <class T>
 static void upload(DevBuf<T>& buf, const T* src, size_t n) {
     buf.alloc(n);
-    if (n) CYC_CHECK_CUDA(cudaMemcpy(buf.get(), src, n * sizeof(T), cudaMemcpyHostToDevice));
+    if (n) CYC_CHECK_CUDA(cudaMemcpyAsync(buf.get(), src, n * sizeof(T), cudaMemcpyHostToDevice, alloc_stream()));
 }
 
 void Dataset::ensure_csr() {
     if (have_csr) return;
+    StreamScope scope(stream);
     // counting sort by row; columns visited in ascending order, so each row
     // lists its columns ascending (the order of zeroXBeta + axpyXBeta per j,
     // CyclicCoordinateDescent.cpp:1452-1470)
@@ -61,7 +111,10 @@ void Dataset::ensure_csr() {
     std::vector<int> rc(rp[K]);
     std::vector<double> rv(rp[K]);
     std::vector<double> hval(nnz_val);
-    if (nnz_val) CYC_CHECK_CUDA(cudaMemcpy(hval.data(), d_val.get(), nnz_val * sizeof(double), cudaMemcpyDeviceToHost));
+    if (nnz_val) {
+        CYC_CHECK_CUDA(cudaMemcpyAsync(hval.data(), d_val.get(), nnz_val * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+    }
     for (int j = 0; j < J; ++j) {
         const int f = fmt[j];
         const long long n = col_len(j);
@@ -76,6 +129,7 @@ void Dataset::ensure_csr() {
     upload(d_row_ptr, rp.data(), rp.size());
     upload(d_row_col, rc.data(), rc.size());
     upload(d_row_val, rv.data(), rv.size());
+    CYC_CHECK_CUDA(cudaStreamSynchronize(stream));   // usable from every stream
     have_csr = true;
 }
 
@@ -104,6 +158,10 @@ extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_datase
         std::unique_ptr<cyc_dataset> guard(h);
         Dataset& s = h->ds;
         s.device = device;
+        prepare_pool(device);
+        CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&s.own.s, cudaStreamNonBlocking));
+        s.stream = s.own.s;
+        StreamScope scope(s.stream);
         s.model = d->model;
         s.K = d->K;
         s.J = d->J;
@@ -167,6 +225,7 @@ extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_datase
         if (d->time) upload(s.d_time, d->time, (size_t)d->K);
         upload(s.d_strat, s.strat.data(), s.strat.size());
         upload(s.d_strat_ptr, s.strat_ptr.data(), s.strat_ptr.size());
+        CYC_CHECK_CUDA(cudaStreamSynchronize(s.stream));   // usable from every stream
         *out = guard.release();
     });
 }

@@ -19,8 +19,9 @@ namespace cyc {
 
 Engine::Engine(Dataset* d) : ds(d), device(d->device) {
     CYC_CHECK_CUDA(cudaSetDevice(ds->device));
-    CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    CYC_CHECK_CUDA(cudaMallocHost(&h_result, 8 * sizeof(double)));
+    CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&own.s, cudaStreamNonBlocking));
+    stream = own.s;
+    StreamScope scope(stream);
     model = ds->model;
     const int K = ds->K;
     // initialize (ModelSpecifics.hpp:1899-1952)
@@ -46,9 +47,8 @@ Engine::Engine(Dataset* d) : ds(d), device(d->device) {
 }
 
 Engine::~Engine() {
+    // the buffers are freed on the stream after its work; `own` then releases it
     cudaSetDevice(device);
-    if (stream) cudaStreamDestroy(stream);
-    if (h_result) cudaFreeHost(h_result);
 }
 
 void Engine::sync() { CYC_CHECK_CUDA(cudaStreamSynchronize(stream)); }
@@ -479,6 +479,7 @@ using namespace cyc;
     guarded([&] {                                                              \
         CYC_REQUIRE((e) != nullptr, CYC_ERR_ARGUMENT, "null engine");          \
         CYC_CHECK_CUDA(cudaSetDevice((e)->eng->ds->device));                   \
+        StreamScope scope_((e)->eng->stream);                                  \
         body;                                                                  \
     })
 

@@ -12,6 +12,7 @@ struct Engine {
     Engine(const Engine&) = delete;
     Engine& operator=(const Engine&) = delete;
 
+    OwnedStream own;              // the engine's stream (declared first: destroyed last)
     Dataset* ds;                  // borrowed: the caller keeps the dataset alive
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -25,7 +26,8 @@ struct Engine {
     DevBuf<double2> partial;
     DevBuf<unsigned> ticket;
     DevBuf<double> result, ll_fixed;
-    double* h_result = nullptr;   // pinned
+    PinnedBlock h_block;          // results read back (pinned, from the process-wide pool)
+    double* h_result = h_block.as<double>();
 
     // cox
     DevBuf<int> group, grow_ptr, gstart, gend, glist;

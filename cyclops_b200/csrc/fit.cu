@@ -95,7 +95,8 @@ struct FitRunner {
     DevBuf<int> ptype, flags;
     DevBuf<unsigned long long> n_updates;
     double variance;
-    int* h_flags = nullptr;
+    PinnedBlock h_block;                 // two flags read back per cycle (pinned, pooled)
+    int* h_flags = h_block.as<int>();
     std::vector<cudaGraphExec_t> graphs;
     std::vector<double> h_start;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -115,14 +116,12 @@ struct FitRunner {
         ptype.alloc(J); flags.alloc(2); n_updates.alloc(1);
         CYC_CHECK_CUDA(cudaMemcpyAsync(ptype.get(), pt.data(), J * sizeof(int), cudaMemcpyHostToDevice, e.stream));
         CYC_CHECK_CUDA(cudaMemsetAsync(n_updates.get(), 0, sizeof(unsigned long long), e.stream));
-        CYC_CHECK_CUDA(cudaMallocHost(&h_flags, 2 * sizeof(int)));
         CYC_CHECK_CUDA(cudaEventCreate(&ev0));
         CYC_CHECK_CUDA(cudaEventCreate(&ev1));
         e.sync();
     }
     ~FitRunner() {
         for (auto g : graphs) cudaGraphExecDestroy(g);
-        if (h_flags) cudaFreeHost(h_flags);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
     }
@@ -394,6 +393,7 @@ extern "C" int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_sp
                     "prior variance must be positive");
         CYC_CHECK_CUDA(cudaSetDevice(ds->ds.device));
         Engine eng(&ds->ds);
+        StreamScope scope(eng.stream);
         eng.set_weights(spec->weights, spec->weights != nullptr);
         FitRunner r(eng, *prior, *spec, *control);
         r.run(out);
@@ -408,6 +408,7 @@ extern "C" int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const 
                     CYC_ERR_ARGUMENT, "Unknown prior type");
         CYC_CHECK_CUDA(cudaSetDevice(ds->ds.device));
         Engine eng(&ds->ds);
+        StreamScope scope(eng.stream);
         eng.set_weights(spec->weights, spec->weights != nullptr);
         cudaEvent_t e0, e1;
         CYC_CHECK_CUDA(cudaEventCreate(&e0));

@@ -82,17 +82,64 @@ int guarded(F&& f) {
     }
 }
 
+// Device memory is stream-ordered: a buffer is allocated (cudaMallocAsync) on
+// the stream its owner set for the calling thread (StreamScope) and freed
+// (cudaFreeAsync) on that same stream, after the owner's work on it.  Neither
+// waits for other streams, so fits running side by side on one device never
+// stall one another the way cudaMalloc / cudaFree (device-wide waits) would.
+// Without a scope a buffer falls back to cudaMalloc / cudaFree.
+cudaStream_t& alloc_stream();          // per thread
+void prepare_pool(int device);         // keeps freed memory cached in the device's pool
+
+struct StreamScope {
+    cudaStream_t prev;
+    explicit StreamScope(cudaStream_t s) : prev(alloc_stream()) { alloc_stream() = s; }
+    ~StreamScope() { alloc_stream() = prev; }
+    StreamScope(const StreamScope&) = delete;
+    StreamScope& operator=(const StreamScope&) = delete;
+};
+
+// a stream owned by an object; declared first among the owner's members so
+// that it is destroyed last, after every buffer freed on it
+struct OwnedStream {
+    cudaStream_t s = nullptr;
+    OwnedStream() = default;
+    OwnedStream(const OwnedStream&) = delete;
+    OwnedStream& operator=(const OwnedStream&) = delete;
+    ~OwnedStream() { if (s) cudaStreamDestroy(s); }
+};
+
+// 64 pinned host bytes from a process-wide pool (allocated in chunks, never
+// freed: cudaFreeHost would wait for the whole device)
+void* pinned_block();
+void release_pinned_block(void* p);
+
+struct PinnedBlock {
+    void* p = nullptr;
+    PinnedBlock() : p(pinned_block()) {}
+    ~PinnedBlock() { release_pinned_block(p); }
+    PinnedBlock(const PinnedBlock&) = delete;
+    PinnedBlock& operator=(const PinnedBlock&) = delete;
+    template <class T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
 // device buffer with RAII
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;
+    bool ordered = false;
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (ordered) cudaFreeAsync(p, s);
+            else cudaFree(p);
+        }
         p = nullptr;
         n = 0;
     }
@@ -100,7 +147,10 @@ struct DevBuf {
         if (count == n && p) return;
         release();
         if (count == 0) return;
-        CYC_CHECK_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        s = alloc_stream();
+        ordered = (s != nullptr);
+        if (ordered) CYC_CHECK_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s));
+        else CYC_CHECK_CUDA(cudaMalloc(&p, count * sizeof(T)));
         n = count;
     }
     size_t bytes() const { return n * sizeof(T); }
@@ -157,6 +207,8 @@ struct RunPlan {
 // dataset
 // ---------------------------------------------------------------------------
 struct Dataset {
+    OwnedStream own;                // uploads and the dataset's buffers (declared first: destroyed last)
+    cudaStream_t stream = nullptr;
     int device = 0;
     int model = 0;
     int K = 0, J = 0;
