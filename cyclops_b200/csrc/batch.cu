@@ -173,18 +173,30 @@ __device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp,
 // (Logistic / PoissonRegression::incrementGradientAndHessian,
 // ModelSpecifics.h:540-568, 1508-1543); the logistic probability is formed as
 // 1 / (1 + exp(-xb)), which equals exb / (1 + exb) without overflowing
+// the row's mean under the model: the logistic probability, or exp(xb)
 template <class T, int MODEL>
-__device__ __forceinline__ void row_terms(T v, T x, T wt, bool ind, T& gi, T& hi) {
+__device__ __forceinline__ T row_mean(T v) {
+    if (MODEL == CYC_LR) return T(1) / (T(1) + fexp(-v));
+    return fexp(v);
+}
+
+// (gradient, Hessian) terms of one entry from its row's mean
+template <class T, int MODEL>
+__device__ __forceinline__ void mean_terms(T m, T x, T wt, bool ind, T& gi, T& hi) {
     if (MODEL == CYC_LR) {
-        const T p = T(1) / (T(1) + fexp(-v));
-        const T g1 = p * x;
+        const T g1 = m * x;
         gi = wt * g1;
-        hi = wt * (ind ? g1 * (T(1) - g1) : x * x * p * (T(1) - p));
+        hi = wt * (ind ? g1 * (T(1) - g1) : x * x * m * (T(1) - m));
     } else {
-        const T n1 = fexp(v) * x;
+        const T n1 = m * x;
         gi = wt * n1;
         hi = wt * (ind ? n1 : n1 * x);
     }
+}
+
+template <class T, int MODEL>
+__device__ __forceinline__ void row_terms(T v, T x, T wt, bool ind, T& gi, T& hi) {
+    mean_terms<T, MODEL>(row_mean<T, MODEL>(v), x, wt, ind, gi, hi);
 }
 
 template <class T, int MODEL>
@@ -551,6 +563,8 @@ constexpr int kRunItems = 8;
 // k_batch).  Columns of at most kBatchCap entries in every CTA's rows join.
 constexpr int kDirtyMax = 32;
 constexpr int kBatchCap = 256;
+// levels of the serial replay a batch may have (each costs a step chain)
+constexpr int kLevelMax = kRunMax;
 
 // 8-fit groups of independent-rows models take the thread-per-row paths
 template <int MODEL, int G>
@@ -631,12 +645,14 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     // groups of independent-rows models, each thread's cp.async row slots
     T* s_sx = reinterpret_cast<T*>(dyn_smem + 3 * kChunk * G * sizeof(double) + kStage * sizeof(int));
     T* s_abuf = s_sx + (size_t)threadIdx.x * LayB::D * LayB::FPT;
-    // shared rows of the open batch: as pushed by their owners (by parity),
-    // the working copy of the serial replay, and their weights
+    // shared rows of the open batch: as pushed by their owners (by parity; the
+    // replay then moves this CTA's copy of the current parity in place), their
+    // model means at the batch's start and now, and their weights
     T* s_dirty = reinterpret_cast<T*>(reinterpret_cast<unsigned char*>(s_sx) + staged_value_bytes<T, MODEL, G>());
     T (*s_dst)[kDirtyMax][G] = reinterpret_cast<T (*)[kDirtyMax][G]>(s_dirty);
-    T (*s_dcur)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 2 * kDirtyMax * G);
-    T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 3 * kDirtyMax * G);
+    T (*s_m0)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 2 * kDirtyMax * G);
+    T (*s_mc)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 3 * kDirtyMax * G);
+    T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 4 * kDirtyMax * G);
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
     if (threadIdx.x < G) {
@@ -830,9 +846,15 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 // the serial steps, replayed identically in every CTA: level by
                 // level, a column's (g, h) is its partials plus, for each of its
                 // entries on a shared row, the change of that row's terms since
-                // the batch's start (zero unless an earlier column moved it)
+                // the batch's start (zero unless an earlier column moved it).
+                // The shared rows move in place in s_dst[par]; their means at the
+                // start (s_m0) and now (s_mc) make a correction exp-free.
                 if (nd > 0) {
-                    for (int t = threadIdx.x; t < nd * G; t += kBT) s_dcur[t / G][t % G] = s_dst[par][t / G][t % G];
+                    for (int t = threadIdx.x; t < nd * G; t += kBT) {
+                        const T m = row_mean<T, MODEL>(s_dst[par][t / G][t % G]);
+                        s_m0[t / G][t % G] = m;
+                        s_mc[t / G][t % G] = m;
+                    }
                     __syncthreads();
                 }
                 int nlev = 1;
@@ -847,13 +869,13 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         if (!((done_m >> fw) & 1u))
                             for (int i = i0 + sl; i < i1; i += 32 / G) {
                                 const int d = s_bde_d[i];
-                                const T vc = s_dcur[d][fw], vs = s_dst[par][d][fw];
-                                if (vc == vs) continue;        // not moved yet: the change is exactly zero
+                                const T mc = s_mc[d][fw], m0 = s_m0[d][fw];
+                                if (mc == m0) continue;        // not moved yet: the change is exactly zero
                                 const T x = (T)s_bde_x[i];
                                 const T wt = (WM == 1) ? (((s_dwm[d] >> fw) & 1u) ? T(1) : T(0)) : s_dw[d][fw];
                                 T g1, h1, g0, h0;
-                                row_terms<T, MODEL>(vc, x, wt, ind, g1, h1);
-                                row_terms<T, MODEL>(vs, x, wt, ind, g0, h0);
+                                mean_terms<T, MODEL>(mc, x, wt, ind, g1, h1);
+                                mean_terms<T, MODEL>(m0, x, wt, ind, g0, h0);
                                 gc += (double)g1 - (double)g0;
                                 hc += (double)h1 - (double)h0;
                             }
@@ -863,14 +885,23 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         }
                         double dl = 0.0;
                         if (lane < G) {
-                            double g = 0.0, h = 0.0;
-                            for (int r = 0; r < C; ++r) {
-                                const double2 pp = s_part[par][r][warp][lane];
-                                g += pp.x;
-                                h += pp.y;
+                            // the CTAs' partials summed as a tree (the same order in every CTA)
+                            double gv[kMaxC], hv[kMaxC];
+                            #pragma unroll
+                            for (int r = 0; r < kMaxC; ++r) {
+                                const double2 pp = r < C ? s_part[par][r][warp][lane] : make_double2(0.0, 0.0);
+                                gv[r] = pp.x;
+                                hv[r] = pp.y;
                             }
-                            g += gc;
-                            h += hc;
+                            #pragma unroll
+                            for (int st = 1; st < kMaxC; st <<= 1) {
+                                #pragma unroll
+                                for (int r = 0; r + st < kMaxC; r += 2 * st) {
+                                    gv[r] += gv[r + st];
+                                    hv[r] += hv[r + st];
+                                }
+                            }
+                            const double g = gv[0] + gc, h = hv[0] + hc;
                             dl = coord_step(qq, lane, g, h);
                             s_dr[warp][lane] = dl;
                         }
@@ -878,7 +909,9 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                         if (dl != 0.0)
                             for (int i = i0 + sl; i < i1; i += 32 / G) {
                                 const int d = s_bde_d[i];
-                                s_dcur[d][fw] = upd_fma((T)dl, (T)s_bde_x[i], s_dcur[d][fw]);
+                                const T v = upd_fma((T)dl, (T)s_bde_x[i], s_dst[par][d][fw]);
+                                s_dst[par][d][fw] = v;
+                                s_mc[d][fw] = row_mean<T, MODEL>(v);
                             }
                     }
                     __syncthreads();
@@ -903,7 +936,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                                    s_dr, s_drow, nd);
                 for (int t = threadIdx.x; t < nd * G; t += kBT) {
                     const int d = t / G, k = s_drow[d];
-                    if (k >= r0 && k < r1) xbg[(size_t)k * G + t % G] = s_dcur[d][t % G];
+                    if (k >= r0 && k < r1) xbg[(size_t)k * G + t % G] = s_dst[par][d][t % G];
                 }
                 __syncthreads();
                 if (rank == 0 && threadIdx.x == 0) count_run(q, L);
@@ -1571,7 +1604,7 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
                     fresh += dslot[rows[e]] < 0;
                     level = std::max(level, rlvl[rows[e]] + 1);
                 }
-        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax)) {
+        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > kLevelMax)) {
             close();
             level = 1;
         }
@@ -1612,7 +1645,7 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
     const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * sizeof(int) + staged_value_bytes<T, MODEL, G>() +
-                       4 * kDirtyMax * G * sizeof(T);
+                       5 * kDirtyMax * G * sizeof(T);
     CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     cfg.dynamicSmemBytes = dyn;
     cfg.stream = stream;

@@ -252,6 +252,12 @@ def summarize(res: Sequence[Response], wall: float) -> dict:
         "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
         "latency_mean_s": float(lat.mean()), "wall_s": wall, "fits_per_s": len(ok) / wall if wall > 0 else None,
         "batched_requests": int(sum(r.batch_size > 1 for r in ok)),
+        # time on the device once admitted, and how many fits ran at once on average
+        "service_p50_s": float(np.percentile([r.finished - r.admitted for r in ok], 50)) if ok else None,
+        "service_p99_s": float(np.percentile([r.finished - r.admitted for r in ok], 99)) if ok else None,
+        "mean_concurrency": float(sum(r.finished - r.admitted for r in ok) / wall) if ok and wall > 0 else None,
+        "cycles_p50": float(np.percentile([r.iterations for r in ok], 50)) if ok else None,
+        "cycles_max": int(max(r.iterations for r in ok)) if ok else None,
     }
 
 
