@@ -129,7 +129,8 @@ def peaks():
 
 
 def traffic_record(workload_name):
-    """DRAM bytes per launch of the dominant kernel from a committed ncu summary."""
+    """DRAM traffic per algorithmic byte of the dominant kernel, from the
+    committed ncu capture of the same workload (2 cycles per fit)."""
     path = os.path.join(ROOT, "profiles", "batch_cv_traffic.json")
     try:
         with open(path) as f:
@@ -361,7 +362,12 @@ def run_ours(args):
                     "kernel": f"k_batch<{'float' if state_bytes[dom] == 4 else 'double'},LR,8>",
                     "algorithmic_bytes_per_launch": phase_bytes[dom] / args.steps,
                     "launch_ms": phase_ms[dom] / args.steps,
-                    "traffic": (tr["dram_bytes_per_launch"] if tr else None)}
+                    # DRAM bytes per launch: the committed 2-cycle ncu capture's traffic per
+                    # algorithmic byte times this launch's algorithmic bytes
+                    "traffic": (tr["dram_per_algorithmic_byte"] * phase_bytes[dom] / args.steps
+                                if tr and tr.get("precision", "fp64") == args.precision else None),
+                    "traffic_source": ("scaled from profiles/batch_cv_traffic.json (ncu, 2-cycle capture)"
+                                       if tr else None)}
         mean_cycles = float(np.mean([f.iterations for f in res.fits]))
         line = {
             "metric": "cv_fits_per_second", "value": value, "unit": "fits/s", "n_gpus": world,
