@@ -220,3 +220,116 @@ def ref_cv_weights(K, ids, fold, seed, by_row=True, n_reps=1) -> np.ndarray:
                         str(int(by_row)), str(n_reps)], input=ids.tobytes(), capture_output=True,
                        check=True)
     return np.frombuffer(p.stdout, dtype=np.float64).reshape(n_reps * fold, K).copy()
+
+
+class IngestInput(C.Structure):
+    _fields_ = [("model", C.c_int), ("n_outcomes", C.c_longlong), ("stratum_id", C.c_void_p),
+                ("row_id", C.c_void_p), ("y", C.c_void_p), ("time", C.c_void_p),
+                ("n_covariates", C.c_longlong), ("covariate_id", C.c_void_p), ("covariate_row", C.c_void_p),
+                ("covariate_value", C.c_void_p), ("add_intercept", C.c_int), ("offset_from_time", C.c_int)]
+
+
+class IngestOutput(C.Structure):
+    _fields_ = [("K", C.c_int), ("J", C.c_int), ("col_format", C.POINTER(C.c_int)),
+                ("col_ptr", C.POINTER(C.c_longlong)), ("col_idx", C.POINTER(C.c_int)),
+                ("val_ptr", C.POINTER(C.c_longlong)), ("col_val", C.POINTER(C.c_double)),
+                ("col_label", C.POINTER(C.c_longlong)), ("pid", C.POINTER(C.c_int)),
+                ("y", C.POINTER(C.c_double)), ("time", C.POINTER(C.c_double)),
+                ("has_offset", C.c_int), ("has_intercept", C.c_int)]
+
+
+_INGEST_SCRIPT = r"""
+import ctypes as C, sys, struct
+L = C.CDLL(sys.argv[1])
+class IngestInput(C.Structure):
+    _fields_ = [("model", C.c_int), ("n_outcomes", C.c_longlong), ("stratum_id", C.c_void_p),
+                ("row_id", C.c_void_p), ("y", C.c_void_p), ("time", C.c_void_p),
+                ("n_covariates", C.c_longlong), ("covariate_id", C.c_void_p), ("covariate_row", C.c_void_p),
+                ("covariate_value", C.c_void_p), ("add_intercept", C.c_int), ("offset_from_time", C.c_int)]
+class IngestOutput(C.Structure):
+    _fields_ = [("K", C.c_int), ("J", C.c_int), ("col_format", C.POINTER(C.c_int)),
+                ("col_ptr", C.POINTER(C.c_longlong)), ("col_idx", C.POINTER(C.c_int)),
+                ("val_ptr", C.POINTER(C.c_longlong)), ("col_val", C.POINTER(C.c_double)),
+                ("col_label", C.POINTER(C.c_longlong)), ("pid", C.POINTER(C.c_int)),
+                ("y", C.POINTER(C.c_double)), ("time", C.POINTER(C.c_double)),
+                ("has_offset", C.c_int), ("has_intercept", C.c_int)]
+raw = sys.stdin.buffer.read()
+model, n, m, hs, ht, hv, ai, off = struct.unpack_from("<iqqiiiii", raw, 0)
+pos = struct.calcsize("<iqqiiiii")
+def take(count, ctype):
+    global pos
+    size = count * C.sizeof(ctype)
+    buf = (ctype * max(count, 1)).from_buffer_copy(raw[pos:pos + size] + bytes(C.sizeof(ctype)))
+    pos += size
+    return buf
+st = take(n, C.c_longlong) if hs else None
+row = take(n, C.c_longlong); y = take(n, C.c_double)
+tm = take(n, C.c_double) if ht else None
+cid = take(m, C.c_longlong); crow = take(m, C.c_longlong)
+cv = take(m, C.c_double) if hv else None
+a = lambda b: C.addressof(b) if b is not None else None
+inp = IngestInput(model, n, a(st), a(row), a(y), a(tm), m, a(cid), a(crow), a(cv), ai, off)
+out = IngestOutput()
+L.ref_ingest.argtypes = [C.POINTER(IngestInput), C.POINTER(IngestOutput)]
+L.ref_last_error.restype = C.c_char_p
+if L.ref_ingest(C.byref(inp), C.byref(out)):
+    sys.stderr.write(L.ref_last_error().decode())
+    sys.exit(3)
+J, K = out.J, out.K
+ni, nv = out.col_ptr[J], out.val_ptr[J]
+w = sys.stdout.buffer
+w.write(struct.pack("<iiiiiqq", K, J, 1 if out.time else 0, out.has_offset, out.has_intercept, ni, nv))
+def put(ptr, count, ctype):
+    w.write(C.string_at(ptr, count * C.sizeof(ctype)) if count else b"")
+put(out.col_format, J, C.c_int); put(out.col_ptr, J + 1, C.c_longlong); put(out.col_idx, ni, C.c_int)
+put(out.val_ptr, J + 1, C.c_longlong); put(out.col_val, nv, C.c_double); put(out.col_label, J, C.c_longlong)
+put(out.pid, K, C.c_int); put(out.y, K, C.c_double)
+if out.time:
+    put(out.time, K, C.c_double)
+"""
+
+
+def ref_ingest(model, outcomes, covariates, add_intercept, offset_from_time) -> dict:
+    """The reference's ModelData loader (loadY, intercept loadX, loadMultipleX,
+    the Poisson offset) on tables already in the reference's sort order.
+
+    Runs in a child interpreter without numpy, for the reason given at
+    ref_cv_weights (loadY formats row labels through a stringstream)."""
+    import struct
+    import sys
+    path = os.path.join(REF_DIR, "libcyclops_ref.so")
+    if not os.path.exists(path):
+        build()
+    st, tm, cv = outcomes.get("stratumId"), outcomes.get("time"), covariates.get("covariateValue")
+    n, m = len(outcomes["rowId"]), len(covariates["rowId"])
+    parts = [struct.pack("<iqqiiiii", model, n, m, st is not None, tm is not None, cv is not None,
+                         int(add_intercept), int(offset_from_time))]
+    if st is not None:
+        parts.append(np.ascontiguousarray(st, np.int64).tobytes())
+    parts += [np.ascontiguousarray(outcomes["rowId"], np.int64).tobytes(),
+              np.ascontiguousarray(outcomes["y"], np.float64).tobytes()]
+    if tm is not None:
+        parts.append(np.ascontiguousarray(tm, np.float64).tobytes())
+    parts += [np.ascontiguousarray(covariates["covariateId"], np.int64).tobytes(),
+              np.ascontiguousarray(covariates["rowId"], np.int64).tobytes()]
+    if cv is not None:
+        parts.append(np.ascontiguousarray(cv, np.float64).tobytes())
+    p = subprocess.run([sys.executable, "-c", _INGEST_SCRIPT, path], input=b"".join(parts), capture_output=True)
+    if p.returncode:
+        raise RuntimeError(p.stderr.decode(errors="replace")[-500:])
+    buf = p.stdout
+    K, J, ht, hoff, hint, ni, nv = struct.unpack_from("<iiiiiqq", buf, 0)
+    pos = struct.calcsize("<iiiiiqq")
+
+    def take(count, dt):
+        nonlocal pos
+        a = np.frombuffer(buf, dtype=dt, count=count, offset=pos).copy()
+        pos += count * np.dtype(dt).itemsize
+        return a
+
+    res = {"col_format": take(J, np.int32), "col_ptr": take(J + 1, np.int64), "col_idx": take(ni, np.int32),
+           "val_ptr": take(J + 1, np.int64), "col_val": take(nv, np.float64), "col_label": take(J, np.int64),
+           "pid": take(K, np.int32), "y": take(K, np.float64)}
+    res["time"] = take(K, np.float64) if ht else None
+    res["has_offset"], res["has_intercept"] = hoff, hint
+    return res

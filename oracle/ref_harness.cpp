@@ -18,6 +18,7 @@
 //   * CV fold masks     CrossValidationSelector  src/cyclops/drivers/CrossValidationSelector.cpp:21-116
 //   * engine probes     AbstractModelSpecifics virtuals, called directly on the
 //                       same engine object the CCD uses.
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <sstream>
@@ -291,6 +292,83 @@ int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n
             std::memcpy(out + (size_t)task * K, w.data(), sizeof(double) * K);
         }
     });
+}
+
+int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out) {
+    return guarded([&] {
+        std::memset(out, 0, sizeof(*out));
+        ModelData<double> md(toModelType(in->model), bsccs::make_shared<QuietLogger>(),
+                             bsccs::make_shared<ThrowingErrorHandler>());
+        const size_t n = (size_t)in->n_outcomes;
+        std::vector<IdType> strata, rows(in->row_id, in->row_id + n);
+        if (in->stratum_id) strata.assign(in->stratum_id, in->stratum_id + n);
+        std::vector<double> y(in->y, in->y + n), time;
+        if (in->time) time.assign(in->time, in->time + n);
+        md.loadY(strata, rows, y, time);
+        if (in->add_intercept) md.loadX(0, std::vector<IdType>(), std::vector<double>(), false, false, false);
+        const size_t m = (size_t)in->n_covariates;
+        if (m) {
+            std::vector<int64_t> cid(in->covariate_id, in->covariate_id + m), crow(in->covariate_row, in->covariate_row + m);
+            std::vector<double> cval;
+            if (in->covariate_value) cval.assign(in->covariate_value, in->covariate_value + m);
+            md.loadMultipleX(cid, crow, cval, false, false, false, false);
+        }
+        if (in->offset_from_time) {
+            md.setOffsetCovariate(-1);
+            md.logTransformCovariate(0);
+        }
+        const auto& X = md.getX();
+        const int J = (int)X.getNumberOfColumns(), K = (int)X.getNumberOfRows();
+        out->K = K;
+        out->J = J;
+        out->col_format = (int*)std::malloc(sizeof(int) * (J + 1));
+        out->col_ptr = (long long*)std::malloc(sizeof(long long) * (J + 1));
+        out->val_ptr = (long long*)std::malloc(sizeof(long long) * (J + 1));
+        out->col_label = (long long*)std::malloc(sizeof(long long) * (J + 1));
+        std::vector<int> idx;
+        std::vector<double> val;
+        out->col_ptr[0] = out->val_ptr[0] = 0;
+        for (int j = 0; j < J; ++j) {
+            const auto& c = X.getColumn(j);
+            const FormatType f = c.getFormatType();
+            out->col_format[j] = f == DENSE ? REF_DENSE : f == SPARSE ? REF_SPARSE : f == INDICATOR ? REF_INDICATOR : REF_INTERCEPT;
+            out->col_label[j] = (long long)c.getNumericalLabel();
+            if (f == SPARSE || f == INDICATOR) {
+                const auto& r = c.getColumnsVector();
+                idx.insert(idx.end(), r.begin(), r.end());
+            }
+            if (f == SPARSE || f == DENSE) {
+                const auto& v = c.getDataVector();
+                val.insert(val.end(), v.begin(), v.end());
+            }
+            out->col_ptr[j + 1] = (long long)idx.size();
+            out->val_ptr[j + 1] = (long long)val.size();
+        }
+        out->col_idx = (int*)std::malloc(sizeof(int) * (idx.size() + 1));
+        out->col_val = (double*)std::malloc(sizeof(double) * (val.size() + 1));
+        std::memcpy(out->col_idx, idx.data(), sizeof(int) * idx.size());
+        std::memcpy(out->col_val, val.data(), sizeof(double) * val.size());
+        const auto pid = md.getPidVectorSTL();
+        out->pid = (int*)std::malloc(sizeof(int) * (K + 1));
+        for (int k = 0; k < K; ++k) out->pid[k] = pid.empty() ? k : pid[k];
+        out->y = (double*)std::malloc(sizeof(double) * (K + 1));
+        const auto& yy = md.getYVectorRef();
+        for (int k = 0; k < K; ++k) out->y[k] = yy[k];
+        if (!time.empty()) {
+            out->time = (double*)std::malloc(sizeof(double) * (K + 1));
+            const auto& tt = md.getTimeVectorRef();
+            for (int k = 0; k < K; ++k) out->time[k] = tt[k];
+        }
+        out->has_offset = md.getHasOffsetCovariate() ? 1 : 0;
+        out->has_intercept = md.getHasInterceptCovariate() ? 1 : 0;
+    });
+}
+
+void ref_ingest_free(ref_ingest_output* out) {
+    if (!out) return;
+    std::free(out->col_format); std::free(out->col_ptr); std::free(out->col_idx); std::free(out->val_ptr);
+    std::free(out->col_val); std::free(out->col_label); std::free(out->pid); std::free(out->y); std::free(out->time);
+    std::memset(out, 0, sizeof(*out));
 }
 
 }  // extern "C"

@@ -55,4 +55,41 @@ int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient,
 int ref_predictive_loglik(const ref_problem* p, const double* beta, const double* held_out,
                           double* out);
 int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n_reps, double* out);
+
+/* The reference's own data loader on tables already in the reference's
+ * sort order (the R layer sorts, R/NewDataConversion.R:125-176):
+ * ModelData::loadY, loadX for the intercept, loadMultipleX, and for Poisson
+ * models setOffsetCovariate(-1) + logTransformCovariate(0)
+ * (src/cyclops/ModelData.cpp:69-145, 148-243, 246-370, 609-651). */
+typedef struct {
+    int model;
+    long long n_outcomes;
+    const long long* stratum_id;      /* n_outcomes or NULL */
+    const long long* row_id;          /* n_outcomes */
+    const double* y;                  /* n_outcomes */
+    const double* time;               /* n_outcomes or NULL */
+    long long n_covariates;
+    const long long* covariate_id;    /* n_covariates */
+    const long long* covariate_row;   /* n_covariates */
+    const double* covariate_value;    /* n_covariates or NULL (indicators) */
+    int add_intercept;
+    int offset_from_time;
+} ref_ingest_input;
+
+typedef struct {
+    int K, J;
+    int* col_format;          /* J */
+    long long* col_ptr;       /* J+1 offsets into col_idx */
+    int* col_idx;
+    long long* val_ptr;       /* J+1 offsets into col_val */
+    double* col_val;
+    long long* col_label;     /* J numerical labels */
+    int* pid;                 /* K strata renumbered by runs */
+    double* y;                /* K */
+    double* time;             /* K, or NULL */
+    int has_offset, has_intercept;
+} ref_ingest_output;
+
+int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out);
+void ref_ingest_free(ref_ingest_output* out);
 #endif

@@ -20,7 +20,7 @@ def pytest_configure(config):
 
 def golden_names():
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not p.endswith("cv_folds.npz"))
+                  if not p.endswith("cv_folds.npz") and not os.path.basename(p).startswith("ingest_"))
 
 
 def load_golden(name):

@@ -118,12 +118,54 @@ def save_cv():
     print("cv_folds", by_row.shape, by_pid.shape)
 
 
+def ingest_tables(model_type, seed, with_values=True, n=80, m=400):
+    """Unsorted long-format tables with the awkward cases: rowIds in random
+    order, covariate rows without an outcome, zero values, columns that start
+    as indicators and hold a non-0/1 value later, ties in Cox times."""
+    rng = np.random.default_rng(seed)
+    outcomes = {"rowId": rng.permutation(np.arange(1000, 1000 + n)).astype(np.int64),
+                "y": rng.integers(0, 2, n).astype(np.float64),
+                "stratumId": rng.integers(0, max(2, n // 5), n).astype(np.int64),
+                "time": rng.choice([0.25, 0.5, 1.0, 2.0, 3.0], n).astype(np.float64)}
+    rows = rng.integers(990, 1000 + n, m).astype(np.int64)
+    cids = rng.integers(1, 15, m).astype(np.int64)
+    key = rows * 100 + cids
+    _, u = np.unique(key, return_index=True)
+    u = rng.permutation(u)
+    cov = {"rowId": rows[u], "covariateId": cids[u]}
+    if with_values:
+        cov["covariateValue"] = rng.choice([0.0, 1.0, 1.0, 1.0, 2.5, -0.75], u.size).astype(np.float64)
+    return outcomes, cov
+
+
+def save_ingest():
+    """The reference loader's result for each model type (tables sorted by
+    the R layer's rules, then ModelData::loadY / loadX / loadMultipleX)."""
+    from cyclops_b200 import ingest
+    for mt, seed, vals in [("lr", 1, True), ("pr", 2, True), ("clr", 3, True), ("cox", 4, True), ("lr", 5, False)]:
+        model = ingest._MODELS[mt]
+        outcomes, cov = ingest_tables(mt, seed, vals)
+        outs = ingest.sort_outcomes(model, outcomes)
+        covs = ingest.sort_covariates(model, cov, outs)
+        ref = O.ref_ingest(model, {k: outs[k] for k in ("rowId", "y", "stratumId", "time") if outs[k] is not None},
+                           {"rowId": covs["rowId"], "covariateId": covs["covariateId"],
+                            "covariateValue": covs["covariateValue"]},
+                           mt in ("lr", "pr"), mt in ("pr", "cpr"))
+        name = f"ingest_{mt}_{seed}"
+        arrays = {"model_type": mt, **{"in_" + k: v for k, v in outcomes.items()},
+                  **{"cov_" + k: v for k, v in cov.items()},
+                  **{"ref_" + k: v for k, v in ref.items() if v is not None}}
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+        print(name, "J", len(ref["col_format"]), "nnz", int(ref["col_ptr"][-1]))
+
+
 def main():
     if not O.have_ref():
         O.build()
     for name, spec in cases().items():
         save_case(name, spec)
     save_cv()
+    save_ingest()
 
 
 if __name__ == "__main__":
