@@ -91,6 +91,7 @@ _SIGS = {
     "cyc_engine_save_xbeta": [C.c_void_p],
     "cyc_engine_get_xbeta_save": [C.c_void_p, C.c_void_p],
     "cyc_engine_get_n": [C.c_void_p, C.POINTER(C.c_int)],
+    "cyc_engine_fisher_information": [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p],
     "cyc_fit": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.POINTER(FitResult)],
     "cyc_batch_fit": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.c_int, C.POINTER(Control),
                       C.POINTER(FitResult)],

@@ -80,8 +80,16 @@ public:
     void computeNumeratorForGradient(int index, bool useWeights) override {
         check(cyc_engine_compute_numerator_for_gradient(engine_, index, useWeights ? 1 : 0));
     }
-    void computeFisherInformation(int, int, double*, bool) override {
-        throw std::logic_error("cyclops_b200: Fisher information is not offered on the GPU engine");
+    // computeFisherInformation (ModelSpecifics.hpp:1203-1351) for one pair
+    void computeFisherInformation(int indexOne, int indexTwo, double* oinfo, bool useWeights) override {
+        if (indexOne == indexTwo) {
+            check(cyc_engine_fisher_information(engine_, &indexOne, 1, useWeights ? 1 : 0, oinfo));
+        } else {
+            const int cols[2] = {indexOne, indexTwo};
+            double m[4];
+            check(cyc_engine_fisher_information(engine_, cols, 2, useWeights ? 1 : 0, m));
+            *oinfo = m[1];
+        }
     }
     void updateXBeta(double delta, int index, bool useWeights) override {
         check(cyc_engine_update_xbeta(engine_, delta, index, useWeights ? 1 : 0));

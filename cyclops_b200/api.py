@@ -211,6 +211,15 @@ class Engine:
         N.check(N.lib().cyc_engine_get_xbeta_save(self.handle, _ptr(out)))
         return out
 
+    def fisher_information(self, columns, use_cv=False) -> np.ndarray:
+        """computeFisherInformation for every pair of `columns` at the current
+        coefficients (CyclicCoordinateDescent.cpp:1288-1300): n x n."""
+        cols = np.ascontiguousarray(columns, np.int32)
+        out = np.zeros((cols.size, cols.size))
+        N.check(N.lib().cyc_engine_fisher_information(self.handle, _ptr(cols), int(cols.size), int(use_cv),
+                                                      _ptr(out)))
+        return out
+
     def n_denominators(self) -> int:
         n = C.c_int()
         N.check(N.lib().cyc_engine_get_n(self.handle, C.byref(n)))
@@ -271,6 +280,31 @@ def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional
     fn = N.lib().cyc_fit_host_loop if host_loop else N.lib().cyc_fit
     N.check(fn(ds.handle, C.byref(p), C.byref(spec), C.byref(c), C.byref(out)))
     return FitResult(beta, out.log_likelihood, out.log_prior, out.iterations, out.return_flag)
+
+
+@dataclasses.dataclass
+class AsymptoticVariance:
+    columns: np.ndarray           # the columns with a row / column in the matrices
+    fisher: np.ndarray            # Fisher information (precision) matrix
+    variance: np.ndarray          # its inverse
+    standard_errors: np.ndarray   # sqrt of the variance diagonal
+
+
+def asymptotic_variance(data, beta, prior: PriorSpec, device: int = 0) -> AsymptoticVariance:
+    """getAsymptoticVariance (CyclicCoordinateDescent.cpp:1249-1352): the
+    Fisher information over the columns that are not fixed and, under a
+    Laplace prior, not at zero, computed on the GPU at `beta`; its inverse
+    (the reference inverts with Eigen on the host, as here)."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    b = np.ascontiguousarray(beta, np.float64)
+    cols = [j for j in range(ds.data.J)
+            if not (ds.data.has_offset and j == 0) and (prior.prior_type != PRIOR_LAPLACE or b[j] != 0.0)]
+    eng = Engine(ds)
+    eng.compute_xbeta(b)
+    eng.compute_remaining_statistics()
+    fisher = eng.fisher_information(cols)
+    var = np.linalg.inv(fisher) if len(cols) else np.zeros((0, 0))
+    return AsymptoticVariance(np.asarray(cols, np.int32), fisher, var, np.sqrt(np.diag(var)))
 
 
 def launch_count() -> int:

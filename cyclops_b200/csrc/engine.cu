@@ -450,6 +450,52 @@ void Engine::predictive_estimates(double* y, const double* w) {
     sync();
 }
 
+// computeFisherInformation over every pair of `cols` (CyclicCoordinateDescent
+// computeFisherInformation, src/cyclops/CyclicCoordinateDescent.cpp:1288-1300):
+// out is the n x n symmetric matrix, row-major
+void Engine::fisher_information(const int* cols, int n, double* out) {
+    CYC_REQUIRE(model_independent(model) || model_grouped(model), CYC_ERR_UNSUPPORTED,
+                "Fisher information is offered for lr, pr, clr and cpr");
+    const int K = ds->K, S = ds->S, J = ds->J;
+    for (int i = 0; i < n; ++i)
+        CYC_REQUIRE(cols[i] >= 0 && cols[i] < J, CYC_ERR_ARGUMENT, "column index out of range");
+    if (n == 0) return;
+    remaining_statistics(false);
+    const bool grouped = model_grouped(model);
+    if (grouped)
+        CYC_REQUIRE((double)n * S <= (double)(1u << 27), CYC_ERR_MEMORY,
+                    "too many columns x strata for one Fisher information call");
+    std::vector<int> pa, pb;
+    for (int i = 0; i < n; ++i)
+        for (int j = i; j < n; ++j) { pa.push_back(i); pb.push_back(j); }
+    const int np = (int)pa.size();
+    DevBuf<int> d_cols, d_pa, d_pb;
+    DevBuf<double> d_v, d_t, d_out;
+    d_cols.alloc(n); d_pa.alloc(np); d_pb.alloc(np); d_v.alloc(K); d_out.alloc(np);
+    CYC_CHECK_CUDA(cudaMemcpyAsync(d_cols.get(), cols, n * sizeof(int), cudaMemcpyHostToDevice, stream));
+    CYC_CHECK_CUDA(cudaMemcpyAsync(d_pa.get(), pa.data(), np * sizeof(int), cudaMemcpyHostToDevice, stream));
+    CYC_CHECK_CUDA(cudaMemcpyAsync(d_pb.get(), pb.data(), np * sizeof(int), cudaMemcpyHostToDevice, stream));
+    launch(k_fisher_row, grid_for(K, 4), kThreads, 0, stream, K, model, (const double*)exb.get(),
+           (const double*)denom.get(), (const int*)ds->d_strat.get(), d_v.get());
+    if (grouped) {
+        d_t.alloc((size_t)n * S);
+        CYC_CHECK_CUDA(cudaMemsetAsync(d_t.get(), 0, (size_t)n * S * sizeof(double), stream));
+        launch(k_fisher_strata, std::min(n, 148 * 8), kThreads, 0, stream, n, (const int*)d_cols.get(), K, S,
+               (const int*)ds->d_fmt.get(), (const long long*)ds->d_col_ptr.get(), (const long long*)ds->d_val_ptr.get(),
+               (const int*)ds->d_idx.get(), (const double*)ds->d_val.get(), (const int*)ds->d_strat.get(),
+               (const double*)exb.get(), d_t.get());
+    }
+    launch(k_fisher_pairs, std::min(np, 148 * 8), kThreads, 0, stream, np, (const int*)d_pa.get(),
+           (const int*)d_pb.get(), (const int*)d_cols.get(), K, S, grouped ? 1 : 0, (const int*)ds->d_fmt.get(),
+           (const long long*)ds->d_col_ptr.get(), (const long long*)ds->d_val_ptr.get(), (const int*)ds->d_idx.get(),
+           (const double*)ds->d_val.get(), (const double*)d_v.get(), (const int*)ds->d_strat.get(),
+           (const double*)denom.get(), (const double*)d_t.get(), d_out.get());
+    std::vector<double> h(np);
+    CYC_CHECK_CUDA(cudaMemcpyAsync(h.data(), d_out.get(), np * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    sync();
+    for (int p = 0; p < np; ++p) out[(size_t)pa[p] * n + pb[p]] = out[(size_t)pb[p] * n + pa[p]] = h[p];
+}
+
 void Engine::get_xbeta(double* out) {
     CYC_CHECK_CUDA(cudaMemcpyAsync(out, xb.get(), ds->K * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();
@@ -566,6 +612,15 @@ extern "C" int cyc_engine_save_xbeta(cyc_engine* e) {
 extern "C" int cyc_engine_get_xbeta_save(cyc_engine* e, double* out) {
     return ENGINE_CALL(e, CYC_REQUIRE(out, CYC_ERR_ARGUMENT, "null output"); e->eng->get_xbeta_save(out));
 }
+extern "C" int cyc_engine_fisher_information(cyc_engine* e, const int* columns, int n, int use_cv, double* out) {
+    return ENGINE_CALL(e, {
+        CYC_REQUIRE((columns && out) || n == 0, CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(n >= 0, CYC_ERR_ARGUMENT, "negative column count");
+        CYC_REQUIRE(!use_cv, CYC_ERR_UNSUPPORTED, "Weights are not yet implemented in Fisher Information calculations");
+        e->eng->fisher_information(columns, n, out);
+    });
+}
+
 extern "C" int cyc_engine_get_n(const cyc_engine* e, int* n) {
     return guarded([&] {
         CYC_REQUIRE(e && n, CYC_ERR_ARGUMENT, "null argument");

@@ -67,6 +67,7 @@ struct Engine {
     double predictive_log_likelihood(const double* w);
     void predictive_estimates(double* y, const double* w);
     void get_xbeta(double* out);
+    void fisher_information(const int* cols, int n, double* out);
     void save_xbeta();
     void get_xbeta_save(double* out);
 };

@@ -122,6 +122,114 @@ __global__ void k_rs_grouped(int G, const int* __restrict__ grow_ptr, const doub
     }
 }
 
+// ---- Fisher information (ModelSpecifics.hpp:1203-1351) ------------------------
+
+// per row, the factor of x_i * x_j in incrementFisherInformation: Logistic
+// (ModelSpecifics.h:524-538) p - p^2 with p = exb / denom; PoissonRegression
+// (:1497-1506) exb; the grouped models' Survival (:488-497) exb / denom of
+// the row's stratum.  Unweighted, as the reference (:1207-1209).
+__global__ void k_fisher_row(int K, int model, const double* __restrict__ exb, const double* __restrict__ denom,
+                             const int* __restrict__ strat, double* __restrict__ v) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        if (model == CYC_LR) {
+            const double g = exb[k] / denom[k];
+            v[k] = exb[k] / denom[k] - g * g;
+        } else if (model == CYC_PR) {
+            v[k] = exb[k];
+        } else {
+            v[k] = exb[k] / denom[strat[k]];
+        }
+    }
+}
+
+__device__ __forceinline__ ColView fisher_view(int j, int K, const int* fmt, const long long* col_ptr,
+                                               const long long* val_ptr, const int* idx, const double* val) {
+    ColView c;
+    c.fmt = fmt[j];
+    c.n = (c.fmt == CYC_DENSE || c.fmt == CYC_INTERCEPT) ? K : col_ptr[j + 1] - col_ptr[j];
+    c.idx = idx + col_ptr[j];
+    c.val = val + val_ptr[j];
+    return c;
+}
+
+// row k in column c (binary search of its ascending row ids): its value, or false
+__device__ __forceinline__ bool fisher_lookup(const ColView& c, int k, double& x) {
+    if (c.fmt == CYC_DENSE) { x = __ldg(c.val + k); return true; }
+    if (c.fmt == CYC_INTERCEPT) { x = 1.0; return true; }
+    long long lo = 0, hi = c.n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (__ldg(c.idx + mid) < k) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < c.n && __ldg(c.idx + lo) == k) {
+        x = c.fmt == CYC_SPARSE ? __ldg(c.val + lo) : 1.0;
+        return true;
+    }
+    return false;
+}
+
+// grouped models: per column of the set, its per-stratum sums of x * exb
+// (getSubjectSpecificHessianIterator, ModelSpecifics.hpp:1247-1270), dense
+// over strata (t[c * S + s], zero where the column has no row); the first
+// entry of each run of one stratum walks the run
+__global__ void k_fisher_strata(int n_cols, const int* __restrict__ cols, int K, int S, const int* fmt,
+                                const long long* col_ptr, const long long* val_ptr, const int* idx,
+                                const double* val, const int* __restrict__ strat, const double* __restrict__ exb,
+                                double* __restrict__ t) {
+    for (int c = blockIdx.x; c < n_cols; c += gridDim.x) {
+        const ColView a = fisher_view(cols[c], K, fmt, col_ptr, val_ptr, idx, val);
+        for (long long e = threadIdx.x; e < a.n; e += blockDim.x) {
+            const int k = a.row(e), s = strat[k];
+            if (e > 0 && strat[a.row(e - 1)] == s) continue;
+            double sum = 0.0;
+            long long q = e;
+            do {
+                const int kq = a.row(q);
+                sum += exb[kq] * a.x(q);
+                ++q;
+            } while (q < a.n && strat[a.row(q)] == s);
+            t[(size_t)c * S + s] = sum;
+        }
+    }
+}
+
+// one block per pair (a, b) of the set: the sum over the rows of both columns
+// of v_k * x_a * x_b (PairProductIterator, :1276-1289), walking the shorter
+// column and looking its rows up in the other; grouped models subtract
+// sum_s t_a(s) t_b(s) / denom_s^2 (:1296-1347).  Fixed order: deterministic.
+__global__ void k_fisher_pairs(int n_pairs, const int* __restrict__ pa, const int* __restrict__ pb,
+                               const int* __restrict__ cols, int K, int S, int grouped, const int* fmt,
+                               const long long* col_ptr, const long long* val_ptr, const int* idx,
+                               const double* val, const double* __restrict__ v, const int* __restrict__ strat,
+                               const double* __restrict__ denom, const double* __restrict__ t,
+                               double* __restrict__ out) {
+    for (int p = blockIdx.x; p < n_pairs; p += gridDim.x) {
+        ColView a = fisher_view(cols[pa[p]], K, fmt, col_ptr, val_ptr, idx, val);
+        ColView b = fisher_view(cols[pb[p]], K, fmt, col_ptr, val_ptr, idx, val);
+        if (b.n < a.n) { const ColView tmp = a; a = b; b = tmp; }
+        double info = 0.0, cross = 0.0;
+        for (long long e = threadIdx.x; e < a.n; e += blockDim.x) {
+            const int k = a.row(e);
+            double xb;
+            if (fisher_lookup(b, k, xb)) info += v[k] * (a.x(e) * xb);
+        }
+        if (grouped) {
+            const double* ta = t + (size_t)pa[p] * S;
+            const double* tb = t + (size_t)pb[p] * S;
+            const ColView c = fisher_view(cols[pa[p]], K, fmt, col_ptr, val_ptr, idx, val);
+            for (long long e = threadIdx.x; e < c.n; e += blockDim.x) {
+                const int s = strat[c.row(e)];
+                if (e > 0 && strat[c.row(e - 1)] == s) continue;
+                cross += (ta[s] * tb[s]) / (denom[s] * denom[s]);
+            }
+        }
+        block_sum2(info, cross);
+        if (threadIdx.x == 0) out[p] = info - cross;
+        __syncthreads();
+    }
+}
+
 // ---- gradient and Hessian ---------------------------------------------------
 
 // independent rows (ModelSpecifics.hpp:1022-1038 with LogisticRegression /

@@ -149,6 +149,13 @@ int cyc_engine_get_predictive_estimates(cyc_engine* e, double* y, const double* 
 int cyc_engine_get_xbeta(cyc_engine* e, double* out);
 int cyc_engine_save_xbeta(cyc_engine* e);
 int cyc_engine_get_xbeta_save(cyc_engine* e, double* out);
+/* computeFisherInformation (ModelSpecifics.hpp:1203-1351) for every pair of
+ * `columns` at the engine's current coefficients, as
+ * CyclicCoordinateDescent::computeFisherInformation
+ * (CyclicCoordinateDescent.cpp:1288-1300) assembles it: `out` is the n x n
+ * symmetric matrix, row-major.  lr, pr, clr, cpr; unweighted (use_cv != 0 is
+ * CYC_ERR_UNSUPPORTED, as the reference throws, :1207-1209). */
+int cyc_engine_fisher_information(cyc_engine* e, const int* columns, int n, int use_cv, double* out);
 /* number of denominators N (patients / strata / risk-set groups) */
 int cyc_engine_get_n(const cyc_engine* e, int* n);
 

@@ -121,6 +121,7 @@ class _Lib:
         }
         if prefix == "ref_":
             sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
+            sigs["fisher"] = [P(Problem), V, V, C.c_int, V, C.c_int]
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
         for name, args in sigs.items():
             fn = getattr(self.lib, prefix + name, None)
@@ -155,6 +156,17 @@ class _Lib:
         if rc:
             raise RuntimeError(self.err())
         return g, h, xb, ll.value
+
+    def fisher(self, data, beta, columns, device=0):
+        """CyclicCoordinateDescent::computeFisherInformation at `beta` (n x n)."""
+        p, keep = make_problem(data, 1, 1.0, None, None)
+        b = np.ascontiguousarray(beta, np.float64)
+        cols = np.ascontiguousarray(columns, np.int32)
+        out = np.zeros((cols.size, cols.size))
+        rc = self.lib.ref_fisher(C.byref(p), _ptr(b), _ptr(cols), int(cols.size), _ptr(out), int(device))
+        if rc:
+            raise RuntimeError(self.err())
+        return out
 
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)

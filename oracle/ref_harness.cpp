@@ -294,6 +294,19 @@ int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n
     });
 }
 
+int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int n, double* out, int device) {
+    return guarded([&] {
+        auto inst = build(p, device);
+        std::vector<double> b(beta, beta + p->J);
+        inst->ccd->setBeta(b);
+        inst->ccd->getLogLikelihood();          // runs the lazy set-up (exp(xb), denominators)
+        std::vector<size_t> idx(columns, columns + n);
+        const auto m = inst->ccd->computeFisherInformation(idx);
+        for (int i = 0; i < n; ++i)
+            for (int j = 0; j < n; ++j) out[(size_t)i * n + j] = m(i, j);
+    });
+}
+
 int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out) {
     return guarded([&] {
         std::memset(out, 0, sizeof(*out));

@@ -91,5 +91,10 @@ typedef struct {
 } ref_ingest_output;
 
 int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out);
+
+/* CyclicCoordinateDescent::computeFisherInformation (src/cyclops/
+ * CyclicCoordinateDescent.cpp:1288-1300) at `beta` for `n` columns; out is
+ * n x n row-major.  device 1 runs it through the CUDA adapter. */
+int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int n, double* out, int device);
 void ref_ingest_free(ref_ingest_output* out);
 #endif
