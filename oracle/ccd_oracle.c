@@ -517,6 +517,63 @@ static int find_mode(Ctx* c, const ccd_control* ctl, double initial_bound, int* 
     return flag;
 }
 
+/* kktSwindle (CyclicCoordinateDescent.cpp:636-814): the intercept and
+ * columns whose prior has no KKT boundary (flat, normal) start active, the
+ * Laplace columns inactive with beta 0 (zeroed through updateXBeta, as
+ * setBeta does, :473-486); each pass runs findMode over the active set
+ * (:617-634), stops when nothing is inactive or the fit failed, else moves
+ * every inactive column whose |gradient| exceeds lambda into the active set
+ * (computeKktConditions :817-837; the sorted list's violators are exactly
+ * those); MAX_ITERATIONS after max_iterations passes.  An empty active set
+ * skips findMode and keeps the last iteration count. */
+static int kkt_swindle(Ctx* c, const ccd_control* ctl, double bound, int* iterations) {
+    const int J = c->J;
+    int intercept = -1;
+    if (c->p->has_intercept) intercept = c->p->has_offset ? 1 : 0;
+    int* excluded = (int*)malloc(sizeof(int) * J);
+    int* active = (int*)malloc(sizeof(int) * J);
+    int n_active = 0, n_inactive = 0;
+    for (int j = 0; j < J; ++j) {
+        excluded[j] = c->fixb[j];
+        active[j] = !excluded[j] && (j == intercept || prior_of(c, j) != REF_PRIOR_LAPLACE);
+        if (excluded[j]) continue;
+        if (active[j]) ++n_active;
+        else ++n_inactive;
+    }
+    const double lambda = sqrt(2.0 / c->p->variance);                 /* getKktBoundary, CovariatePrior.h:235-238 */
+    int flag = FLAG_SUCCESS;
+    for (int pass = 1;; ++pass) {
+        for (int j = 0; j < J; ++j) {
+            if (excluded[j] || active[j] || c->beta[j] == 0.0) continue;
+            const double delta = 0.0 - c->beta[j];
+            c->beta[j] += delta;
+            update_xbeta(c, j, delta);
+        }
+        flag = FLAG_SUCCESS;
+        if (n_active > 0) {
+            for (int j = 0; j < J; ++j) c->fixb[j] = !active[j];
+            flag = find_mode(c, ctl, bound, iterations);
+        }
+        if (n_inactive == 0 || flag != FLAG_SUCCESS) break;
+        if (pass == ctl->max_iterations) { flag = FLAG_MAX_ITERATIONS; break; }
+        int moved = 0;
+        for (int j = 0; j < J; ++j) {
+            if (excluded[j] || active[j]) continue;
+            double g, h;
+            numerator_for_gradient(c, j);
+            gradient_hessian(c, j, &g, &h);
+            if (!(fabs(g) <= lambda)) { active[j] = 1; ++moved; }
+        }
+        if (moved == 0) break;
+        n_active += moved;
+        n_inactive -= moved;
+    }
+    for (int j = 0; j < J; ++j) c->fixb[j] = excluded[j];
+    free(excluded);
+    free(active);
+    return flag;
+}
+
 /* ---- context lifetime --------------------------------------------------- */
 
 static void ctx_free(Ctx* c) {
@@ -597,8 +654,10 @@ int ccd_oracle_fit(const ccd_problem* p, const ccd_control* ctl, const double* s
      * bounding box while ill-conditioned */
     double bound = ctl->initial_bound;
     int count = 0, flag = FLAG_SUCCESS, iters = 0;
+    /* the swindle runs when some prior has a KKT boundary (JointPrior.h:149-157) */
+    const int swindle = ctl->use_kkt_swindle && p->prior_type == REF_PRIOR_LAPLACE;
     for (;;) {
-        flag = find_mode(&c, ctl, bound, &iters);
+        flag = swindle ? kkt_swindle(&c, ctl, bound, &iters) : find_mode(&c, ctl, bound, &iters);
         ++count;
         if (flag == FLAG_ILLCONDITIONED && count < ctl->max_bound_count) {
             bound /= 10.0;

@@ -19,8 +19,15 @@ def pytest_configure(config):
 
 
 def golden_names():
+    """The plain fit fixtures (not the CV folds, ingest tables or swindle fits)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not p.endswith("cv_folds.npz") and not os.path.basename(p).startswith("ingest_"))
+                  if not p.endswith("cv_folds.npz")
+                  and not os.path.basename(p).startswith(("ingest_", "swindle_")))
+
+
+def swindle_names():
+    """Fits made with the KKT swindle (useKktSwindle)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "swindle_*.npz")))
 
 
 def load_golden(name):

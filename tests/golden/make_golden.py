@@ -81,7 +81,8 @@ def cases():
 def save_case(name, spec):
     d: D.CyclopsData = spec["data"]
     ctl = O.make_control(tolerance=spec.get("tolerance", 1e-6),
-                         convergence_type=spec.get("convergence", D.CONV_GRADIENT))
+                         convergence_type=spec.get("convergence", D.CONV_GRADIENT),
+                         use_kkt_swindle=spec.get("swindle", 0))
     w = spec.get("weights")
     fit = O.ref().fit(d, spec["prior"], spec["variance"], control=ctl, weights=w)
     rng = np.random.default_rng(99)
@@ -102,6 +103,8 @@ def save_case(name, spec):
         iterations=fit.iterations, return_flag=fit.return_flag,
         probe_beta=beta_probe, probe_gradient=g, probe_hessian=h, probe_xbeta=xb, probe_loglik=ll,
     )
+    if spec.get("swindle"):
+        arrays["swindle"] = 1
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
     print(f"{name:22s} K={d.K:6d} J={d.J:5d} nnz={d.nnz:7d} it={fit.iterations:4d} "
           f"flag={fit.return_flag} ll={fit.log_likelihood:.8f}")
@@ -159,14 +162,33 @@ def save_ingest():
         print(name, "J", len(ref["col_format"]), "nnz", int(ref["col_ptr"][-1]))
 
 
-def main():
+SWINDLE_CASES = ["lr_c1", "lr_laplace_small", "lr_zhang_oles", "lr_empty_column", "pr_laplace_weighted",
+                 "clr_laplace", "cox_laplace", "cox_strata"]
+
+
+def save_swindle():
+    """The Laplace problems fitted with the KKT swindle (ModeFindingArguments
+    useKktSwindle, CyclicCoordinateDescent::kktSwindle,
+    src/cyclops/CyclicCoordinateDescent.cpp:636-814): swindle_<case>.npz."""
+    all_cases = cases()
+    for name in SWINDLE_CASES:
+        save_case("swindle_" + name, dict(all_cases[name], swindle=1))
+
+
+def main(parts):
     if not O.have_ref():
         O.build()
-    for name, spec in cases().items():
-        save_case(name, spec)
-    save_cv()
-    save_ingest()
+    if "fits" in parts:
+        for name, spec in cases().items():
+            save_case(name, spec)
+    if "cv" in parts:
+        save_cv()
+    if "ingest" in parts:
+        save_ingest()
+    if "swindle" in parts:
+        save_swindle()
 
 
 if __name__ == "__main__":
-    main()
+    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle]   (default: all)
+    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle"])

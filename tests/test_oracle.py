@@ -3,7 +3,7 @@ engine (tests/golden/make_golden.py).  No GPU."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, rel_err
+from conftest import golden_names, load_golden, rel_err, swindle_names
 from cyclops_b200 import data as D
 from oracle import oracle as O
 
@@ -54,3 +54,29 @@ def test_planted_mistake_is_caught():
     data, s = load_golden("lr_laplace_small")
     bad = O.port().fit(data, int(s["prior"]), float(s["variance"]) * 1.01)
     assert np.max(rel_err(bad.beta[bad.beta != 0], s["beta"][bad.beta != 0], 1e-6)) > 1e-4
+
+
+@pytest.mark.parametrize("name", swindle_names())
+def test_port_swindle_matches_reference_fixture(name):
+    """kktSwindle (CyclicCoordinateDescent.cpp:636-814): the restatement's
+    active-set passes reproduce the reference's fit, iteration count and flag."""
+    data, s = load_golden(name)
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                         use_kkt_swindle=1)
+    fit = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
+    assert fit.iterations == int(s["iterations"])
+    assert fit.return_flag == int(s["return_flag"])
+    np.testing.assert_allclose(fit.beta, s["beta"], rtol=1e-12, atol=1e-14)
+    assert abs(fit.log_likelihood - float(s["log_likelihood"])) <= 1e-12 * abs(float(s["log_likelihood"]))
+
+
+def test_swindle_fixtures_differ_from_plain_fits():
+    """The swindle fixtures are not the plain fits renamed: the active-set
+    passes end at a different point, within the convergence tolerance's reach
+    of the plain fit (relative objective change below 1e-6 allows beta moves
+    of a few hundredths on these problems)."""
+    for name in swindle_names():
+        _, sw = load_golden(name)
+        _, plain = load_golden(name[len("swindle_"):])
+        assert not np.array_equal(sw["beta"], plain["beta"])
+        np.testing.assert_allclose(sw["beta"], plain["beta"], atol=5e-2)
