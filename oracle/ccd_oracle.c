@@ -16,6 +16,7 @@
  */
 #include "ccd_oracle.h"
 
+#include <float.h>
 #include <math.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -644,35 +645,188 @@ static void prepare(Ctx* c) {
     remaining_statistics(c);
 }
 
+/* update (CyclicCoordinateDescent.cpp:586-615): restart with a smaller
+ * bounding box while ill-conditioned; the swindle runs when some prior has
+ * a KKT boundary (JointPrior.h:149-157) */
+static int update(Ctx* c, const ccd_control* ctl, int* iters) {
+    double bound = ctl->initial_bound;
+    int count = 0, flag = FLAG_SUCCESS;
+    const int swindle = ctl->use_kkt_swindle && c->p->prior_type == REF_PRIOR_LAPLACE;
+    for (;;) {
+        flag = swindle ? kkt_swindle(c, ctl, bound, iters) : find_mode(c, ctl, bound, iters);
+        ++count;
+        if (flag == FLAG_ILLCONDITIONED && count < ctl->max_bound_count) {
+            bound /= 10.0;
+            for (int j = c->p->has_offset ? 1 : 0; j < c->J; ++j) c->beta[j] = 0.0;  /* resetBeta :256-264 */
+            compute_xbeta(c);
+            remaining_statistics(c);
+        } else {
+            break;
+        }
+    }
+    return flag;
+}
+
 int ccd_oracle_fit(const ccd_problem* p, const ccd_control* ctl, const double* start,
                    ccd_result* out) {
     Ctx c;
     if (ctx_init(&c, p)) return 1;
     if (start) for (int j = 0; j < p->J; ++j) c.beta[j] = start[j];
     prepare(&c);
-    /* update (CyclicCoordinateDescent.cpp:586-615): restart with a smaller
-     * bounding box while ill-conditioned */
-    double bound = ctl->initial_bound;
-    int count = 0, flag = FLAG_SUCCESS, iters = 0;
-    /* the swindle runs when some prior has a KKT boundary (JointPrior.h:149-157) */
-    const int swindle = ctl->use_kkt_swindle && p->prior_type == REF_PRIOR_LAPLACE;
-    for (;;) {
-        flag = swindle ? kkt_swindle(&c, ctl, bound, &iters) : find_mode(&c, ctl, bound, &iters);
-        ++count;
-        if (flag == FLAG_ILLCONDITIONED && count < ctl->max_bound_count) {
-            bound /= 10.0;
-            for (int j = p->has_offset ? 1 : 0; j < p->J; ++j) c.beta[j] = 0.0;  /* resetBeta */
-            compute_xbeta(&c);
-            remaining_statistics(&c);
-        } else {
-            break;
-        }
-    }
+    int iters = 0;
+    const int flag = update(&c, ctl, &iters);
     for (int j = 0; j < p->J; ++j) out->beta[j] = c.beta[j];
     out->log_likelihood = log_likelihood(&c);
     out->log_prior = log_prior(&c);
     out->iterations = iters;
     out->return_flag = flag;
+    ctx_free(&c);
+    return 0;
+}
+
+/* ---- profile likelihood (CcdInterface.cpp:223-420) ----------------------- */
+
+typedef struct {
+    Ctx* c;
+    const ccd_control* ctl;
+    int index;
+    double mode, threshold;
+    int penalty;
+    int evals;
+} Profile;
+
+/* OptimizationProfile::objective (CcdInterface.cpp:238-249): beta[index] set
+ * to x through updateXBeta (setBeta, CyclicCoordinateDescent.cpp:473-486),
+ * held fixed while update refits the rest from the current state, then the
+ * log likelihood (+ log prior) + threshold - mode */
+static double profile_objective(Profile* f, double x) {
+    Ctx* c = f->c;
+    f->evals++;
+    const double delta = x - c->beta[f->index];
+    c->beta[f->index] += delta;
+    update_xbeta(c, f->index, delta);
+    c->fixb[f->index] = 1;
+    int iters = 0;
+    update(c, f->ctl, &iters);
+    c->fixb[f->index] = 0;
+    double y = log_likelihood(c) + f->threshold - f->mode;
+    if (f->penalty) y += log_prior(c);
+    return y;
+}
+
+/* bracketSignChange (src/utils/RZeroIn.h): steps of 0.1, 0.2, 0.4, ... times
+ * max(|x0|, 0.01) from x0 in `direction` until the objective is no longer
+ * positive; NaN objective when it turns NaN or after 22 steps */
+static double profile_bracket(Profile* f, double x0, double f0, double direction, double* f1) {
+    const double displacement = cmax(fabs(x0), 0.01);
+    double multiplier = 0.1;
+    double x1 = x0, y1 = f0;
+    for (int steps = 0; y1 > 0; ++steps) {
+        x1 = x0 + direction * displacement * multiplier;
+        y1 = profile_objective(f, x1);
+        if (isnan(y1)) break;
+        if (steps > 20) { y1 = NAN; break; }
+        multiplier *= 2.0;
+    }
+    *f1 = y1;
+    return x1;
+}
+
+/* Brent's root finder as Forsythe, Malcolm & Moler give it (Computer Methods
+ * for Mathematical Computations, 1977, zeroin), the variant RZeroIn::getRoot
+ * runs (src/utils/RZeroIn.h): f(a), f(b) of opposite signs known; each step
+ * takes inverse quadratic (or secant) interpolation when it falls well inside
+ * [b, c] and shrinks fast enough, else bisection; stops when half the
+ * bracket is within 2 eps |b| + tol / 2, or after max_it + 1 steps. */
+static double profile_root(Profile* f, double a, double b, double fa, double fb, double tol, int max_it) {
+    if (b < a) {
+        double t = a; a = b; b = t;
+        t = fa; fa = fb; fb = t;
+    }
+    if (fa == 0.0) return a;
+    if (fb == 0.0) return b;
+    double c = a, fc = fa;
+    for (int k = 0; k <= max_it; ++k) {
+        const double prev_step = b - a;
+        if (fabs(fc) < fabs(fb)) {                       /* b: the best point so far */
+            a = b; b = c; c = a;
+            fa = fb; fb = fc; fc = fa;
+        }
+        const double tol_act = 2 * DBL_EPSILON * fabs(b) + tol / 2;
+        double step = (c - b) / 2;
+        if (fabs(step) <= tol_act || fb == 0.0) return b;
+        if (fabs(prev_step) >= tol_act && fabs(fa) > fabs(fb)) {
+            const double cb = c - b;
+            double p, q;
+            if (a == c) {                                /* secant */
+                const double t1 = fb / fa;
+                p = cb * t1;
+                q = 1.0 - t1;
+            } else {                                     /* inverse quadratic */
+                const double r = fa / fc, t1 = fb / fc, t2 = fb / fa;
+                p = t2 * (cb * r * (r - t1) - (b - a) * (t1 - 1.0));
+                q = (r - 1.0) * (t1 - 1.0) * (t2 - 1.0);
+            }
+            if (p > 0) q = -q;
+            else p = -p;
+            if (p < (0.75 * cb * q - fabs(tol_act * q) / 2) && p < fabs(prev_step * q / 2)) step = p / q;
+        }
+        if (fabs(step) < tol_act) step = step > 0 ? tol_act : -tol_act;
+        a = b; fa = fb;
+        b += step;
+        fb = profile_objective(f, b);
+        if ((fb > 0 && fc > 0) || (fb < 0 && fc < 0)) { c = a; fc = fa; }
+    }
+    return b;
+}
+
+int ccd_oracle_profile(const ccd_problem* p, const ccd_control* ctl, const double* start, const int* cols, int n,
+                       double threshold, int include_penalty, int override_no_regularization, double* lower,
+                       double* upper, int* evaluations, ccd_result* fit) {
+    Ctx c;
+    if (ctx_init(&c, p)) return 1;
+    for (int i = 0; i < n; ++i) {
+        if (cols[i] < 0 || cols[i] >= p->J || (p->has_offset && cols[i] == 0)) {
+            snprintf(g_err, sizeof g_err, "profile column %d out of range", cols[i]);
+            ctx_free(&c);
+            return 1;
+        }
+        if (!override_no_regularization && prior_of(&c, cols[i]) != REF_PRIOR_NONE) {
+            snprintf(g_err, sizeof g_err, "Variable %d is regularized.", cols[i]);
+            ctx_free(&c);
+            return 1;
+        }
+    }
+    if (start) for (int j = 0; j < p->J; ++j) c.beta[j] = start[j];
+    prepare(&c);
+    int iters = 0;
+    const int flag = update(&c, ctl, &iters);
+    if (fit) {
+        for (int j = 0; j < p->J; ++j) fit->beta[j] = c.beta[j];
+        fit->log_likelihood = log_likelihood(&c);
+        fit->log_prior = log_prior(&c);
+        fit->iterations = iters;
+        fit->return_flag = flag;
+    }
+    double mode = log_likelihood(&c);
+    if (include_penalty) mode += log_prior(&c);
+    double* x0s = (double*)malloc(sizeof(double) * p->J);
+    memcpy(x0s, c.beta, sizeof(double) * p->J);
+    for (int i = 0; i < n; ++i) {              /* (column, +1) then (column, -1), one state throughout */
+        int count = 0;
+        for (int d = 0; d < 2; ++d) {
+            const double direction = d == 0 ? 1.0 : -1.0;
+            Profile f = {&c, ctl, cols[i], mode, threshold, include_penalty, 0};
+            const double x0 = x0s[cols[i]];
+            double f1;
+            const double x1 = profile_bracket(&f, x0, threshold, direction, &f1);
+            const double pt = isnan(f1) ? NAN : profile_root(&f, x0, x1, threshold, f1, 1e-3, 1000);
+            (d == 0 ? upper : lower)[i] = pt;
+            count += f.evals;
+        }
+        evaluations[i] = count;
+    }
+    free(x0s);
     ctx_free(&c);
     return 0;
 }

@@ -123,6 +123,11 @@ class _Lib:
             sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
             sigs["fisher"] = [P(Problem), V, V, C.c_int, V, C.c_int]
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
+            sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
+                               P(Result), C.c_int]
+        else:
+            sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
+                               P(Result)]
         for name, args in sigs.items():
             fn = getattr(self.lib, prefix + name, None)
             if fn is not None:
@@ -167,6 +172,28 @@ class _Lib:
         if rc:
             raise RuntimeError(self.err())
         return out
+
+    def profile(self, data, columns, prior_type=1, variance=1.0, threshold=1.920729, include_penalty=True,
+                override_no_regularization=False, control: Optional[Control] = None, exclude=None,
+                weights=None, start=None, device=0):
+        """CcdInterface::profileModel with one thread: fit, then each column's
+        (lower, upper) profile bound and the refits both took.  Returns
+        (lower, upper, evaluations, Fit)."""
+        p, keep = make_problem(data, prior_type, variance, exclude, weights)
+        c = control or make_control()
+        cols = np.ascontiguousarray(columns, np.int32)
+        n = int(cols.size)
+        lo, up, ev = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+        beta = np.zeros(data.J)
+        r = Result(beta=beta.ctypes.data)
+        s = None if start is None else np.ascontiguousarray(start, np.float64)
+        args = [C.byref(p), C.byref(c), _ptr(s), _ptr(cols), n, float(threshold), int(include_penalty),
+                int(override_no_regularization), _ptr(lo), _ptr(up), _ptr(ev), C.byref(r)]
+        if self.prefix == "ref_":
+            args.append(int(device))
+        if getattr(self.lib, self.prefix + "profile")(*args):
+            raise RuntimeError(self.err())
+        return lo, up, ev, Fit(beta, r.log_likelihood, r.log_prior, r.iterations, r.return_flag)
 
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)

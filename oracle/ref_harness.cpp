@@ -18,6 +18,13 @@
 //   * CV fold masks     CrossValidationSelector  src/cyclops/drivers/CrossValidationSelector.cpp:21-116
 //   * engine probes     AbstractModelSpecifics virtuals, called directly on the
 //                       same engine object the CCD uses.
+//   * profile bounds    CcdInterface::profileModel with one thread
+//                       src/cyclops/CcdInterface.cpp:262-420: the reference's
+//                       own RZeroIn (src/utils/RZeroIn.h, header-only) over
+//                       OptimizationProfile (:223-260, restated below since
+//                       CcdInterface.cpp needs the R runtime).
+#include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -33,6 +40,8 @@
 #include "priors/CovariatePrior.h"
 #include "drivers/CrossValidationSelector.h"
 #include "io/ProgressLogger.h"
+
+#include "utils/RZeroIn.h"
 
 #ifdef CYC_REF_WITH_CUDA_ADAPTER
 #include "CudaModelSpecifics.h"
@@ -304,6 +313,76 @@ int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int
         const auto m = inst->ccd->computeFisherInformation(idx);
         for (int i = 0; i < n; ++i)
             for (int j = 0; j < n; ++j) out[(size_t)i * n + j] = m(i, j);
+    });
+}
+
+}  // extern "C"
+
+namespace {
+// OptimizationProfile (src/cyclops/CcdInterface.cpp:223-260): the profile
+// objective at beta[index] = x, the other coefficients refitted
+struct ProfileObjective {
+    CyclicCoordinateDescent& ccd;
+    ModeFindingArguments args;
+    int index;
+    double max, threshold;
+    bool includePenalty;
+    int nEvals = 0;
+    double objective(double x) {
+        ++nEvals;
+        ccd.setBeta(index, x);
+        ccd.setFixedBeta(index, true);
+        ccd.update(args);
+        ccd.setFixedBeta(index, false);
+        double y = ccd.getLogLikelihood() + threshold - max;
+        if (includePenalty) y += ccd.getLogPrior();
+        return y;
+    }
+    double getMaximum() { return threshold; }
+};
+}  // namespace
+
+extern "C" {
+
+int ref_profile(const ref_problem* p, const ref_control* c, const double* start_beta, const int* columns, int n,
+                double threshold, int include_penalty, int override_no_regularization, double* lower,
+                double* upper, int* evaluations, ref_result* fit, int device) {
+    return guarded([&] {
+        auto inst = build(p, device);
+        if (start_beta) {
+            std::vector<double> b(start_beta, start_beta + p->J);
+            inst->ccd->setBeta(b);
+        }
+        const ModeFindingArguments args = toArguments(c);
+        CyclicCoordinateDescent& ccd = *inst->ccd;
+        ccd.update(args);
+        if (fit) fillResult(*inst, p->J, fit);
+        double mode = ccd.getLogLikelihood();
+        if (include_penalty) mode += ccd.getLogPrior();
+        std::vector<double> x0s(p->J);
+        for (int j = 0; j < p->J; ++j) x0s[j] = ccd.getBeta(j);
+        for (int i = 0; i < n; ++i) {
+            if (!override_no_regularization && ccd.getIsRegularized(columns[i])) {
+                std::ostringstream m;
+                m << "Variable " << columns[i] << " is regularized.";
+                throw std::runtime_error(m.str());
+            }
+        }
+        for (int i = 0; i < n; ++i) {                     // bounds (id, +1), (id, -1) in order, one CCD
+            int count = 0;
+            for (double direction : {+1.0, -1.0}) {
+                const int index = columns[i];
+                ProfileObjective eval{ccd, args, index, mode, threshold, include_penalty != 0};
+                bsccs::RZeroIn<ProfileObjective> zeroIn(eval, 1E-3);
+                const double obj0 = eval.getMaximum();
+                auto bracket = zeroIn.bracketSignChange(x0s[index], obj0, direction);
+                const double pt = std::isnan(bracket.second)
+                                      ? NAN : zeroIn.getRoot(x0s[index], bracket.first, obj0, bracket.second);
+                (direction > 0 ? upper : lower)[i] = pt;
+                count += eval.nEvals;
+            }
+            evaluations[i] = count;
+        }
     });
 }
 

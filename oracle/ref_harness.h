@@ -97,4 +97,12 @@ int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out);
  * n x n row-major.  device 1 runs it through the CUDA adapter. */
 int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int n, double* out, int device);
 void ref_ingest_free(ref_ingest_output* out);
+/* Profile-likelihood bounds (CcdInterface::profileModel, src/cyclops/
+ * CcdInterface.cpp:262-420, one thread): fit, then for each column its upper
+ * and lower bound where the profile log likelihood drops by `threshold`
+ * (NaN when the bracket fails); evaluations[i] counts the refits of both.
+ * fit (may be NULL) receives the fit before profiling. */
+int ref_profile(const ref_problem* p, const ref_control* c, const double* start_beta, const int* columns, int n,
+                double threshold, int include_penalty, int override_no_regularization, double* lower,
+                double* upper, int* evaluations, ref_result* fit, int device);
 #endif

@@ -22,7 +22,12 @@ def golden_names():
     """The plain fit fixtures (not the CV folds, ingest tables or swindle fits)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
                   if not p.endswith("cv_folds.npz")
-                  and not os.path.basename(p).startswith(("ingest_", "swindle_")))
+                  and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_")))
+
+
+def profile_names():
+    """Profile-likelihood bound fixtures (profileModel)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "profile_*.npz")))
 
 
 def swindle_names():

@@ -175,6 +175,46 @@ def save_swindle():
         save_case("swindle_" + name, dict(all_cases[name], swindle=1))
 
 
+# (fixture, columns, override_no_regularization, include_penalty, KKT swindle)
+PROFILE_CASES = [("lr_flat", [0, 1, 2, 3], False, True, 0),
+                 ("lr_normal_weighted", [0, 3, 7], True, True, 0),
+                 ("clr_normal_weighted", [0, 5, 9], True, False, 0),
+                 ("pr_offset_normal", [1, 2, 8], True, True, 0),
+                 ("cox_ties_weighted", [0, 4], True, True, 0),
+                 ("lr_laplace_small", [0, 1, 2], True, True, 1)]
+
+
+def save_profile():
+    """Profile-likelihood bounds (CcdInterface::profileModel with one thread,
+    src/cyclops/CcdInterface.cpp:262-420) at the 95 % threshold
+    qchisq(0.95, 1) / 2: profile_<case>.npz holds the problem, the columns
+    and the reference's lower / upper bounds and refit counts."""
+    all_cases = cases()
+    threshold = 1.920729410347062          # qchisq(0.95, df = 1) / 2
+    for name, cols, override, penalty, swindle in PROFILE_CASES:
+        spec = all_cases[name]
+        d = spec["data"]
+        ctl = O.make_control(tolerance=spec.get("tolerance", 1e-6),
+                             convergence_type=spec.get("convergence", D.CONV_GRADIENT), use_kkt_swindle=swindle)
+        w = spec.get("weights")
+        lo, up, ev, fit = O.ref().profile(d, cols, spec["prior"], spec["variance"], threshold, penalty, override,
+                                          control=ctl, weights=w)
+        arrays = dict(
+            model=d.model, y=d.y, col_format=d.col_format, col_ptr=d.col_ptr, col_idx=d.col_idx,
+            val_ptr=d.val_ptr, col_val=d.col_val,
+            pid=d.pid if d.pid is not None else np.zeros(0, np.int32),
+            time=d.time if d.time is not None else np.zeros(0),
+            has_offset=int(d.has_offset), has_intercept=int(d.has_intercept),
+            prior=spec["prior"], variance=spec["variance"],
+            weights=w if w is not None else np.zeros(0),
+            tolerance=ctl.tolerance, convergence=ctl.convergence_type, swindle=swindle,
+            columns=np.asarray(cols, np.int32), threshold=threshold, include_penalty=int(penalty),
+            override=int(override), lower=lo, upper=up, evaluations=ev, beta=fit.beta,
+        )
+        np.savez_compressed(os.path.join(HERE, "profile_" + name + ".npz"), **arrays)
+        print(f"profile_{name:20s} cols={cols} evals={ev.tolist()}")
+
+
 def main(parts):
     if not O.have_ref():
         O.build()
@@ -187,8 +227,10 @@ def main(parts):
         save_ingest()
     if "swindle" in parts:
         save_swindle()
+    if "profile" in parts:
+        save_profile()
 
 
 if __name__ == "__main__":
-    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle]   (default: all)
-    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle"])
+    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile]   (default: all)
+    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile"])

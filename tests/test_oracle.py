@@ -3,7 +3,7 @@ engine (tests/golden/make_golden.py).  No GPU."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, rel_err, swindle_names
+from conftest import golden_names, load_golden, profile_names, rel_err, swindle_names
 from cyclops_b200 import data as D
 from oracle import oracle as O
 
@@ -80,3 +80,43 @@ def test_swindle_fixtures_differ_from_plain_fits():
         _, plain = load_golden(name[len("swindle_"):])
         assert not np.array_equal(sw["beta"], plain["beta"])
         np.testing.assert_allclose(sw["beta"], plain["beta"], atol=5e-2)
+
+
+def test_port_swindle_warm_start_and_pass_limit_match_reference():
+    """A nonzero start on inactive columns (zeroed through updateXBeta) and a
+    pass limit of 2 (MAX_ITERATIONS), against the reference run live."""
+    if not O.have_ref():
+        pytest.skip("reference engine not built here")
+    data, s = load_golden("swindle_lr_laplace_small")
+    start = np.where(np.arange(data.J) % 3 == 0, 0.05, 0.0)
+    for max_it in (1000, 2):
+        ctl = O.make_control(tolerance=1e-8, max_iterations=max_it, use_kkt_swindle=1)
+        a = O.ref().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, start=start)
+        b = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, start=start)
+        assert (a.iterations, a.return_flag) == (b.iterations, b.return_flag)
+        np.testing.assert_allclose(b.beta, a.beta, rtol=1e-12, atol=1e-14)
+    assert b.return_flag == 2          # the pass limit was reached
+
+
+@pytest.mark.parametrize("name", profile_names())
+def test_port_profile_matches_reference_fixture(name):
+    """profileModel (CcdInterface.cpp:262-420, one thread): the restated
+    bracket + Brent root search over warm-started refits lands on the
+    reference's bounds with the same number of refits."""
+    data, s = load_golden(name)
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                         use_kkt_swindle=int(s["swindle"]))
+    lo, up, ev, fit = O.port().profile(data, s["columns"], int(s["prior"]), float(s["variance"]),
+                                       float(s["threshold"]), bool(s["include_penalty"]), bool(s["override"]),
+                                       control=ctl, weights=s["weights"])
+    np.testing.assert_array_equal(ev, s["evaluations"])
+    np.testing.assert_allclose(lo, s["lower"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(up, s["upper"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(fit.beta, s["beta"], rtol=1e-12, atol=1e-14)
+    assert np.all(lo < fit.beta[s["columns"]]) and np.all(fit.beta[s["columns"]] < up)
+
+
+def test_port_profile_rejects_regularized_column():
+    data, s = load_golden("profile_lr_normal_weighted")
+    with pytest.raises(RuntimeError, match="regularized"):
+        O.port().profile(data, [3], int(s["prior"]), float(s["variance"]), override_no_regularization=False)
