@@ -36,7 +36,7 @@ class Control(C.Structure):
     _fields_ = [
         ("tolerance", C.c_double), ("max_iterations", C.c_int), ("convergence_type", C.c_int),
         ("initial_bound", C.c_double), ("max_bound_count", C.c_int), ("precision", C.c_int),
-        ("polish_tolerance", C.c_double),
+        ("polish_tolerance", C.c_double), ("use_kkt_swindle", C.c_int),
     ]
 
 
@@ -104,6 +104,11 @@ _SIGS = {
                         C.POINTER(Control), C.POINTER(FitResult), C.c_void_p, C.c_void_p],
     "cyc_fit_host_loop": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control),
                           C.POINTER(FitResult)],
+    "cyc_profile_log_likelihood": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_int,
+                                   C.c_void_p, C.c_int, C.c_int, C.c_void_p],
+    "cyc_profile_bounds": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_void_p,
+                           C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                           C.POINTER(FitResult)],
 }
 _RESTYPE = {"cyc_last_error": C.c_char_p, "cyc_launch_count": C.c_longlong}
 

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import ctypes as C
 import dataclasses
+import statistics
 from typing import List, Optional, Sequence
 
 import numpy as np
@@ -54,16 +55,19 @@ class ControlSpec:
     max_bound_count: int = 5
     precision: int = FP64
     polish_tolerance: float = 1e-4
+    use_kkt_swindle: bool = False
 
 
 def create_control(tolerance=1e-6, max_iterations=1000, convergence_type="gradient",
                    initial_bound=2.0, max_bound_count=5, precision="fp64",
-                   polish_tolerance=1e-4) -> ControlSpec:
-    """createControl (R/ModelFit.R:489-540); defaults are the reference's."""
+                   polish_tolerance=1e-4, use_kkt_swindle=False) -> ControlSpec:
+    """createControl (R/ModelFit.R:489-540); defaults are the reference's.
+    `use_kkt_swindle` is createControl's useKKTSwindle: fit_cyclops_model
+    then runs the reference's active-set passes under a Laplace prior."""
     ct = _CONV[convergence_type] if isinstance(convergence_type, str) else int(convergence_type)
     pr = {"fp64": FP64, "mixed": MIXED}[precision] if isinstance(precision, str) else int(precision)
     return ControlSpec(tolerance, max_iterations, ct, initial_bound, max_bound_count, pr,
-                       polish_tolerance)
+                       polish_tolerance, bool(use_kkt_swindle))
 
 
 def _exclude_for(data: CyclopsData, prior: PriorSpec) -> List[int]:
@@ -250,7 +254,7 @@ def _control_struct(c: ControlSpec) -> N.Control:
     return N.Control(tolerance=c.tolerance, max_iterations=c.max_iterations,
                      convergence_type=c.convergence_type, initial_bound=c.initial_bound,
                      max_bound_count=c.max_bound_count, precision=c.precision,
-                     polish_tolerance=c.polish_tolerance)
+                     polish_tolerance=c.polish_tolerance, use_kkt_swindle=int(c.use_kkt_swindle))
 
 
 def _prior_struct(data: CyclopsData, prior: PriorSpec):
@@ -280,6 +284,73 @@ def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional
     fn = N.lib().cyc_fit_host_loop if host_loop else N.lib().cyc_fit
     N.check(fn(ds.handle, C.byref(p), C.byref(spec), C.byref(c), C.byref(out)))
     return FitResult(beta, out.log_likelihood, out.log_prior, out.iterations, out.return_flag)
+
+
+@dataclasses.dataclass
+class ProfileBounds:
+    columns: np.ndarray           # the profiled columns
+    lower: np.ndarray             # lower confidence bound per column (NaN: no bracket found)
+    upper: np.ndarray             # upper confidence bound per column
+    evaluations: np.ndarray       # refits spent on both bounds
+    fit: FitResult                # the fit the bounds are around
+
+
+def profile_threshold(level: float = 0.95) -> float:
+    """qchisq(level, df = 1) / 2 (R/ModelFit.R:772): z^2 / 2 with z the
+    (1 + level) / 2 normal quantile."""
+    if not 0.01 <= level <= 0.99:
+        raise ValueError("level must be between 0 and 1")
+    z = statistics.NormalDist().inv_cdf((1.0 + level) / 2.0)
+    return z * z / 2.0
+
+
+def profile_bounds(data, columns: Sequence[int], prior: Optional[PriorSpec] = None,
+                   control: Optional[ControlSpec] = None, level: float = 0.95, threshold: Optional[float] = None,
+                   include_penalty: bool = True, override_no_regularization: bool = False, weights=None,
+                   starting_coefficients=None, device: int = 0) -> ProfileBounds:
+    """confint.cyclopsFit (R/ModelFit.R:762-800) through
+    CcdInterface::profileModel with one thread: fit on the GPU, then the
+    profile-likelihood bounds of `columns`, each refit on the GPU."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    prior = prior or create_prior("none")
+    control = control or create_control()
+    thr = profile_threshold(level) if threshold is None else float(threshold)
+    p, keep_ex = _prior_struct(ds.data, prior)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    s = None if starting_coefficients is None else np.ascontiguousarray(starting_coefficients, np.float64)
+    spec = N.FitSpec(weights=_ptr(w), variance=prior.variance, start_beta=_ptr(s))
+    cols = np.ascontiguousarray(columns, np.int32)
+    n = int(cols.size)
+    lo, up, ev = np.zeros(n), np.zeros(n), np.zeros(n, np.int32)
+    beta = np.zeros(ds.data.J)
+    out = N.FitResult(beta=beta.ctypes.data)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_profile_bounds(ds.handle, C.byref(p), C.byref(spec), C.byref(c), _ptr(cols), n, thr,
+                                       int(include_penalty), int(override_no_regularization), _ptr(lo), _ptr(up),
+                                       _ptr(ev), C.byref(out)))
+    return ProfileBounds(cols, lo, up, ev, FitResult(beta, out.log_likelihood, out.log_prior, out.iterations,
+                                                     out.return_flag))
+
+
+def profile_log_likelihood(data, column: int, points: Sequence[float], prior: Optional[PriorSpec] = None,
+                           control: Optional[ControlSpec] = None, include_penalty: bool = True, weights=None,
+                           starting_coefficients=None, device: int = 0) -> np.ndarray:
+    """getCyclopsProfileLogLikelihood (R/ModelFit.R:816-826) through
+    CcdInterface::evaluateProfileModel with one thread: fit on the GPU,
+    then the profile log likelihood of `column` at each point."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    prior = prior or create_prior("none")
+    control = control or create_control()
+    p, keep_ex = _prior_struct(ds.data, prior)
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    s = None if starting_coefficients is None else np.ascontiguousarray(starting_coefficients, np.float64)
+    spec = N.FitSpec(weights=_ptr(w), variance=prior.variance, start_beta=_ptr(s))
+    pts = np.ascontiguousarray(points, np.float64)
+    vals = np.zeros(pts.size)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_profile_log_likelihood(ds.handle, C.byref(p), C.byref(spec), C.byref(c), int(column),
+                                               _ptr(pts), int(pts.size), int(include_penalty), _ptr(vals)))
+    return vals
 
 
 @dataclasses.dataclass

@@ -1935,6 +1935,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
                std::vector<double>* pll) {
     CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
                 "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
+    CYC_REQUIRE(!ctl->use_kkt_swindle, CYC_ERR_UNSUPPORTED, "the KKT swindle is offered by cyc_fit only");
     CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
                     ctl->convergence_type == CYC_CONV_LANGE,
                 CYC_ERR_UNSUPPORTED, "batched fits support gradient, mittal and lange convergence");

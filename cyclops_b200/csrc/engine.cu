@@ -496,6 +496,45 @@ void Engine::fisher_information(const int* cols, int n, double* out) {
     for (int p = 0; p < np; ++p) out[(size_t)pa[p] * n + pb[p]] = out[(size_t)pb[p] * n + pa[p]] = h[p];
 }
 
+// computeKktConditions (CyclicCoordinateDescent.cpp:817-837): |gradient| of
+// columns cols[0..n) (host ids; d_cols the same ids on the device) into
+// d_out[0..n) at the current state.  lr / pr / clr / cpr score every column
+// in one launch; cox walks its risk sets column by column.
+void Engine::kkt_scores(const int* cols, const int* d_cols, int n, bool use_weights, double* d_out) {
+    if (n == 0) return;
+    const bool uw = use_weights && use_w;
+    const int K = ds->K;
+    const int blocks = std::min((n + kThreads / 32 - 1) / (kThreads / 32), 148 * 16);
+    const int* fmt = ds->d_fmt.get();
+    const long long* cp = ds->d_col_ptr.get();
+    const long long* vp = ds->d_val_ptr.get();
+    const int* ix = ds->d_idx.get();
+    const double* vl = ds->d_val.get();
+    if (model_independent(model)) {
+        if (model == CYC_LR)
+            launch(k_kkt_independent<CYC_LR>, blocks, kThreads, 0, stream, n, d_cols, K, fmt, cp, vp, ix, vl,
+                   (const double*)exb.get(), (const double*)denom.get(), (const double*)nw.get(), uw ? 1 : 0,
+                   (const double*)xjy.get(), d_out);
+        else
+            launch(k_kkt_independent<CYC_PR>, blocks, kThreads, 0, stream, n, d_cols, K, fmt, cp, vp, ix, vl,
+                   (const double*)exb.get(), (const double*)denom.get(), (const double*)nw.get(), uw ? 1 : 0,
+                   (const double*)xjy.get(), d_out);
+    } else if (model_grouped(model)) {
+        launch(k_kkt_grouped, blocks, kThreads, 0, stream, n, d_cols, K, fmt, cp, vp, ix, vl, groups(),
+               (const double*)exb.get(), (const double*)denom.get(), (const double*)nw.get(),
+               (const double*)xjy.get(), d_out);
+    } else {
+        DevBuf<double> gh;
+        gh.alloc(2 * (size_t)n);
+        for (int i = 0; i < n; ++i) {
+            numerator_for_gradient(cols[i], use_weights);
+            launch_gradient(cols[i], use_weights, gh.get() + 2 * (size_t)i);
+        }
+        launch(k_abs_gradients, grid_for(n, 1), kThreads, 0, stream, n, (const double*)gh.get(), d_out);
+    }
+    CYC_CHECK_LAUNCH();
+}
+
 void Engine::get_xbeta(double* out) {
     CYC_CHECK_CUDA(cudaMemcpyAsync(out, xb.get(), ds->K * sizeof(double), cudaMemcpyDeviceToHost, stream));
     sync();

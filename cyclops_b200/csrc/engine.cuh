@@ -68,6 +68,7 @@ struct Engine {
     void predictive_estimates(double* y, const double* w);
     void get_xbeta(double* out);
     void fisher_information(const int* cols, int n, double* out);
+    void kkt_scores(const int* cols, const int* d_cols, int n, bool use_weights, double* d_out);
     void save_xbeta();
     void get_xbeta_save(double* out);
 };

@@ -409,6 +409,68 @@ __global__ void k_copy_neg_xjy(const double* __restrict__ xjy, int j, double* ou
     out[1] = 0.0;
 }
 
+// ---- KKT conditions (CyclicCoordinateDescent.cpp:817-837) ---------------------
+
+// |gradient| of every listed column at the current state, one warp per
+// column: the gradient halves of k_gh_independent / k_gh_grouped, so one
+// launch scores the whole inactive set of the KKT swindle.  Empty columns
+// score 0 (ModelSpecifics.hpp:720-723).
+template <int MODEL>
+__global__ void k_kkt_independent(int n_cols, const int* __restrict__ cols, int K, const int* fmt,
+                                  const long long* col_ptr, const long long* val_ptr, const int* idx,
+                                  const double* val, const double* __restrict__ exb,
+                                  const double* __restrict__ denom, const double* __restrict__ nw, int use_w,
+                                  const double* __restrict__ xjy, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_cols; c += nwarps) {
+        const int j = cols[c];
+        const ColView v = fisher_view(j, K, fmt, col_ptr, val_ptr, idx, val);
+        double g = 0.0;
+        for (long long e = lane; e < v.n; e += 32) {
+            const int k = v.row(e);
+            const double n1 = exb[k] * v.x(e);
+            const double w = use_w ? nw[k] : 1.0;
+            g += w * (MODEL == CYC_LR ? n1 / denom[k] : n1);
+        }
+        for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+        if (lane == 0) out[c] = v.n == 0 ? 0.0 : fabs(g - xjy[j]);
+    }
+}
+
+// grouped rows: the first entry of each run of one stratum walks the run
+__global__ void k_kkt_grouped(int n_cols, const int* __restrict__ cols, int K, const int* fmt,
+                              const long long* col_ptr, const long long* val_ptr, const int* idx,
+                              const double* val, const int* __restrict__ group, const double* __restrict__ exb,
+                              const double* __restrict__ denom, const double* __restrict__ nw,
+                              const double* __restrict__ xjy, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < n_cols; c += nwarps) {
+        const int j = cols[c];
+        const ColView v = fisher_view(j, K, fmt, col_ptr, val_ptr, idx, val);
+        double g = 0.0;
+        for (long long e = lane; e < v.n; e += 32) {
+            const int key = group[v.row(e)];
+            if (e > 0 && group[v.row(e - 1)] == key) continue;
+            double n1 = 0.0;
+            long long f = e;
+            do {
+                n1 += exb[v.row(f)] * v.x(f);
+                ++f;
+            } while (f < v.n && group[v.row(f)] == key);
+            g += nw[key] * (n1 / denom[key]);
+        }
+        for (int o = 16; o; o >>= 1) g += __shfl_xor_sync(0xffffffffu, g, o);
+        if (lane == 0) out[c] = v.n == 0 ? 0.0 : fabs(g - xjy[j]);
+    }
+}
+
+// |gh[2i]| -> out[i]
+__global__ void k_abs_gradients(int n, const double* __restrict__ gh, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = fabs(gh[2 * i]);
+}
+
 // ---- updateXBeta (ModelSpecifics.hpp:1524-1586) -----------------------------
 
 // independent rows: each row is its own denominator

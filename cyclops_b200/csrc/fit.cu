@@ -12,8 +12,10 @@
 #include "solver_common.cuh"
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <memory>
+#include <string>
 
 namespace cyc {
 
@@ -90,7 +92,7 @@ struct FitRunner {
     Engine& e;
     const cyc_control& ctl;
     int J;
-    std::vector<int> fixb;
+    std::vector<int> fixb, base_fix, pt, graphs_fix;
     DevBuf<double> beta, hdelta, gh, delta, obj, last;
     DevBuf<int> ptype, flags;
     DevBuf<unsigned long long> n_updates;
@@ -107,7 +109,8 @@ struct FitRunner {
         h_start.assign(J, 0.0);
         if (spec.start_beta) std::copy(spec.start_beta, spec.start_beta + J, h_start.begin());
         if (e.ds->has_offset) { fixb[0] = 1; h_start[0] = 1.0; }   // CCD init :218-221
-        std::vector<int> pt(J, prior.prior_type);
+        base_fix = fixb;
+        pt.assign(J, prior.prior_type);
         for (int i = 0; i < prior.n_exclude; ++i) {
             CYC_REQUIRE(prior.exclude[i] >= 0 && prior.exclude[i] < J, CYC_ERR_ARGUMENT, "exclude index out of range");
             pt[prior.exclude[i]] = CYC_PRIOR_NONE;
@@ -153,6 +156,9 @@ struct FitRunner {
 
     // one cycle as a list of graphs of at most `chunk` coordinates each
     void build_graphs() {
+        for (auto g : graphs) CYC_CHECK_CUDA(cudaGraphExecDestroy(g));
+        graphs.clear();
+        graphs_fix = fixb;
         const int chunk = 4096;
         for (int b = 0; b < J; b += chunk) {
             cudaGraph_t g;
@@ -221,23 +227,91 @@ struct FitRunner {
         return CYC_MAX_ITERATIONS;
     }
 
-    void run(cyc_fit_result* out) {
-        const double* w = nullptr;
-        (void)w;
-        e.fixed_terms_ll(true);
-        e.fixed_terms_gh(true);
-        set_beta(h_start);
-        e.remaining_statistics(true);
-        build_graphs();
-        CYC_CHECK_CUDA(cudaEventRecord(ev0, e.stream));
+    // kktSwindle (CyclicCoordinateDescent.cpp:636-814).  The intercept and
+    // the columns whose prior has no KKT boundary (flat, normal) start
+    // active, the Laplace columns inactive at beta 0 (a nonzero start is
+    // zeroed through updateXBeta, as setBeta does, :473-486).  Each pass runs
+    // findMode over the active set (:617-634: every other column fixed), then
+    // scores the inactive columns' |gradient| in one launch and moves every
+    // column above lambda into the active set (the violators at the front of
+    // the reference's sorted list, :739-792); it ends when nothing is
+    // inactive, the fit failed, no column violates, or after max_iterations
+    // passes (MAX_ITERATIONS).  An empty active set skips findMode.
+    int kkt_swindle(double bound, int* iterations) {
+        const int intercept = e.ds->has_intercept ? (e.ds->has_offset ? 1 : 0) : -1;
+        std::vector<char> active(J, 0);
+        int n_active = 0, n_inactive = 0;
+        for (int j = 0; j < J; ++j) {
+            if (base_fix[j]) continue;
+            active[j] = (j == intercept || pt[j] != CYC_PRIOR_LAPLACE);
+            if (active[j]) ++n_active;
+            else ++n_inactive;
+        }
+        const double lambda = std::sqrt(2.0 / variance);      // getKktBoundary, CovariatePrior.h:235-238
+        std::vector<double> hb(J);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(hb.data(), beta.get(), J * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        e.sync();
+        for (int j = 0; j < J; ++j) {
+            if (base_fix[j] || active[j] || hb[j] == 0.0) continue;
+            CYC_CHECK_CUDA(cudaMemsetAsync(beta.get() + j, 0, sizeof(double), e.stream));
+            e.launch_update(j, true, nullptr, 0.0 - hb[j]);
+        }
+        std::vector<int> inactive;
+        DevBuf<int> d_inactive;
+        DevBuf<double> d_score;
+        std::vector<double> score;
+        int flag = CYC_SUCCESS;
+        for (int pass = 1;; ++pass) {
+            flag = CYC_SUCCESS;
+            if (n_active > 0) {
+                for (int j = 0; j < J; ++j) fixb[j] = !active[j];
+                build_graphs();
+                flag = find_mode(bound, iterations);
+            }
+            if (n_inactive == 0 || flag != CYC_SUCCESS) break;
+            if (pass == ctl.max_iterations) { flag = CYC_MAX_ITERATIONS; break; }
+            inactive.clear();
+            for (int j = 0; j < J; ++j)
+                if (!base_fix[j] && !active[j]) inactive.push_back(j);
+            const int n = (int)inactive.size();
+            d_inactive.alloc(n);
+            d_score.alloc(n);
+            score.resize(n);
+            CYC_CHECK_CUDA(cudaMemcpyAsync(d_inactive.get(), inactive.data(), n * sizeof(int), cudaMemcpyHostToDevice, e.stream));
+            e.kkt_scores(inactive.data(), d_inactive.get(), n, true, d_score.get());
+            CYC_CHECK_CUDA(cudaMemcpyAsync(score.data(), d_score.get(), n * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+            e.sync();
+            int moved = 0;
+            for (int i = 0; i < n; ++i)
+                if (!(score[i] <= lambda)) { active[inactive[i]] = 1; ++moved; }
+            if (moved == 0) break;
+            n_active += moved;
+            n_inactive -= moved;
+        }
+        fixb = base_fix;
+        return flag;
+    }
+
+    bool swindle = false;
+
+    // the graphs replay one cycle over the columns not fixed now
+    void ensure_graphs() {
+        if (graphs.empty() || graphs_fix != fixb) build_graphs();
+    }
+
+    // update (CyclicCoordinateDescent.cpp:586-615): findMode (or the
+    // swindle), restarted from beta 0 with a tenfold smaller trust region
+    // while ill-conditioned, at most max_bound_count times
+    int update(int* iters) {
         double bound = ctl.initial_bound;
-        int count = 0, flag = CYC_SUCCESS, iters = 0;
-        for (;;) {                                               // update :586-615
-            flag = find_mode(bound, &iters);
+        int count = 0, flag = CYC_SUCCESS;
+        for (;;) {
+            if (!swindle) ensure_graphs();
+            flag = swindle ? kkt_swindle(bound, iters) : find_mode(bound, iters);
             ++count;
             if (flag == CYC_ILLCONDITIONED && count < ctl.max_bound_count) {
                 bound /= 10.0;
-                std::vector<double> b(J, 0.0);                   // resetBeta
+                std::vector<double> b(J, 0.0);                   // resetBeta :256-264
                 if (e.ds->has_offset) b[0] = 1.0;
                 set_beta(b);
                 e.remaining_statistics(true);
@@ -245,21 +319,45 @@ struct FitRunner {
                 break;
             }
         }
-        CYC_CHECK_CUDA(cudaEventRecord(ev1, e.stream));
-        // results
-        CYC_CHECK_CUDA(cudaMemcpyAsync(out->beta, beta.get(), J * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        return flag;
+    }
+
+    void prepare() {
+        e.fixed_terms_ll(true);
+        e.fixed_terms_gh(true);
+        set_beta(h_start);
+        e.remaining_statistics(true);
+        // the swindle runs when some prior has a KKT boundary (JointPrior.h:149-157)
+        swindle = ctl.use_kkt_swindle && std::count(pt.begin(), pt.end(), (int)CYC_PRIOR_LAPLACE) > 0;
+        if (!swindle) ensure_graphs();
+    }
+
+    // getLogLikelihood and getLogPrior at the current state
+    void objective_terms(double* ll, double* lp) {
         e.launch_loglik(true, obj.get());
         launch(k_add_logprior, 1, kThreads, 0, e.stream, J, beta.get(), ptype.get(), variance, nullptr, last.get());
-        double h2[2];
-        CYC_CHECK_CUDA(cudaMemcpyAsync(&h2[0], obj.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
-        CYC_CHECK_CUDA(cudaMemcpyAsync(&h2[1], last.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
-        unsigned long long nup = 0;
-        CYC_CHECK_CUDA(cudaMemcpyAsync(&nup, n_updates.get(), sizeof(nup), cudaMemcpyDeviceToHost, e.stream));
+        CYC_CHECK_LAUNCH();
+        CYC_CHECK_CUDA(cudaMemcpyAsync(&h_block.as<double>()[1], obj.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        CYC_CHECK_CUDA(cudaMemcpyAsync(&h_block.as<double>()[2], last.get(), sizeof(double), cudaMemcpyDeviceToHost, e.stream));
         e.sync();
-        out->log_likelihood = h2[0];
-        out->log_prior = h2[1];
+        *ll = h_block.as<double>()[1];
+        *lp = h_block.as<double>()[2];
+    }
+
+    void results(cyc_fit_result* out, int flag, int iters) {
+        CYC_CHECK_CUDA(cudaMemcpyAsync(out->beta, beta.get(), J * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        objective_terms(&out->log_likelihood, &out->log_prior);
         out->iterations = iters;
         out->return_flag = flag;
+    }
+
+    void run(cyc_fit_result* out) {
+        prepare();
+        CYC_CHECK_CUDA(cudaEventRecord(ev0, e.stream));
+        int iters = 0;
+        const int flag = update(&iters);
+        CYC_CHECK_CUDA(cudaEventRecord(ev1, e.stream));
+        results(out, flag, iters);
         float ms = 0.f;
         CYC_CHECK_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
         cyc_run_stats st{};
@@ -270,7 +368,167 @@ struct FitRunner {
         st.phase_ms[0] = ms;
         st.phase_state_bytes[0] = 8;
         set_last_stats(st);
-        (void)nup;
+    }
+
+    // ---- profile likelihood (CcdInterface.cpp:223-420) ----------------------
+
+    // setBeta(j, x) (CyclicCoordinateDescent.cpp:473-486): beta_j += x - beta_j
+    // through updateXBeta, so the statistics stay current
+    void set_coordinate(int j, double x) {
+        double* hb = h_block.as<double>() + 3;
+        CYC_CHECK_CUDA(cudaMemcpyAsync(hb, beta.get() + j, sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        e.sync();
+        const double delta = x - hb[0];
+        hb[0] += delta;
+        CYC_CHECK_CUDA(cudaMemcpyAsync(beta.get() + j, hb, sizeof(double), cudaMemcpyHostToDevice, e.stream));
+        e.launch_update(j, true, nullptr, delta);
+        e.sync();
+    }
+
+    // OptimizationProfile::objective (CcdInterface.cpp:238-249): beta_j = x
+    // held fixed while update refits the rest from the current state
+    double profile_objective(int j, double x, double mode, double threshold, bool penalty, int* evals) {
+        ++*evals;
+        set_coordinate(j, x);
+        fixb[j] = base_fix[j] = 1;
+        int iters = 0;
+        update(&iters);
+        fixb[j] = base_fix[j] = 0;
+        double ll, lp;
+        objective_terms(&ll, &lp);
+        double y = ll + threshold - mode;
+        if (penalty) y += lp;
+        return y;
+    }
+
+    // RZeroIn::bracketSignChange (src/utils/RZeroIn.h): steps of 0.1, 0.2,
+    // 0.4, ... times max(|x0|, 0.01) from x0 until the objective is no
+    // longer positive; a NaN objective when it turns NaN or after 22 steps
+    double bracket(int j, double x0, double f0, double direction, double* f1, double mode, double threshold,
+                   bool penalty, int* evals) {
+        const double displacement = std::max(std::fabs(x0), 0.01);
+        double multiplier = 0.1;
+        double x1 = x0, y1 = f0;
+        for (int steps = 0; y1 > 0; ++steps) {
+            x1 = x0 + direction * displacement * multiplier;
+            y1 = profile_objective(j, x1, mode, threshold, penalty, evals);
+            if (std::isnan(y1)) break;
+            if (steps > 20) { y1 = NAN; break; }
+            multiplier *= 2.0;
+        }
+        *f1 = y1;
+        return x1;
+    }
+
+    // Brent's root finder in the form of Forsythe, Malcolm & Moler
+    // (Computer Methods for Mathematical Computations, 1977, zeroin), the
+    // variant RZeroIn::getRoot runs: given f(a), f(b) of opposite signs, each
+    // step takes inverse quadratic (or secant) interpolation when it lands
+    // well inside [b, c] and shrinks the bracket fast enough, bisection
+    // otherwise; it stops when half the bracket is within 2 eps |b| + tol / 2
+    // or after max_it + 1 steps
+    double root(int j, double a, double b, double fa, double fb, double tol, int max_it, double mode,
+                double threshold, bool penalty, int* evals) {
+        if (b < a) {
+            std::swap(a, b);
+            std::swap(fa, fb);
+        }
+        if (fa == 0.0) return a;
+        if (fb == 0.0) return b;
+        double c = a, fc = fa;
+        for (int k = 0; k <= max_it; ++k) {
+            const double prev_step = b - a;
+            if (std::fabs(fc) < std::fabs(fb)) {                 // b: the best point so far
+                a = b; b = c; c = a;
+                fa = fb; fb = fc; fc = fa;
+            }
+            const double tol_act = 2 * DBL_EPSILON * std::fabs(b) + tol / 2;
+            double step = (c - b) / 2;
+            if (std::fabs(step) <= tol_act || fb == 0.0) return b;
+            if (std::fabs(prev_step) >= tol_act && std::fabs(fa) > std::fabs(fb)) {
+                const double cb = c - b;
+                double p, q;
+                if (a == c) {                                    // secant
+                    const double t1 = fb / fa;
+                    p = cb * t1;
+                    q = 1.0 - t1;
+                } else {                                         // inverse quadratic
+                    const double r = fa / fc, t1 = fb / fc, t2 = fb / fa;
+                    p = t2 * (cb * r * (r - t1) - (b - a) * (t1 - 1.0));
+                    q = (r - 1.0) * (t1 - 1.0) * (t2 - 1.0);
+                }
+                if (p > 0) q = -q;
+                else p = -p;
+                if (p < (0.75 * cb * q - std::fabs(tol_act * q) / 2) && p < std::fabs(prev_step * q / 2)) step = p / q;
+            }
+            if (std::fabs(step) < tol_act) step = step > 0 ? tol_act : -tol_act;
+            a = b;
+            fa = fb;
+            b += step;
+            fb = profile_objective(j, b, mode, threshold, penalty, evals);
+            if ((fb > 0 && fc > 0) || (fb < 0 && fc < 0)) {
+                c = a;
+                fc = fa;
+            }
+        }
+        return b;
+    }
+
+    // evaluateProfileModel with one thread (CcdInterface.cpp:527-618): fit;
+    // makeDirty (CyclicCoordinateDescent.cpp:448-452), so the first refit
+    // rebuilds the fixed terms, xbeta and the statistics from beta; one
+    // refit at 0; then the objective (threshold 0, mode 0) at each point,
+    // each refit warm-started from the last
+    void profile_points(int j, const double* points, int n, bool penalty, double* values) {
+        prepare();
+        int iters = 0;
+        update(&iters);
+        set_coordinate(j, 0.0);
+        e.fixed_terms_ll(true);
+        e.fixed_terms_gh(true);
+        e.compute_xbeta_device(beta.get());
+        e.remaining_statistics(true);
+        fixb[j] = base_fix[j] = 1;
+        update(&iters);
+        fixb[j] = base_fix[j] = 0;
+        int evals = 0;
+        for (int i = 0; i < n; ++i) values[i] = profile_objective(j, points[i], 0.0, 0.0, penalty, &evals);
+    }
+
+    // profileModel with one thread (CcdInterface.cpp:262-420): fit, then for
+    // each column its upper and then its lower bound, all on one state
+    void profile(const int* cols, int n, double threshold, bool penalty, double* lower, double* upper,
+                 int* evaluations, cyc_fit_result* out) {
+        prepare();
+        int iters = 0;
+        const int flag = update(&iters);
+        std::vector<double> x0s(J);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(x0s.data(), beta.get(), J * sizeof(double), cudaMemcpyDeviceToHost, e.stream));
+        double ll, lp;
+        objective_terms(&ll, &lp);
+        if (out) {
+            std::copy(x0s.begin(), x0s.end(), out->beta);
+            out->log_likelihood = ll;
+            out->log_prior = lp;
+            out->iterations = iters;
+            out->return_flag = flag;
+        }
+        const double mode = penalty ? ll + lp : ll;
+        for (int i = 0; i < n; ++i) {
+            const int j = cols[i];
+            int count = 0;
+            for (double direction : {1.0, -1.0}) {
+                int evals = 0;
+                double f1;
+                const double x1 = bracket(j, x0s[j], threshold, direction, &f1, mode, threshold, penalty, &evals);
+                const double pt = std::isnan(f1) ? NAN
+                                                 : root(j, x0s[j], x1, threshold, f1, 1e-3, 1000, mode, threshold,
+                                                        penalty, &evals);
+                (direction > 0 ? upper : lower)[i] = pt;
+                count += evals;
+            }
+            evaluations[i] = count;
+        }
     }
 };
 
@@ -400,12 +658,63 @@ extern "C" int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_sp
     });
 }
 
+extern "C" int cyc_profile_bounds(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                                  const cyc_control* control, const int* columns, int n, double threshold,
+                                  int include_penalty, int override_no_regularization, double* lower,
+                                  double* upper, int* evaluations, cyc_fit_result* fit) {
+    return guarded([&] {
+        CYC_REQUIRE(ds && prior && spec && control && n >= 0, CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(n == 0 || (columns && lower && upper && evaluations), CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(!fit || fit->beta, CYC_ERR_ARGUMENT, "null result buffer");
+        CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
+                    CYC_ERR_ARGUMENT, "Unknown prior type");
+        CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || spec->variance > 0, CYC_ERR_ARGUMENT,
+                    "prior variance must be positive");
+        const Dataset& d = ds->ds;
+        for (int i = 0; i < n; ++i)
+            CYC_REQUIRE(columns[i] >= 0 && columns[i] < d.J && !(d.has_offset && columns[i] == 0), CYC_ERR_ARGUMENT,
+                        "profile column out of range (or the offset)");
+        CYC_CHECK_CUDA(cudaSetDevice(d.device));
+        Engine eng(&ds->ds);
+        StreamScope scope(eng.stream);
+        eng.set_weights(spec->weights, spec->weights != nullptr);
+        FitRunner r(eng, *prior, *spec, *control);
+        for (int i = 0; i < n; ++i)                       // CcdInterface.cpp:297-302
+            CYC_REQUIRE(override_no_regularization || r.pt[columns[i]] == CYC_PRIOR_NONE, CYC_ERR_ARGUMENT,
+                        "Variable " + std::to_string(columns[i]) + " is regularized.");
+        r.profile(columns, n, threshold, include_penalty != 0, lower, upper, evaluations, fit);
+    });
+}
+
+extern "C" int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                                          const cyc_control* control, int column, const double* points, int n,
+                                          int include_penalty, double* values) {
+    return guarded([&] {
+        CYC_REQUIRE(ds && prior && spec && control && n >= 0 && (n == 0 || (points && values)), CYC_ERR_ARGUMENT,
+                    "null argument");
+        CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
+                    CYC_ERR_ARGUMENT, "Unknown prior type");
+        CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || spec->variance > 0, CYC_ERR_ARGUMENT,
+                    "prior variance must be positive");
+        const Dataset& d = ds->ds;
+        CYC_REQUIRE(column >= 0 && column < d.J && !(d.has_offset && column == 0), CYC_ERR_ARGUMENT,
+                    "profile column out of range (or the offset)");
+        CYC_CHECK_CUDA(cudaSetDevice(d.device));
+        Engine eng(&ds->ds);
+        StreamScope scope(eng.stream);
+        eng.set_weights(spec->weights, spec->weights != nullptr);
+        FitRunner r(eng, *prior, *spec, *control);
+        r.profile_points(column, points, n, include_penalty != 0, values);
+    });
+}
+
 extern "C" int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
                                  const cyc_control* control, cyc_fit_result* out) {
     return guarded([&] {
         CYC_REQUIRE(ds && prior && spec && control && out && out->beta, CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
                     CYC_ERR_ARGUMENT, "Unknown prior type");
+        CYC_REQUIRE(!control->use_kkt_swindle, CYC_ERR_UNSUPPORTED, "the KKT swindle is offered by cyc_fit only");
         CYC_CHECK_CUDA(cudaSetDevice(ds->ds.device));
         Engine eng(&ds->ds);
         StreamScope scope(eng.stream);

@@ -170,6 +170,11 @@ typedef struct {
     int max_bound_count;        /* default 5 */
     int precision;              /* cyc_precision */
     double polish_tolerance;    /* CYC_MIXED: FP32 phase stops at this tolerance */
+    int use_kkt_swindle;        /* useKktSwindle (CcdInterface.h:77): the active-set
+                                   passes of CyclicCoordinateDescent::kktSwindle
+                                   (CyclicCoordinateDescent.cpp:636-814) under a
+                                   Laplace prior; cyc_fit only, the batched
+                                   solvers return CYC_ERR_UNSUPPORTED */
 } cyc_control;
 
 /* the prior: one default prior for every column, a flat prior on `exclude`
@@ -221,6 +226,33 @@ int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* s
 int cyc_cv_grid_fit(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds,
                     const double* variances, int n_var, const cyc_control* control,
                     cyc_fit_result* out, double* pred_loglik, double* grid_mean);
+
+/* Profile-likelihood confidence bounds (CcdInterface::profileModel with one
+ * thread, src/cyclops/CcdInterface.cpp:262-420; R confint.cyclopsFit,
+ * R/ModelFit.R:762-800): fits (as cyc_fit), then for each column of
+ * `columns` finds where the profile log likelihood (plus the log prior when
+ * include_penalty) has dropped by `threshold` (qchisq(level, 1) / 2) above
+ * (`upper[i]`) and below (`lower[i]`) the estimate, NaN where no bracket was
+ * found; `evaluations[i]` counts the refits of both.  Each refit holds the
+ * column fixed and warm-starts from the previous refit's state
+ * (OptimizationProfile, :223-260); the bracket grows as RZeroIn's
+ * bracketSignChange and the root is Brent's zeroin at tolerance 1e-3
+ * (src/utils/RZeroIn.h).  A column with a prior is rejected unless
+ * override_no_regularization; the offset column is rejected.  `fit` (may
+ * be NULL) receives the fit before profiling. */
+int cyc_profile_bounds(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                       const cyc_control* control, const int* columns, int n, double threshold,
+                       int include_penalty, int override_no_regularization, double* lower, double* upper,
+                       int* evaluations, cyc_fit_result* fit);
+
+/* The profile log likelihood (plus the log prior when include_penalty) of
+ * `column` at `points` (CcdInterface::evaluateProfileModel with one thread,
+ * src/cyclops/CcdInterface.cpp:527-618; R getCyclopsProfileLogLikelihood,
+ * R/ModelFit.R:816-826): fits (as cyc_fit), then refits with the column
+ * held at each point in turn, each refit warm-started from the last. */
+int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                               const cyc_control* control, int column, const double* points, int n,
+                               int include_penalty, double* values);
 
 /* Cross-validation fold masks, `n_reps * folds` rows of K weights (0 = held
  * out), exactly as CrossValidationSelector draws them

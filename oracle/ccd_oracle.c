@@ -780,6 +780,38 @@ static double profile_root(Profile* f, double a, double b, double fa, double fb,
     return b;
 }
 
+/* evaluateProfileModel with one thread (CcdInterface.cpp:527-618): fit;
+ * makeDirty (CyclicCoordinateDescent.cpp:448-452), so the first refit's
+ * findMode recomputes the fixed terms, xbeta and the statistics from beta;
+ * one refit at 0; then values[i] = the refit objective at points[i]
+ * (threshold 0, mode 0), each refit warm-started from the last */
+int ccd_oracle_profile_points(const ccd_problem* p, const ccd_control* ctl, const double* start, int column,
+                              const double* points, int n, int include_penalty, double* values) {
+    Ctx c;
+    if (ctx_init(&c, p)) return 1;
+    if (column < 0 || column >= p->J || (p->has_offset && column == 0)) {
+        snprintf(g_err, sizeof g_err, "profile column %d out of range", column);
+        ctx_free(&c);
+        return 1;
+    }
+    if (start) for (int j = 0; j < p->J; ++j) c.beta[j] = start[j];
+    prepare(&c);
+    int iters = 0;
+    update(&c, ctl, &iters);
+    Profile f = {&c, ctl, column, 0.0, 0.0, include_penalty, 0};
+    /* the first refit: setBeta through updateXBeta, then the dirty state is rebuilt from beta */
+    const double delta = 0.0 - c.beta[column];
+    c.beta[column] += delta;
+    update_xbeta(&c, column, delta);
+    prepare(&c);
+    c.fixb[column] = 1;
+    update(&c, ctl, &iters);
+    c.fixb[column] = 0;
+    for (int i = 0; i < n; ++i) values[i] = profile_objective(&f, points[i]);
+    ctx_free(&c);
+    return 0;
+}
+
 int ccd_oracle_profile(const ccd_problem* p, const ccd_control* ctl, const double* start, const int* cols, int n,
                        double threshold, int include_penalty, int override_no_regularization, double* lower,
                        double* upper, int* evaluations, ccd_result* fit) {

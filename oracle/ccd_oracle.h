@@ -18,6 +18,8 @@ int ccd_oracle_probe(const ccd_problem* p, const double* beta, double* gradient,
 int ccd_oracle_profile(const ccd_problem* p, const ccd_control* c, const double* start_beta, const int* columns,
                        int n, double threshold, int include_penalty, int override_no_regularization,
                        double* lower, double* upper, int* evaluations, ccd_result* fit);
+int ccd_oracle_profile_points(const ccd_problem* p, const ccd_control* c, const double* start_beta, int column,
+                              const double* points, int n, int include_penalty, double* values);
 int ccd_oracle_predictive_loglik(const ccd_problem* p, const double* beta, const double* held_out,
                                  double* out);
 #endif

@@ -125,7 +125,9 @@ class _Lib:
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
             sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
                                P(Result), C.c_int]
+            sigs["profile_points"] = [P(Problem), P(Control), V, C.c_int, V, C.c_int, C.c_int, V, C.c_int]
         else:
+            sigs["profile_points"] = [P(Problem), P(Control), V, C.c_int, V, C.c_int, C.c_int, V]
             sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
                                P(Result)]
         for name, args in sigs.items():
@@ -194,6 +196,23 @@ class _Lib:
         if getattr(self.lib, self.prefix + "profile")(*args):
             raise RuntimeError(self.err())
         return lo, up, ev, Fit(beta, r.log_likelihood, r.log_prior, r.iterations, r.return_flag)
+
+    def profile_points(self, data, column, points, prior_type=1, variance=1.0, include_penalty=True,
+                       control: Optional[Control] = None, exclude=None, weights=None, start=None, device=0):
+        """CcdInterface::evaluateProfileModel with one thread: the profile log
+        likelihood (+ log prior) of `column` at each of `points`."""
+        p, keep = make_problem(data, prior_type, variance, exclude, weights)
+        c = control or make_control()
+        pts = np.ascontiguousarray(points, np.float64)
+        vals = np.zeros(pts.size)
+        s = None if start is None else np.ascontiguousarray(start, np.float64)
+        args = [C.byref(p), C.byref(c), _ptr(s), int(column), _ptr(pts), int(pts.size), int(include_penalty),
+                _ptr(vals)]
+        if self.prefix == "ref_":
+            args.append(int(device))
+        if getattr(self.lib, self.prefix + "profile_points")(*args):
+            raise RuntimeError(self.err())
+        return vals
 
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)

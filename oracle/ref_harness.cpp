@@ -18,6 +18,8 @@
 //   * CV fold masks     CrossValidationSelector  src/cyclops/drivers/CrossValidationSelector.cpp:21-116
 //   * engine probes     AbstractModelSpecifics virtuals, called directly on the
 //                       same engine object the CCD uses.
+//   * profile points    CcdInterface::evaluateProfileModel with one thread
+//                       src/cyclops/CcdInterface.cpp:527-618
 //   * profile bounds    CcdInterface::profileModel with one thread
 //                       src/cyclops/CcdInterface.cpp:262-420: the reference's
 //                       own RZeroIn (src/utils/RZeroIn.h, header-only) over
@@ -382,6 +384,31 @@ int ref_profile(const ref_problem* p, const ref_control* c, const double* start_
                 count += eval.nEvals;
             }
             evaluations[i] = count;
+        }
+    });
+}
+
+int ref_profile_points(const ref_problem* p, const ref_control* c, const double* start_beta, int column,
+                       const double* points, int n, int include_penalty, double* values, int device) {
+    return guarded([&] {
+        auto inst = build(p, device);
+        if (start_beta) {
+            std::vector<double> b(start_beta, start_beta + p->J);
+            inst->ccd->setBeta(b);
+        }
+        const ModeFindingArguments args = toArguments(c);
+        CyclicCoordinateDescent& ccd = *inst->ccd;
+        ccd.update(args);
+        for (int j = 0; j < p->J; ++j) ccd.getBeta(j);    // x0s (CcdInterface.cpp:555-559)
+        // evaluateProfileModel with one thread (CcdInterface.cpp:527-618)
+        ccd.makeDirty();
+        {
+            ProfileObjective eval{ccd, args, column, 0.0, 0.0, include_penalty != 0};
+            eval.objective(0.0);
+        }
+        for (int i = 0; i < n; ++i) {
+            ProfileObjective eval{ccd, args, column, 0.0, 0.0, include_penalty != 0};
+            values[i] = eval.objective(points[i]);
         }
     });
 }

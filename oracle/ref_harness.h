@@ -105,4 +105,10 @@ void ref_ingest_free(ref_ingest_output* out);
 int ref_profile(const ref_problem* p, const ref_control* c, const double* start_beta, const int* columns, int n,
                 double threshold, int include_penalty, int override_no_regularization, double* lower,
                 double* upper, int* evaluations, ref_result* fit, int device);
+/* The profile log likelihood (plus log prior when include_penalty) at
+ * `points` for one column (CcdInterface::evaluateProfileModel, src/cyclops/
+ * CcdInterface.cpp:527-618, one thread): fit, makeDirty, one refit at 0,
+ * then one refit per point, each warm-started from the last. */
+int ref_profile_points(const ref_problem* p, const ref_control* c, const double* start_beta, int column,
+                       const double* points, int n, int include_penalty, double* values, int device);
 #endif

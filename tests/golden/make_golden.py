@@ -187,8 +187,10 @@ PROFILE_CASES = [("lr_flat", [0, 1, 2, 3], False, True, 0),
 def save_profile():
     """Profile-likelihood bounds (CcdInterface::profileModel with one thread,
     src/cyclops/CcdInterface.cpp:262-420) at the 95 % threshold
-    qchisq(0.95, 1) / 2: profile_<case>.npz holds the problem, the columns
-    and the reference's lower / upper bounds and refit counts."""
+    qchisq(0.95, 1) / 2, and the profile log likelihood at 9 points around
+    the estimate of the last column (evaluateProfileModel, :527-618):
+    profile_<case>.npz holds the problem, the columns, the reference's lower /
+    upper bounds and refit counts, the points and their values."""
     all_cases = cases()
     threshold = 1.920729410347062          # qchisq(0.95, df = 1) / 2
     for name, cols, override, penalty, swindle in PROFILE_CASES:
@@ -199,6 +201,10 @@ def save_profile():
         w = spec.get("weights")
         lo, up, ev, fit = O.ref().profile(d, cols, spec["prior"], spec["variance"], threshold, penalty, override,
                                           control=ctl, weights=w)
+        # getCyclopsProfileLogLikelihood (evaluateProfileModel) on the last column
+        points = fit.beta[cols[-1]] + np.linspace(-0.6, 0.6, 9)
+        values = O.ref().profile_points(d, cols[-1], points, spec["prior"], spec["variance"], penalty,
+                                        control=ctl, weights=w)
         arrays = dict(
             model=d.model, y=d.y, col_format=d.col_format, col_ptr=d.col_ptr, col_idx=d.col_idx,
             val_ptr=d.val_ptr, col_val=d.col_val,
@@ -210,6 +216,7 @@ def save_profile():
             tolerance=ctl.tolerance, convergence=ctl.convergence_type, swindle=swindle,
             columns=np.asarray(cols, np.int32), threshold=threshold, include_penalty=int(penalty),
             override=int(override), lower=lo, upper=up, evaluations=ev, beta=fit.beta,
+            point_column=int(cols[-1]), points=points, point_values=values,
         )
         np.savez_compressed(os.path.join(HERE, "profile_" + name + ".npz"), **arrays)
         print(f"profile_{name:20s} cols={cols} evals={ev.tolist()}")

@@ -120,3 +120,16 @@ def test_port_profile_rejects_regularized_column():
     data, s = load_golden("profile_lr_normal_weighted")
     with pytest.raises(RuntimeError, match="regularized"):
         O.port().profile(data, [3], int(s["prior"]), float(s["variance"]), override_no_regularization=False)
+
+
+@pytest.mark.parametrize("name", profile_names())
+def test_port_profile_points_match_reference_fixture(name):
+    """evaluateProfileModel (CcdInterface.cpp:527-618, one thread)."""
+    data, s = load_golden(name)
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                         use_kkt_swindle=int(s["swindle"]))
+    vals = O.port().profile_points(data, int(s["point_column"]), s["points"], int(s["prior"]),
+                                   float(s["variance"]), bool(s["include_penalty"]), control=ctl,
+                                   weights=s["weights"])
+    np.testing.assert_allclose(vals, s["point_values"], rtol=1e-13)
+    assert np.argmax(vals) in (3, 4, 5)            # the points straddle the estimate

@@ -1,0 +1,110 @@
+"""The KKT swindle on the GPU (cyc_fit with use_kkt_swindle: active-set
+passes with the inactive columns' |gradient| scored in one launch) against
+the reference's CyclicCoordinateDescent::kktSwindle
+(src/cyclops/CyclicCoordinateDescent.cpp:636-814): the swindle_* fixtures
+the reference made, the restatement oracle at a tight tolerance, and the
+reference's own swindle driving the CUDA engine through the adapter."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, exclude_for, load_golden, rel_err, swindle_names
+from cyclops_b200 import data as D
+
+pytestmark = pytest.mark.gpu
+
+ADAPTER = os.path.join(ROOT, "oracle", "_ref", "libcyclops_ref_cuda.so")
+
+
+def _gpu_fit(data, s, swindle=True, tolerance=None, convergence=None, max_iterations=1000, start=None):
+    from cyclops_b200 import api
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    ctl = api.create_control(tolerance=float(s["tolerance"]) if tolerance is None else tolerance,
+                             convergence_type=int(s["convergence"]) if convergence is None else convergence,
+                             max_iterations=max_iterations, use_kkt_swindle=swindle)
+    return api.fit_cyclops_model(data, prior, ctl, weights=s["weights"], starting_coefficients=start)
+
+
+@pytest.mark.parametrize("name", swindle_names())
+def test_swindle_matches_reference_fixture(cuda_lib, name):
+    """Same prior, tolerance and convergence rule as the reference's swindle
+    run: flag, iterations of the last findMode, zero pattern, coefficients."""
+    data, s = load_golden(name)
+    fit = _gpu_fit(data, s)
+    assert fit.return_flag == int(s["return_flag"])
+    assert abs(fit.iterations - int(s["iterations"])) <= 1
+    ref = s["beta"]
+    np.testing.assert_array_equal(fit.beta != 0, ref != 0)
+    err = np.abs(fit.beta - ref) / np.maximum(np.abs(ref), 1.0)
+    assert err.max() < 1e-4, err.max()
+    assert rel_err(fit.log_likelihood, float(s["log_likelihood"])) < 1e-6
+
+
+@pytest.mark.parametrize("name", ["swindle_lr_c1", "swindle_pr_laplace_weighted", "swindle_clr_laplace",
+                                  "swindle_cox_strata"])
+def test_swindle_tight_contract(cuda_lib, name):
+    """Both sides converged tightly (tolerance 1e-12): identical active-set
+    decisions and iterations, beta 1e-6 relative, log likelihood 1e-9."""
+    from oracle import oracle as O
+    data, s = load_golden(name)
+    ctl = O.make_control(tolerance=1e-12, convergence_type=D.CONV_MITTAL, max_iterations=5000, use_kkt_swindle=1)
+    ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
+    fit = _gpu_fit(data, s, tolerance=1e-12, convergence=D.CONV_MITTAL, max_iterations=5000)
+    assert fit.iterations == ref.iterations
+    assert fit.return_flag == ref.return_flag
+    np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
+    ok = np.abs(fit.beta - ref.beta) <= 1e-6 * np.abs(ref.beta) + 1e-9
+    assert ok.all(), np.max(np.abs(fit.beta - ref.beta) / (np.abs(ref.beta) + 1e-3))
+    assert rel_err(fit.log_likelihood, ref.log_likelihood) < 1e-9
+
+
+def test_swindle_warm_start_and_pass_limit(cuda_lib):
+    """A nonzero start on inactive columns is zeroed first (setBeta through
+    updateXBeta); max_iterations also caps the passes (MAX_ITERATIONS)."""
+    from oracle import oracle as O
+    data, s = load_golden("swindle_lr_laplace_small")
+    start = np.where(np.arange(data.J) % 3 == 0, 0.05, 0.0)
+    for max_it in (1000, 2):
+        ctl = O.make_control(tolerance=1e-8, max_iterations=max_it, use_kkt_swindle=1)
+        ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, start=start)
+        fit = _gpu_fit(data, s, tolerance=1e-8, max_iterations=max_it, start=start)
+        assert fit.return_flag == ref.return_flag
+        assert fit.iterations == ref.iterations
+        np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
+        np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
+
+
+def test_swindle_rejected_by_batched_solvers(cuda_lib):
+    from cyclops_b200 import api, _native
+    data, s = load_golden("lr_laplace_small")
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    ctl = api.create_control(use_kkt_swindle=True)
+    with pytest.raises(_native.CyclopsError) as ei:
+        api.batch_fit(data, prior, [float(s["variance"])] * 2, control=ctl)
+    assert ei.value.status == 4
+
+
+@pytest.mark.skipif(not os.path.exists(ADAPTER), reason="adapter harness not built (needs the reference sources)")
+@pytest.mark.parametrize("name", ["swindle_lr_laplace_small", "swindle_clr_laplace", "swindle_cox_laplace"])
+def test_reference_swindle_drives_cuda_engine(cuda_lib, name):
+    """The reference's own kktSwindle, unchanged, on the CUDA engine through
+    CudaModelSpecifics: same result as the reference on its CPU engine."""
+    from oracle import oracle as O
+    data, s = load_golden(name)
+    lib = C.CDLL(ADAPTER)
+    lib.ref_fit_device.argtypes = [C.POINTER(O.Problem), C.POINTER(O.Control), C.c_void_p,
+                                   C.POINTER(O.Result), C.c_int]
+    lib.ref_last_error.restype = C.c_char_p
+    p, keep = O.make_problem(data, int(s["prior"]), float(s["variance"]), None, s["weights"])
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]), use_kkt_swindle=1)
+    beta = np.zeros(data.J)
+    r = O.Result(beta=beta.ctypes.data)
+    assert lib.ref_fit_device(C.byref(p), C.byref(ctl), None, C.byref(r), 1) == 0, lib.ref_last_error()
+    assert r.return_flag == int(s["return_flag"])
+    assert abs(r.iterations - int(s["iterations"])) <= 1
+    ref = s["beta"]
+    np.testing.assert_array_equal(beta != 0, ref != 0)
+    err = np.abs(beta - ref) / np.maximum(np.abs(ref), 1.0)
+    assert err.max() < 1e-4, err.max()
