@@ -106,6 +106,8 @@ _SIGS = {
                           C.POINTER(FitResult)],
     "cyc_profile_log_likelihood": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_void_p],
+    "cyc_profile_log_likelihood_batch": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control),
+                                         C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p],
     "cyc_profile_bounds": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_void_p,
                            C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                            C.POINTER(FitResult)],

@@ -334,10 +334,15 @@ def profile_bounds(data, columns: Sequence[int], prior: Optional[PriorSpec] = No
 
 def profile_log_likelihood(data, column: int, points: Sequence[float], prior: Optional[PriorSpec] = None,
                            control: Optional[ControlSpec] = None, include_penalty: bool = True, weights=None,
-                           starting_coefficients=None, device: int = 0) -> np.ndarray:
+                           starting_coefficients=None, device: int = 0, batched: bool = False) -> np.ndarray:
     """getCyclopsProfileLogLikelihood (R/ModelFit.R:816-826) through
     CcdInterface::evaluateProfileModel with one thread: fit on the GPU,
-    then the profile log likelihood of `column` at each point."""
+    then the profile log likelihood of `column` at each point.
+
+    ``batched=True`` refits all points together in the persistent batch
+    kernel, each from the mode (``starting_coefficients``, or fitted first
+    when None); values then agree with the one-thread order to the
+    convergence tolerance."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     prior = prior or create_prior("none")
     control = control or create_control()
@@ -348,8 +353,9 @@ def profile_log_likelihood(data, column: int, points: Sequence[float], prior: Op
     pts = np.ascontiguousarray(points, np.float64)
     vals = np.zeros(pts.size)
     c = _control_struct(control)
-    N.check(N.lib().cyc_profile_log_likelihood(ds.handle, C.byref(p), C.byref(spec), C.byref(c), int(column),
-                                               _ptr(pts), int(pts.size), int(include_penalty), _ptr(vals)))
+    fn = N.lib().cyc_profile_log_likelihood_batch if batched else N.lib().cyc_profile_log_likelihood
+    N.check(fn(ds.handle, C.byref(p), C.byref(spec), C.byref(c), int(column), _ptr(pts), int(pts.size),
+               int(include_penalty), _ptr(vals)))
     return vals
 
 

@@ -1728,7 +1728,7 @@ struct BatchRunner {
     }
 
     void setup(const cyc_prior& prior, const cyc_fit_spec* specs, const std::vector<double>& h_beta,
-               const std::vector<double>& h_hdelta) {
+               const std::vector<double>& h_hdelta, int fixed_col = -1) {
         const int K = ds.K, J = ds.J;
         d_rpart.alloc(C + 1);
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_rpart.get(), rpart.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -1738,6 +1738,7 @@ struct BatchRunner {
         CYC_CHECK_LAUNCH();
         std::vector<int> fixb(J, 0), pt(J, prior.prior_type), act(Fp, 0);
         if (ds.has_offset) fixb[0] = 1;
+        if (fixed_col >= 0) fixb[fixed_col] = 1;
         for (int i = 0; i < prior.n_exclude; ++i) pt[prior.exclude[i]] = CYC_PRIOR_NONE;
         for (int f = 0; f < F; ++f) act[f] = 1;
         std::vector<double> var(Fp, 1.0);
@@ -1746,13 +1747,14 @@ struct BatchRunner {
         {
             const RunPlan* plan = nullptr;
             for (auto& pl : ds.run_plans)
-                if (pl.C == C && pl.G == G) plan = &pl;
+                if (pl.C == C && pl.G == G && pl.fixed == fixed_col) plan = &pl;
             if (!plan) {
                 const bool rows8 = (G == 8) && model_independent(ds.model);
                 RunPlan pl = plan_runs(ds, rpart, fixb, rows8 ? kBatchCap : (32 / G) * kRunItems,
                                        model_independent(ds.model), rows8 ? kDirtyMax : 0);
                 pl.C = C;
                 pl.G = G;
+                pl.fixed = fixed_col;
                 ds.run_plans.push_back(std::move(pl));
                 plan = &ds.run_plans.back();
             }
@@ -1932,7 +1934,7 @@ namespace {
 // select the CV-grid weights; otherwise `specs[f].weights`.
 void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F, const cyc_control* ctl,
                cyc_fit_result* out, const int* d_fold, int n_folds, const std::vector<int>* fit_fold,
-               std::vector<double>* pll) {
+               std::vector<double>* pll, int fixed_col = -1) {
     CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
                 "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
     CYC_REQUIRE(!ctl->use_kkt_swindle, CYC_ERR_UNSUPPORTED, "the KKT swindle is offered by cyc_fit only");
@@ -2005,7 +2007,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
         BatchRunner<float> r32(ds, stream, F, G);
         if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
-        r32.setup(*prior, specs, beta, hd);
+        r32.setup(*prior, specs, beta, hd, fixed_col);
         float ms = 0.f;
         r32.run(*ctl, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
         r32.results(beta, hd, iters, flags, ctr);
@@ -2015,7 +2017,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     }
     BatchRunner<double> r64(ds, stream, F, G);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
-    r64.setup(*prior, specs, beta, hd);
+    r64.setup(*prior, specs, beta, hd, fixed_col);
     float ms = 0.f;
     r64.run(*ctl, ctl->tolerance, &ms);
     std::vector<int> it64;
@@ -2091,5 +2093,47 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
                 }
                 grid_mean[v] = tot / cnt;
             }
+    });
+}
+
+// getCyclopsProfileLogLikelihood as one batched solve: every point is a fit
+// of the persistent kernel, started from the mode with the column moved to
+// the point and held there (the column joins the offset as a fixed column),
+// so all points refit together instead of one after another.  Each fit
+// starts from the mode, as evaluateProfileModel's per-thread clones do
+// (CcdInterface.cpp:545-598); the one-thread, warm-start-chained order is
+// cyc_profile_log_likelihood.
+extern "C" int cyc_profile_log_likelihood_batch(cyc_dataset* dsh, const cyc_prior* prior, const cyc_fit_spec* spec,
+                                                const cyc_control* ctl, int column, const double* points, int n,
+                                                int include_penalty, double* values) {
+    return guarded([&] {
+        CYC_REQUIRE(dsh && prior && spec && ctl && n >= 0 && (n == 0 || (points && values)), CYC_ERR_ARGUMENT,
+                    "null argument");
+        Dataset& ds = dsh->ds;
+        const int J = ds.J;
+        CYC_REQUIRE(column >= 0 && column < J && !(ds.has_offset && column == 0), CYC_ERR_ARGUMENT,
+                    "profile column out of range (or the offset)");
+        if (n == 0) return;
+        std::vector<double> mode(J, 0.0);
+        if (spec->start_beta) {
+            std::copy(spec->start_beta, spec->start_beta + J, mode.begin());
+        } else {                                          // fit the mode first
+            cyc_fit_result r{};
+            r.beta = mode.data();
+            cyc_fit_spec s0 = *spec;
+            run_batch(ds, prior, &s0, 1, ctl, &r, nullptr, 0, nullptr, nullptr);
+        }
+        std::vector<double> starts((size_t)n * J), outb((size_t)n * J);
+        std::vector<cyc_fit_spec> specs(n, *spec);
+        std::vector<cyc_fit_result> out(n);
+        for (int i = 0; i < n; ++i) {
+            std::copy(mode.begin(), mode.end(), starts.begin() + (size_t)i * J);
+            starts[(size_t)i * J + column] = points[i];
+            specs[i].start_beta = starts.data() + (size_t)i * J;
+            out[i].beta = outb.data() + (size_t)i * J;
+        }
+        run_batch(ds, prior, specs.data(), n, ctl, out.data(), nullptr, 0, nullptr, nullptr, column);
+        for (int i = 0; i < n; ++i)
+            values[i] = out[i].log_likelihood + (include_penalty ? out[i].log_prior : 0.0);
     });
 }

@@ -172,9 +172,16 @@ void Engine::regroup(const double* w) {
     sync();
 }
 
-// setWeights (ModelSpecifics.hpp:427-484)
+// setWeights (ModelSpecifics.hpp:427-484).  As in the reference, the
+// statistics (exb, denominators) stay usable: lr / pr / clr / cpr
+// denominators do not depend on the weights, and cox, whose risk-set groups
+// are rebuilt here, gets its weighted denominators recomputed from the
+// unchanged xbeta when they were current before.  (The reference's CCD calls
+// setWeights again at the start of findMode while it holds its statistics
+// current, e.g. inside kktSwindle.)
 void Engine::set_weights(const double* w, bool use_cv) {
     const int K = ds->K;
+    const bool had_stats = stats_known;
     use_w = use_cv && w != nullptr;
     const double* wp = use_w ? w : nullptr;
     if (model_cumulative(model)) regroup(wp);
@@ -193,7 +200,10 @@ void Engine::set_weights(const double* w, bool use_cv) {
         launch(k_nw_grouped, grid_for(N, 1), kThreads, 0, stream, N, group_rows(), ds->d_y.get(), kw.get(), nw.get());
     }
     CYC_CHECK_LAUNCH();
-    stats_known = false;
+    if (model_cumulative(model)) {
+        if (had_stats) remaining_statistics(true);
+        else stats_known = false;
+    }
 }
 
 void Engine::fixed_terms_ll(bool use_cv) {

@@ -254,6 +254,16 @@ int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prior, const cy
                                const cyc_control* control, int column, const double* points, int n,
                                int include_penalty, double* values);
 
+/* The same values as one batched solve (lr, pr, clr, cpr): every point is a
+ * fit of the persistent batch kernel with `column` held at the point, all
+ * started from the mode (spec->start_beta, or fitted first when NULL), as
+ * evaluateProfileModel's per-thread clones start from it
+ * (CcdInterface.cpp:545-598).  Values agree with the one-thread order to
+ * the fits' convergence tolerance. */
+int cyc_profile_log_likelihood_batch(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
+                                     const cyc_control* control, int column, const double* points, int n,
+                                     int include_penalty, double* values);
+
 /* Cross-validation fold masks, `n_reps * folds` rows of K weights (0 = held
  * out), exactly as CrossValidationSelector draws them
  * (src/cyclops/drivers/CrossValidationSelector.cpp:21-116): by row

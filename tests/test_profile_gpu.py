@@ -77,3 +77,24 @@ def test_profile_points_match_reference_fixture(cuda_lib, name):
     vals = api.profile_log_likelihood(data, int(s["point_column"]), s["points"], prior, ctl,
                                       include_penalty=bool(s["include_penalty"]), weights=s["weights"])
     np.testing.assert_allclose(vals, s["point_values"], rtol=1e-9)
+
+
+@pytest.mark.parametrize("name", ["profile_lr_normal_weighted", "profile_clr_normal_weighted",
+                                  "profile_pr_offset_normal", "profile_lr_flat"])
+def test_profile_points_batched_match_oracle(cuda_lib, name):
+    """All points refit together in the batch kernel (column held fixed,
+    each from the mode), against the oracle's one-thread chain, both
+    converged tightly (Mittal 1e-11): the values agree to 1e-9 relative."""
+    from cyclops_b200 import api
+    from oracle import oracle as O
+    data, s = load_golden(name)
+    col = int(s["point_column"])
+    pts = s["points"]
+    octl = O.make_control(tolerance=1e-11, convergence_type=D.CONV_MITTAL, max_iterations=5000)
+    want = O.port().profile_points(data, col, pts, int(s["prior"]), float(s["variance"]),
+                                   bool(s["include_penalty"]), control=octl, weights=s["weights"])
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    ctl = api.create_control(tolerance=1e-11, convergence_type=D.CONV_MITTAL, max_iterations=5000)
+    got = api.profile_log_likelihood(data, col, pts, prior, ctl, include_penalty=bool(s["include_penalty"]),
+                                     weights=s["weights"], batched=True)
+    np.testing.assert_allclose(got, want, rtol=1e-9)
