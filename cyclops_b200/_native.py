@@ -58,7 +58,8 @@ class RunStats(C.Structure):
                 ("gradient_entries", C.c_double), ("update_entries", C.c_double),
                 ("coordinate_steps", C.c_double), ("index_entries", C.c_double), ("cycles", C.c_double),
                 ("launches", C.c_int), ("phases", C.c_int), ("phase_ms", C.c_double * 2),
-                ("phase_bytes", C.c_double * 2), ("phase_state_bytes", C.c_int * 2)]
+                ("phase_bytes", C.c_double * 2), ("phase_state_bytes", C.c_int * 2),
+                ("cluster_ctas", C.c_int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)

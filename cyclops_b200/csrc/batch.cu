@@ -27,7 +27,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "engine.cuh"
@@ -1674,6 +1677,13 @@ static void launch_model(const BatchArgs& a, int ngroups, cudaStream_t stream) {
 
 // One batched solve at precision T over fits [0, F) with starting
 // coefficients `h_beta` (F x J, updated in place) and trust regions.
+// CTAs per cluster when nothing is tuned: one per 16k rows, at most 8;
+// CYC_BATCH_CLUSTER (1..8) forces a size
+static int default_cluster(int K) {
+    if (const char* e = std::getenv("CYC_BATCH_CLUSTER")) return std::max(1, std::min(kMaxC, std::atoi(e)));
+    return std::max(1, std::min(kMaxC, (K + 16383) / 16384));
+}
+
 template <class T>
 struct BatchRunner {
     Dataset& ds;
@@ -1687,12 +1697,11 @@ struct BatchRunner {
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
 
-    BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_) : ds(d), stream(s), F(F_), G(G_) {
+    BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_, int C_ = 0) : ds(d), stream(s), F(F_), G(G_) {
         ngroups = (F + G - 1) / G;
         Fp = ngroups * G;
         const int K = ds.K;
-        C = std::max(1, std::min(kMaxC, (K + 16383) / 16384));
-        if (const char* e = std::getenv("CYC_BATCH_CLUSTER")) C = std::max(1, std::min(kMaxC, std::atoi(e)));
+        C = C_ > 0 ? std::min(kMaxC, C_) : default_cluster(K);
         // row partition, aligned to strata for grouped models
         rpart.assign(C + 1, K);
         for (int r = 0; r < C; ++r) {
@@ -1929,6 +1938,75 @@ using namespace cyc;
 
 namespace {
 
+// ---- cluster-size tuner ------------------------------------------------------
+// How many CTAs share a group's rows trades per-step work (fewer rows per
+// CTA) against cluster barrier cost and against how many clusters are
+// resident at once (G fits per cluster, F / G clusters).  A solve large
+// enough to amortise it (16 fits or more, 1e8 fit-entries or more per cycle)
+// times one cycle of the real problem at the default size and at its halves
+// (8, 4, 2 CTAs for large K) and keeps the fastest; the choice is cached for
+// the process per problem shape, so repeated solves of one shape (a CV grid
+// per step, a dataset uploaded again) probe once.  CYC_BATCH_CLUSTER skips
+// the tuner.
+struct TuneKey {
+    int model, K, J, F, G, precision, folds, fixed;
+    long long nnz;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(model, K, J, F, G, precision, folds, fixed, nnz) <
+               std::tie(o.model, o.K, o.J, o.F, o.G, o.precision, o.folds, o.fixed, o.nnz);
+    }
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, int>& tuned_sizes() {
+    static auto* m = new std::map<TuneKey, int>();   // lives to process exit
+    return *m;
+}
+
+template <class T>
+float probe_cycle(Dataset& ds, cudaStream_t stream, int F, int G, int C, const cyc_prior& prior,
+                  const cyc_fit_spec* specs, const std::vector<double>& beta, const std::vector<double>& hd,
+                  const int* d_fold, int n_folds, const std::vector<int>* fit_fold, const cyc_control& ctl,
+                  int fixed_col) {
+    BatchRunner<T> r(ds, stream, F, G, C);
+    if (d_fold) r.set_folds(d_fold, n_folds, *fit_fold);
+    r.setup(prior, specs, beta, hd, fixed_col);
+    cyc_control one = ctl;
+    one.max_iterations = 1;
+    float ms = 0.f;
+    r.run(one, ctl.tolerance, &ms);
+    return ms;
+}
+
+int tuned_cluster(Dataset& ds, cudaStream_t stream, int F, int G, const cyc_prior& prior, const cyc_fit_spec* specs,
+                  const std::vector<double>& beta, const std::vector<double>& hd, const int* d_fold, int n_folds,
+                  const std::vector<int>* fit_fold, const cyc_control& ctl, int fixed_col) {
+    const int base = default_cluster(ds.K);
+    const double work = (double)F * (double)(ds.nnz_idx + ds.nnz_val);
+    if (std::getenv("CYC_BATCH_CLUSTER") || base <= 1 || F < 16 || work < 1e8) return base;
+    const TuneKey key{ds.model, ds.K, ds.J, F, G, ctl.precision, d_fold ? n_folds : 0, fixed_col, ds.nnz_idx};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = tuned_sizes().find(key);
+        if (it != tuned_sizes().end()) return it->second;
+    }
+    int best = base;
+    float best_ms = 0.f;
+    for (int c = base; c >= 1 && c >= base / 4; c /= 2) {
+        const float ms = ctl.precision == CYC_MIXED
+                             ? probe_cycle<float>(ds, stream, F, G, c, prior, specs, beta, hd, d_fold, n_folds,
+                                                  fit_fold, ctl, fixed_col)
+                             : probe_cycle<double>(ds, stream, F, G, c, prior, specs, beta, hd, d_fold, n_folds,
+                                                   fit_fold, ctl, fixed_col);
+        if (c == base || ms < best_ms) {
+            best = c;
+            best_ms = ms;
+        }
+    }
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    tuned_sizes()[key] = best;
+    return best;
+}
+
 // The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` (fold id
 // per row, `n_folds` of them) and `fit_fold` (the held-out fold of each fit)
 // select the CV-grid weights; otherwise `specs[f].weights`.
@@ -2002,10 +2080,11 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         st.launches += 1;
         st.phases = phase + 1;
     };
+    const int C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_col);
     int phase = 0;
     if (ctl->precision == CYC_MIXED) {
         // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
-        BatchRunner<float> r32(ds, stream, F, G);
+        BatchRunner<float> r32(ds, stream, F, G, C);
         if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
         r32.setup(*prior, specs, beta, hd, fixed_col);
         float ms = 0.f;
@@ -2015,7 +2094,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         // the FP64 phase restarts the trust regions (resetBounds, :943)
         std::fill(hd.begin(), hd.end(), ctl->initial_bound);
     }
-    BatchRunner<double> r64(ds, stream, F, G);
+    BatchRunner<double> r64(ds, stream, F, G, C);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
     r64.setup(*prior, specs, beta, hd, fixed_col);
     float ms = 0.f;
@@ -2037,6 +2116,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         out[f].log_prior = lp;
     }
     if (pll) pll->assign(p.begin(), p.begin() + F);
+    st.cluster_ctas = C;
     set_last_stats(st);
 }
 

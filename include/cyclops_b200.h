@@ -287,6 +287,8 @@ typedef struct {
     double phase_ms[2];
     double phase_bytes[2];
     int phase_state_bytes[2];   /* bytes per (row, fit) state element of each phase */
+    int cluster_ctas;           /* batched solves: CTAs per thread-block cluster (the
+                                   tuner's choice, or CYC_BATCH_CLUSTER); 0 otherwise */
 } cyc_run_stats;
 int cyc_last_run_stats(cyc_run_stats* out);
 
