@@ -1814,12 +1814,18 @@ struct BatchRunner {
         if (ds.has_offset) for (int f = F; f < Fp; ++f) b[(size_t)f * J] = 1.0;
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_beta.get(), b.data(), b.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_hdelta.get(), hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice, stream));
-        // linear predictors
-        ds.ensure_csr();
+        // linear predictors: zero when every coefficient is zero (a cold
+        // start without an offset), else sum_j beta_j x_kj over the row-major copy
         d_xb.alloc((size_t)ngroups * K * G);
-        launch(k_init_xb<T>, grid_for((long long)K * Fp, 1), 256, 0, stream, K, G, Fp, ds.d_row_ptr.get(), ds.d_row_col.get(),
-                                                                         ds.d_row_val.get(), d_beta.get(), J, d_xb.get());
-        CYC_CHECK_LAUNCH();
+        const bool all_zero = std::all_of(b.begin(), b.end(), [](double v) { return v == 0.0; });
+        if (all_zero) {
+            CYC_CHECK_CUDA(cudaMemsetAsync(d_xb.get(), 0, (size_t)ngroups * K * G * sizeof(T), stream));
+        } else {
+            ds.ensure_csr();
+            launch(k_init_xb<T>, grid_for((long long)K * Fp, 1), 256, 0, stream, K, G, Fp, ds.d_row_ptr.get(),
+                   ds.d_row_col.get(), ds.d_row_val.get(), d_beta.get(), J, d_xb.get());
+            CYC_CHECK_LAUNCH();
+        }
         // fixed gradient terms
         d_xjy.alloc((size_t)Fp * J);
         if (d_fold) {
