@@ -46,3 +46,37 @@ def test_errors_are_status_codes_not_exceptions(cuda_lib):
     assert rc == 1
     assert b"null" in cuda_lib.cyc_last_error()
     assert cuda_lib.cyc_engine_set_weights(None, None, 0) == 1
+
+
+# C struct of the header -> its ctypes mirror in cyclops_b200/_native.py
+_MIRRORS = {"cyc_data_desc": "DataDesc", "cyc_control": "Control", "cyc_prior": "Prior",
+            "cyc_fit_spec": "FitSpec", "cyc_fit_result": "FitResult", "cyc_run_stats": "RunStats"}
+
+
+def test_struct_mirrors_match_the_header(tmp_path):
+    """Size and field offsets of every ABI struct, as a C compiler lays them
+    out from include/cyclops_b200.h, equal the ctypes mirrors' (a field
+    appended to a struct must be appended to its mirror too)."""
+    import shutil
+    import subprocess
+    from cyclops_b200 import _native as N
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "cyclops_b200.h"', "int main(void) {"]
+    for cname, pyname in _MIRRORS.items():
+        st = getattr(N, pyname)
+        lines.append(f'printf("{pyname} size %zu\\n", sizeof({cname}));')
+        for field, _ in st._fields_:
+            lines.append(f'printf("{pyname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    for line in filter(None, out):
+        pyname, field, value = line.split()
+        st = getattr(N, pyname)
+        want = ctypes.sizeof(st) if field == "size" else getattr(st, field).offset
+        assert int(value) == want, (pyname, field, int(value), want)
