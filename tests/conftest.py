@@ -22,7 +22,14 @@ def golden_names():
     """The plain fit fixtures (not the CV folds, ingest tables or swindle fits)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
                   if not p.endswith("cv_folds.npz")
-                  and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_")))
+                  and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_", "small_")))
+
+
+def small_names():
+    """Tiny designs from the reference's own tests (test-smallCox.R,
+    test-smallBernoulli.R, test-smallPoisson.R) with the reference's fits and
+    an independent Newton MLE."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "small_*.npz")))
 
 
 def profile_names():

@@ -14,6 +14,7 @@ CrossValidationSelector.
 from __future__ import annotations
 
 import os
+import re
 import sys
 
 import numpy as np
@@ -222,6 +223,129 @@ def save_profile():
         print(f"profile_{name:20s} cols={cols} evals={ev.tolist()}")
 
 
+REF_TESTS = os.path.join(os.environ.get("CYCLOPS_REFERENCE", "/root/reference"), "tests", "testthat")
+
+
+def _r_vector(text, name):
+    """The numbers of `name <- c(...)` or `name = c(...)` (first occurrence)."""
+    m = re.search(name + r"\s*(?:<-|=)\s*c\(([^)]*)\)", text)
+    if not m:
+        raise RuntimeError(f"{name} not found in the reference test")
+    return np.array([float(v) for v in m.group(1).split(",")])
+
+
+def _r_gl(text, name):
+    """R's gl(n, k, length) factor levels (1-based) for `name = gl(...)`."""
+    m = re.search(name + r"\s*(?:<-|=)\s*gl\((\d+)\s*,\s*(\d+)(?:\s*,\s*(\d+))?\)", text)
+    n, k = int(m.group(1)), int(m.group(2))
+    length = int(m.group(3)) if m.group(3) else n * k
+    return np.resize(np.repeat(np.arange(1, n + 1), k), length)
+
+
+def _r_tables(text):
+    """Every read.table(..., text = "...") block: header + numeric rows."""
+    out = []
+    for block in re.findall(r'text\s*=\s*"([^"]*)"', text):
+        lines = [l.strip() for l in block.strip().splitlines() if l.strip()]
+        cols = [c.strip() for c in lines[0].split(",")]
+        rows = np.array([[float(v) for v in l.split(",")] for l in lines[1:]])
+        out.append({c: rows[:, i] for i, c in enumerate(cols)})
+    return out
+
+
+def small_designs():
+    """The tiny designs of the reference's own tests, read from its test files
+    (tests/testthat/test-smallCox.R, test-smallBernoulli.R,
+    test-smallPoisson.R), in the formats those tests use."""
+    from cyclops_b200 import ingest
+    out = {}
+    cox = _r_tables(open(os.path.join(REF_TESTS, "test-smallCox.R")).read())
+
+    def cox_data(t, strata, weights=None, x1=None):
+        n = len(t["length"])
+        rid = np.arange(1, n + 1, dtype=np.int64)
+        outcomes = {"rowId": rid, "y": t["event"], "time": t["length"],
+                    "stratumId": (t["x2"] if strata else np.zeros(n)).astype(np.int64)}
+        if weights is not None:
+            outcomes["weights"] = weights
+        x1v = t["x1"] if x1 is None else x1
+        cid = [np.full(n, 1)] + ([] if strata else [np.full(n, 2)])
+        vals = [x1v] + ([] if strata else [t["x2"]])
+        cov = {"rowId": np.concatenate([rid] * len(cid)), "covariateId": np.concatenate(cid).astype(np.int64),
+               "covariateValue": np.concatenate(vals)}
+        return ingest.convert_to_cyclops_data(outcomes, cov, model_type="cox")
+
+    out["small_cox_noties"] = cox_data(cox[0], False)
+    out["small_cox_noties_strata"] = cox_data(cox[0], True)
+    out["small_cox_timeties"] = cox_data(cox[1], False)
+    out["small_cox_failties"] = cox_data(cox[2], False)
+    out["small_cox_failties_risk"] = cox_data(cox[3], False)
+    out["small_cox_failties_strata"] = cox_data(cox[3], True)
+    # each row twice, the first copy weighted 0 and two of those given other
+    # x1 values: the fit equals small_cox_failties_strata (zero weight = removal)
+    t = {k: np.repeat(v, 2) for k, v in cox[3].items()}
+    x1 = t["x1"].copy()
+    x1[0], x1[4] = 5.0, 6.0
+    out["small_cox_zero_weights"] = cox_data(t, True, weights=np.tile([0.0, 1.0], len(cox[3]["x1"])), x1=x1)
+
+    bern = open(os.path.join(REF_TESTS, "test-smallBernoulli.R")).read()
+    bid, nn, yy = (_r_vector(bern, v) for v in ("binomial_bid", "binomial_n", "binomial_y"))
+    log_bid = np.log(np.concatenate([np.repeat(bid, (nn - yy).astype(int)), np.repeat(bid, yy.astype(int))]))
+    y = np.concatenate([np.zeros(int(np.sum(nn - yy))), np.ones(int(np.sum(yy)))])
+    K = y.size
+    out["small_lr_dense"] = (D.ColumnBuilder(K).intercept().dense(log_bid).build(D.LR, y, has_intercept=True), None)
+    nz = np.flatnonzero(log_bid != 0)
+    out["small_lr_sparse"] = (D.ColumnBuilder(K).intercept().sparse(nz, log_bid[nz])
+                              .build(D.LR, y, has_intercept=True), None)
+
+    pois = open(os.path.join(REF_TESTS, "test-smallPoisson.R")).read()
+    counts = _r_vector(pois, "counts")
+    outcome, treatment = _r_gl(pois, "outcome"), _r_gl(pois, "treatment")
+    K = counts.size
+    dummies = [(outcome == 2), (outcome == 3), (treatment == 2), (treatment == 3)]
+    b = D.ColumnBuilder(K).intercept()
+    for dmy in dummies:
+        b.dense(dmy.astype(float))
+    out["small_pr_dense"] = (b.build(D.PR, counts, has_intercept=True), None)
+    b = D.ColumnBuilder(K).intercept().dense(dummies[0].astype(float)).dense(dummies[1].astype(float))
+    for dmy in dummies[2:]:
+        b.indicator(np.flatnonzero(dmy))
+    out["small_pr_indicator"] = (b.build(D.PR, counts, has_intercept=True), None)
+    return out
+
+
+def save_small():
+    """small_<design>.npz: a design from the reference's own tests, the
+    reference engine's unpenalised fit of it at the default control and at a
+    tight one (Mittal 1e-17: until the log likelihood stops changing in
+    double precision), and an independent Newton-Raphson MLE
+    (oracle/newton.py) of the same likelihood."""
+    from oracle import newton
+    for name, (d, w) in small_designs().items():
+        ex = [1 if d.has_offset else 0] if d.has_intercept else []
+        fit = O.ref().fit(d, D.PRIOR_NONE, 1.0, control=O.make_control(), exclude=ex, weights=w)
+        tight = O.ref().fit(d, D.PRIOR_NONE, 1.0, exclude=ex, weights=w,
+                            control=O.make_control(tolerance=1e-17, convergence_type=D.CONV_MITTAL,
+                                                   max_iterations=100000))
+        nb, nll = newton.newton_fit(d, w)
+        arrays = dict(
+            model=d.model, y=d.y, col_format=d.col_format, col_ptr=d.col_ptr, col_idx=d.col_idx,
+            val_ptr=d.val_ptr, col_val=d.col_val,
+            pid=d.pid if d.pid is not None else np.zeros(0, np.int32),
+            time=d.time if d.time is not None else np.zeros(0),
+            has_offset=int(d.has_offset), has_intercept=int(d.has_intercept),
+            prior=D.PRIOR_NONE, variance=1.0, weights=w if w is not None else np.zeros(0),
+            tolerance=1e-6, convergence=D.CONV_GRADIENT,
+            beta=fit.beta, log_likelihood=fit.log_likelihood, log_prior=fit.log_prior,
+            iterations=fit.iterations, return_flag=fit.return_flag,
+            tight_beta=tight.beta, tight_log_likelihood=tight.log_likelihood, tight_iterations=tight.iterations,
+            newton_beta=nb, newton_log_likelihood=nll,
+        )
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrays)
+        print(f"{name:26s} K={d.K:4d} J={d.J} it={fit.iterations:3d} tight_it={tight.iterations:4d} "
+              f"|tight-newton|={np.max(np.abs(tight.beta - nb)):.2e}")
+
+
 def main(parts):
     if not O.have_ref():
         O.build()
@@ -236,8 +360,10 @@ def main(parts):
         save_swindle()
     if "profile" in parts:
         save_profile()
+    if "small" in parts:
+        save_small()
 
 
 if __name__ == "__main__":
-    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile]   (default: all)
-    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile"])
+    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile] [small]   (default: all)
+    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile", "small"])

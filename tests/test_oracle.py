@@ -3,7 +3,7 @@ engine (tests/golden/make_golden.py).  No GPU."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, profile_names, rel_err, swindle_names
+from conftest import golden_names, load_golden, profile_names, rel_err, small_names, swindle_names
 from cyclops_b200 import data as D
 from oracle import oracle as O
 
@@ -133,3 +133,42 @@ def test_port_profile_points_match_reference_fixture(name):
                                    weights=s["weights"])
     np.testing.assert_allclose(vals, s["point_values"], rtol=1e-13)
     assert np.argmax(vals) in (3, 4, 5)            # the points straddle the estimate
+
+
+@pytest.mark.parametrize("name", small_names())
+def test_newton_mle_agrees_with_reference_on_small_designs(name):
+    """The second, independent check: a NumPy Newton-Raphson MLE of the same
+    likelihood (oracle/newton.py) lands where the reference engine's CCD
+    does when run until its log likelihood stops changing."""
+    from oracle import newton
+    data, s = load_golden(name)
+    nb, nll = newton.newton_fit(data, s["weights"])
+    np.testing.assert_allclose(nb, s["newton_beta"], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(s["tight_beta"], nb, rtol=2e-6, atol=2e-6)
+    assert abs(float(s["tight_log_likelihood"]) - nll) <= 1e-11 * abs(nll)
+
+
+@pytest.mark.parametrize("name", small_names())
+def test_port_matches_reference_on_small_designs(name):
+    data, s = load_golden(name)
+    ex = [1 if data.has_offset else 0] if data.has_intercept else []
+    fit = O.port().fit(data, D.PRIOR_NONE, 1.0, control=O.make_control(), exclude=ex, weights=s["weights"])
+    assert (fit.iterations, fit.return_flag) == (int(s["iterations"]), int(s["return_flag"]))
+    np.testing.assert_allclose(fit.beta, s["beta"], rtol=1e-12, atol=1e-14)
+    tight = O.port().fit(data, D.PRIOR_NONE, 1.0, exclude=ex, weights=s["weights"],
+                         control=O.make_control(tolerance=1e-17, convergence_type=D.CONV_MITTAL,
+                                                max_iterations=100000))
+    assert tight.iterations == int(s["tight_iterations"])
+    np.testing.assert_allclose(tight.beta, s["tight_beta"], rtol=1e-12, atol=1e-14)
+
+
+def test_small_design_properties():
+    """The reference's own invariances on its small designs: zero weight is
+    removal (test-smallCox.R), and dense, sparse and indicator columns give
+    the same fit (test-smallBernoulli.R, test-smallPoisson.R)."""
+    for a, b in [("small_cox_zero_weights", "small_cox_failties_strata"), ("small_lr_dense", "small_lr_sparse"),
+                 ("small_pr_dense", "small_pr_indicator")]:
+        _, sa = load_golden(a)
+        _, sb = load_golden(b)
+        np.testing.assert_allclose(sa["tight_beta"], sb["tight_beta"], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(sa["newton_beta"], sb["newton_beta"], rtol=1e-9, atol=1e-12)
