@@ -256,7 +256,8 @@ def _r_tables(text):
 def small_designs():
     """The tiny designs of the reference's own tests, read from its test files
     (tests/testthat/test-smallCox.R, test-smallBernoulli.R,
-    test-smallPoisson.R), in the formats those tests use."""
+    test-smallPoisson.R) and its text fixture inst/extdata/infert_ccd.txt, in
+    the formats those tests use."""
     from cyclops_b200 import ingest
     out = {}
     cox = _r_tables(open(os.path.join(REF_TESTS, "test-smallCox.R")).read())
@@ -297,6 +298,26 @@ def small_designs():
     nz = np.flatnonzero(log_bid != 0)
     out["small_lr_sparse"] = (D.ColumnBuilder(K).intercept().sparse(nz, log_bid[nz])
                               .build(D.LR, y, has_intercept=True), None)
+
+    # the reference's CCD text fixture of the infert matched case-control
+    # data (inst/extdata/infert_ccd.txt: stratum, case, covariate:value ...),
+    # conditional logistic as test-smallCLR.R fits it
+    rows, cids, vals, strata, ys = [], [], [], [], []
+    path = os.path.join(os.path.dirname(os.path.dirname(REF_TESTS)), "inst", "extdata", "infert_ccd.txt")
+    for i, line in enumerate(l for l in open(path) if l.strip() and not l.startswith("#")):
+        f = line.split()
+        strata.append(int(f[0]))
+        ys.append(float(f[1]))
+        for item in f[2:]:
+            c, v = item.split(":")
+            rows.append(i + 1)
+            cids.append(int(c))
+            vals.append(float(v))
+    n = len(ys)
+    out["small_clr_infert"] = ingest.convert_to_cyclops_data(
+        {"rowId": np.arange(1, n + 1, dtype=np.int64), "y": np.asarray(ys), "stratumId": np.asarray(strata, np.int64)},
+        {"rowId": np.asarray(rows, np.int64), "covariateId": np.asarray(cids, np.int64),
+         "covariateValue": np.asarray(vals)}, model_type="clr")
 
     pois = open(os.path.join(REF_TESTS, "test-smallPoisson.R")).read()
     counts = _r_vector(pois, "counts")
