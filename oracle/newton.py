@@ -73,19 +73,24 @@ def _loglik_grad_hess(model, X, y, w, beta, offset, time, strata):
     return ll, g, H
 
 
-def newton_fit(data, weights: Optional[np.ndarray] = None, tol: float = 1e-13, max_iter: int = 200):
+def newton_fit(data, weights: Optional[np.ndarray] = None, tol: float = 1e-13, max_iter: int = 200,
+               fixed: Optional[dict] = None):
     """The unpenalised MLE of `data` by Newton steps with step halving.
     Returns (beta, log_likelihood) in the data's column order; the offset
-    column (when present) is held at 1 as the reference holds it."""
+    column (when present) is held at 1 as the reference holds it, and the
+    columns of `fixed` ({column: value}) at their values (a profile point)."""
     X = dense_design(data)
     K, J = X.shape
     y = np.asarray(data.y, np.float64)
     w = np.ones(K) if weights is None else np.asarray(weights, np.float64)
     free = np.ones(J, bool)
     offset = np.zeros(K)
+    held = dict(fixed or {})
     if data.has_offset:
-        free[0] = False
-        offset = X[:, 0].copy()
+        held[0] = 1.0
+    for j, v in held.items():
+        free[j] = False
+        offset = offset + v * X[:, j]
     Xf = X[:, free]
     time = np.zeros(K) if data.time is None else np.asarray(data.time, np.float64)
     if data.model in (CLR, CPR):
@@ -111,6 +116,6 @@ def newton_fit(data, weights: Optional[np.ndarray] = None, tol: float = 1e-13, m
             break
     beta = np.zeros(J)
     beta[free] = b
-    if data.has_offset:
-        beta[0] = 1.0
+    for j, v in held.items():
+        beta[j] = v
     return beta, ll

@@ -172,3 +172,25 @@ def test_small_design_properties():
         _, sb = load_golden(b)
         np.testing.assert_allclose(sa["tight_beta"], sb["tight_beta"], rtol=1e-9, atol=1e-12)
         np.testing.assert_allclose(sa["newton_beta"], sb["newton_beta"], rtol=1e-9, atol=1e-12)
+
+
+@pytest.mark.parametrize("name,cols", [("small_pr_dense", [0, 1, 3]), ("small_lr_dense", [0, 1]),
+                                       ("small_cox_failties_risk", [0, 1]), ("small_clr_infert", [0, 1])])
+def test_profile_bounds_agree_with_newton_profile(name, cols):
+    """The profile search (bracket + Brent at tolerance 1e-3, restated from
+    profileModel) against roots of the Newton profile log likelihood found
+    to 1e-12: within the search's 1e-3 tolerance, as R's confint is."""
+    from scipy.optimize import brentq
+    from oracle import newton
+    data, s = load_golden(name)
+    thr = 1.920729410347062
+    ctl = O.make_control(tolerance=1e-10, convergence_type=D.CONV_MITTAL, max_iterations=100000)
+    lo, up, ev, fit = O.port().profile(data, cols, D.PRIOR_NONE, 1.0, thr, False, True, control=ctl,
+                                       weights=s["weights"])
+    nb, nll = newton.newton_fit(data, s["weights"])
+    with np.errstate(over="ignore", invalid="ignore"):
+        for i, j in enumerate(cols):
+            f = lambda x: newton.newton_fit(data, s["weights"], fixed={j: x})[1] - (nll - thr)
+            ru = brentq(f, nb[j], up[i] + 0.5 * (up[i] - nb[j]), xtol=1e-12)
+            rl = brentq(f, lo[i] - 0.5 * (nb[j] - lo[i]), nb[j], xtol=1e-12)
+            assert abs(up[i] - ru) < 1e-3 and abs(lo[i] - rl) < 1e-3, (j, up[i] - ru, lo[i] - rl)
