@@ -2086,10 +2086,15 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         st.launches += 1;
         st.phases = phase + 1;
     };
-    const int C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_col);
+    int C;
+    {
+        NvtxRange range("cyclops batch: cluster tuner");
+        C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_col);
+    }
     int phase = 0;
     if (ctl->precision == CYC_MIXED) {
         // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
+        NvtxRange range("cyclops batch: fp32 phase");
         BatchRunner<float> r32(ds, stream, F, G, C);
         if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
         r32.setup(*prior, specs, beta, hd, fixed_col);
@@ -2100,6 +2105,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         // the FP64 phase restarts the trust regions (resetBounds, :943)
         std::fill(hd.begin(), hd.end(), ctl->initial_bound);
     }
+    NvtxRange range64("cyclops batch: fp64 phase");
     BatchRunner<double> r64(ds, stream, F, G, C);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
     r64.setup(*prior, specs, beta, hd, fixed_col);
@@ -2131,6 +2137,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
 extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
                              const cyc_control* ctl, cyc_fit_result* out) {
     return guarded([&] {
+        NvtxRange range("cyc_batch_fit");
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
         run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, 0, nullptr, nullptr);
     });
@@ -2140,6 +2147,7 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
                                const double* variances, int n_var, const cyc_control* ctl, cyc_fit_result* out,
                                double* pred_loglik, double* grid_mean) {
     return guarded([&] {
+        NvtxRange range("cyc_cv_grid_fit");
         CYC_REQUIRE(dsh && prior && fold_of_row && variances && ctl && out && n_folds > 1 && n_var > 0,
                     CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(n_folds <= 127, CYC_ERR_ARGUMENT, "at most 127 folds");
@@ -2193,6 +2201,7 @@ extern "C" int cyc_profile_log_likelihood_batch(cyc_dataset* dsh, const cyc_prio
                                                 const cyc_control* ctl, int column, const double* points, int n,
                                                 int include_penalty, double* values) {
     return guarded([&] {
+        NvtxRange range("cyc_profile_log_likelihood_batch");
         CYC_REQUIRE(dsh && prior && spec && ctl && n >= 0 && (n == 0 || (points && values)), CYC_ERR_ARGUMENT,
                     "null argument");
         Dataset& ds = dsh->ds;

@@ -17,6 +17,7 @@
 // reference's column-by-column axpy order.
 #include "internal.cuh"
 
+#include <cmath>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -143,12 +144,26 @@ extern "C" long long cyc_launch_count(void) { return g_launches.load(); }
 
 extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_dataset** out) {
     return guarded([&] {
+        NvtxRange range("cyc_dataset_create");
         CYC_REQUIRE(d && out, CYC_ERR_ARGUMENT, "null argument");
         *out = nullptr;
         CYC_REQUIRE(d->K > 0 && d->J > 0, CYC_ERR_ARGUMENT, "K and J must be positive");
         CYC_REQUIRE(d->model >= CYC_LR && d->model <= CYC_COX, CYC_ERR_ARGUMENT, "Invalid model type.");
         CYC_REQUIRE(d->y && d->col_format && d->col_ptr && d->val_ptr, CYC_ERR_ARGUMENT, "missing arrays");
         CYC_REQUIRE(d->model != CYC_COX || d->time, CYC_ERR_ARGUMENT, "cox needs survival times");
+        // a NaN or an infinity among the outcomes, times or covariate values
+        // leaves every fit undefined (the reference engine runs into it with
+        // no defined result), so such data is refused before any device work
+        auto finite = [](const double* a, long long n) {
+            for (long long i = 0; i < n; ++i)
+                if (!std::isfinite(a[i])) return false;
+            return true;
+        };
+        CYC_REQUIRE(finite(d->y, d->K), CYC_ERR_ARGUMENT, "non-finite outcome (y)");
+        CYC_REQUIRE(!d->time || finite(d->time, d->K), CYC_ERR_ARGUMENT, "non-finite time");
+        CYC_REQUIRE(d->val_ptr[d->J] >= 0, CYC_ERR_ARGUMENT, "offsets must not decrease");
+        CYC_REQUIRE(!d->col_val || finite(d->col_val, d->val_ptr[d->J]), CYC_ERR_ARGUMENT,
+                    "non-finite covariate value");
         int ndev = 0;
         CYC_CHECK_CUDA(cudaGetDeviceCount(&ndev));
         CYC_REQUIRE(device >= 0 && device < ndev, CYC_ERR_ARGUMENT, "no such CUDA device");

@@ -644,6 +644,7 @@ using namespace cyc;
 extern "C" int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
                        const cyc_control* control, cyc_fit_result* out) {
     return guarded([&] {
+        NvtxRange range("cyc_fit");
         CYC_REQUIRE(ds && prior && spec && control && out && out->beta, CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
                     CYC_ERR_ARGUMENT, "Unknown prior type");
@@ -663,6 +664,7 @@ extern "C" int cyc_profile_bounds(cyc_dataset* ds, const cyc_prior* prior, const
                                   int include_penalty, int override_no_regularization, double* lower,
                                   double* upper, int* evaluations, cyc_fit_result* fit) {
     return guarded([&] {
+        NvtxRange range("cyc_profile_bounds");
         CYC_REQUIRE(ds && prior && spec && control && n >= 0, CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(n == 0 || (columns && lower && upper && evaluations), CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(!fit || fit->beta, CYC_ERR_ARGUMENT, "null result buffer");
@@ -690,6 +692,7 @@ extern "C" int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prio
                                           const cyc_control* control, int column, const double* points, int n,
                                           int include_penalty, double* values) {
     return guarded([&] {
+        NvtxRange range("cyc_profile_log_likelihood");
         CYC_REQUIRE(ds && prior && spec && control && n >= 0 && (n == 0 || (points && values)), CYC_ERR_ARGUMENT,
                     "null argument");
         CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
@@ -711,6 +714,7 @@ extern "C" int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prio
 extern "C" int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
                                  const cyc_control* control, cyc_fit_result* out) {
     return guarded([&] {
+        NvtxRange range("cyc_fit_host_loop");
         CYC_REQUIRE(ds && prior && spec && control && out && out->beta, CYC_ERR_ARGUMENT, "null argument");
         CYC_REQUIRE(prior->prior_type >= CYC_PRIOR_NONE && prior->prior_type <= CYC_PRIOR_NORMAL,
                     CYC_ERR_ARGUMENT, "Unknown prior type");

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <cstdio>
 #include <string>
@@ -97,6 +98,16 @@ struct StreamScope {
     ~StreamScope() { alloc_stream() = prev; }
     StreamScope(const StreamScope&) = delete;
     StreamScope& operator=(const StreamScope&) = delete;
+};
+
+// a named NVTX range for the object's lifetime: profilers (nsys, ncu --nvtx)
+// see the library's entry points and solver phases by name; with no tool
+// attached the calls return at once
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
 };
 
 // a stream owned by an object; declared first among the owner's members so

@@ -48,6 +48,29 @@ def test_errors_are_status_codes_not_exceptions(cuda_lib):
     assert cuda_lib.cyc_engine_set_weights(None, None, 0) == 1
 
 
+@pytest.mark.parametrize("where", ["y", "time", "col_val"])
+@pytest.mark.parametrize("bad", [float("nan"), float("inf")])
+def test_non_finite_data_is_refused_before_device_work(cuda_lib, where, bad):
+    """A NaN or infinity in the outcomes, times or covariate values is an
+    argument error from cyc_dataset_create (no GPU needed to see it)."""
+    import numpy as np
+    from cyclops_b200 import _native as N
+    K = 6
+    arr = {"y": np.array([0, 1, 0, 1, 1, 0], float), "time": np.arange(1.0, K + 1),
+           "col_val": np.array([0.5, -1.0, 2.0]), "fmt": np.array([3, 1], np.int32),
+           "cp": np.array([0, 0, 3], np.int64), "ci": np.array([0, 2, 5], np.int32),
+           "vp": np.array([0, 0, 3], np.int64)}
+    arr[where] = arr[where].copy()
+    arr[where][1] = bad
+    d = N.DataDesc(model=4, K=K, J=2, pid=None, y=arr["y"].ctypes.data, time=arr["time"].ctypes.data,
+                   col_format=arr["fmt"].ctypes.data, col_ptr=arr["cp"].ctypes.data,
+                   col_idx=arr["ci"].ctypes.data, val_ptr=arr["vp"].ctypes.data,
+                   col_val=arr["col_val"].ctypes.data, has_offset=0, has_intercept=1)
+    h = ctypes.c_void_p()
+    assert cuda_lib.cyc_dataset_create(ctypes.byref(d), 0, ctypes.byref(h)) == 1
+    assert b"non-finite" in cuda_lib.cyc_last_error()
+
+
 # C struct of the header -> its ctypes mirror in cyclops_b200/_native.py
 _MIRRORS = {"cyc_data_desc": "DataDesc", "cyc_control": "Control", "cyc_prior": "Prior",
             "cyc_fit_spec": "FitSpec", "cyc_fit_result": "FitResult", "cyc_run_stats": "RunStats"}
