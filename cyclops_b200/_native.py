@@ -45,7 +45,8 @@ class Prior(C.Structure):
 
 
 class FitSpec(C.Structure):
-    _fields_ = [("weights", C.c_void_p), ("variance", C.c_double), ("start_beta", C.c_void_p)]
+    _fields_ = [("weights", C.c_void_p), ("variance", C.c_double), ("start_beta", C.c_void_p),
+                ("fixed", C.c_void_p), ("n_fixed", C.c_int)]
 
 
 class FitResult(C.Structure):

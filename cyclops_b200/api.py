@@ -263,21 +263,40 @@ def _prior_struct(data: CyclopsData, prior: PriorSpec):
                    n_exclude=int(ex.size)), ex
 
 
+def _fixed_columns(fixed, J: int) -> Optional[np.ndarray]:
+    """fixedCoefficients as column ids: a boolean mask of length J or a list
+    of ids (None: nothing fixed)."""
+    if fixed is None:
+        return None
+    a = np.asarray(fixed)
+    if a.dtype == bool:
+        if a.size != J:
+            raise ValueError("fixed_coefficients mask must have one entry per column")
+        a = np.flatnonzero(a)
+    a = np.ascontiguousarray(a, np.int32)
+    return a if a.size else None
+
+
 def fit_cyclops_model(data, prior: Optional[PriorSpec] = None, control: Optional[ControlSpec] = None,
                       weights=None, starting_coefficients=None, device: int = 0,
-                      host_loop: bool = False) -> FitResult:
+                      host_loop: bool = False, fixed_coefficients=None) -> FitResult:
     """fitCyclopsModel (R/ModelFit.R:65): one fit, CCD loop on the GPU.
 
-    ``host_loop=True`` runs the plain FP64 single-fit GPU CCD instead: the
-    host drives the engine coordinate by coordinate, reading (gradient,
-    Hessian) back each time, as the reference's CyclicCoordinateDescent does."""
+    ``fixed_coefficients`` (a boolean mask over the columns, or column ids)
+    holds those coefficients at their starting values, as the reference's
+    fixedCoefficients does.  ``host_loop=True`` runs the plain FP64
+    single-fit GPU CCD instead: the host drives the engine coordinate by
+    coordinate, reading (gradient, Hessian) back each time, as the
+    reference's CyclicCoordinateDescent does."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     prior = prior or create_prior("none")
     control = control or create_control()
     p, keep_ex = _prior_struct(ds.data, prior)
     w = None if weights is None else np.ascontiguousarray(weights, np.float64)
     s = None if starting_coefficients is None else np.ascontiguousarray(starting_coefficients, np.float64)
-    spec = N.FitSpec(weights=_ptr(w), variance=prior.variance, start_beta=_ptr(s))
+    fx = _fixed_columns(fixed_coefficients, ds.data.J)
+    spec = N.FitSpec(weights=_ptr(w), variance=prior.variance, start_beta=_ptr(s), fixed=_ptr(fx),
+                     n_fixed=0 if fx is None else int(fx.size))
     beta = np.zeros(ds.data.J)
     out = N.FitResult(beta=beta.ctypes.data)
     c = _control_struct(control)
@@ -390,13 +409,17 @@ def launch_count() -> int:
 
 
 def batch_fit(data, prior: PriorSpec, variances: Sequence[float], weights: Optional[Sequence] = None,
-              control: Optional[ControlSpec] = None, starts=None, device: int = 0) -> List[FitResult]:
+              control: Optional[ControlSpec] = None, starts=None, device: int = 0,
+              fixed_coefficients=None) -> List[FitResult]:
     """F fits sharing one dataset, advanced together on the GPU.  `weights` is
-    a list of K-vectors (or None entries) or a (F, K) array."""
+    a list of K-vectors (or None entries) or a (F, K) array;
+    `fixed_coefficients` (mask or ids) holds the same columns fixed in every
+    fit, at each fit's starting values."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     control = control or create_control()
     F = len(variances)
     p, keep_ex = _prior_struct(ds.data, prior)
+    fx = _fixed_columns(fixed_coefficients, ds.data.J)
     specs = (N.FitSpec * F)()
     results = (N.FitResult * F)()
     keep = []
@@ -410,7 +433,8 @@ def batch_fit(data, prior: PriorSpec, variances: Sequence[float], weights: Optio
         if starts is not None and starts[f] is not None:
             s = np.ascontiguousarray(starts[f], np.float64)
             keep.append(s)
-        specs[f] = N.FitSpec(weights=_ptr(w), variance=float(variances[f]), start_beta=_ptr(s))
+        specs[f] = N.FitSpec(weights=_ptr(w), variance=float(variances[f]), start_beta=_ptr(s), fixed=_ptr(fx),
+                             n_fixed=0 if fx is None else int(fx.size))
         results[f] = N.FitResult(beta=betas[f].ctypes.data)
     c = _control_struct(control)
     N.check(N.lib().cyc_batch_fit(ds.handle, C.byref(p), specs, F, C.byref(c), results))

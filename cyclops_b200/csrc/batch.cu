@@ -1737,7 +1737,7 @@ struct BatchRunner {
     }
 
     void setup(const cyc_prior& prior, const cyc_fit_spec* specs, const std::vector<double>& h_beta,
-               const std::vector<double>& h_hdelta, int fixed_col = -1) {
+               const std::vector<double>& h_hdelta, const std::vector<int>& fixed_cols) {
         const int K = ds.K, J = ds.J;
         d_rpart.alloc(C + 1);
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_rpart.get(), rpart.data(), (C + 1) * sizeof(int), cudaMemcpyHostToDevice, stream));
@@ -1747,7 +1747,7 @@ struct BatchRunner {
         CYC_CHECK_LAUNCH();
         std::vector<int> fixb(J, 0), pt(J, prior.prior_type), act(Fp, 0);
         if (ds.has_offset) fixb[0] = 1;
-        if (fixed_col >= 0) fixb[fixed_col] = 1;
+        for (int j : fixed_cols) fixb[j] = 1;
         for (int i = 0; i < prior.n_exclude; ++i) pt[prior.exclude[i]] = CYC_PRIOR_NONE;
         for (int f = 0; f < F; ++f) act[f] = 1;
         std::vector<double> var(Fp, 1.0);
@@ -1756,14 +1756,14 @@ struct BatchRunner {
         {
             const RunPlan* plan = nullptr;
             for (auto& pl : ds.run_plans)
-                if (pl.C == C && pl.G == G && pl.fixed == fixed_col) plan = &pl;
+                if (pl.C == C && pl.G == G && pl.fixed == fixed_cols) plan = &pl;
             if (!plan) {
                 const bool rows8 = (G == 8) && model_independent(ds.model);
                 RunPlan pl = plan_runs(ds, rpart, fixb, rows8 ? kBatchCap : (32 / G) * kRunItems,
                                        model_independent(ds.model), rows8 ? kDirtyMax : 0);
                 pl.C = C;
                 pl.G = G;
-                pl.fixed = fixed_col;
+                pl.fixed = fixed_cols;
                 ds.run_plans.push_back(std::move(pl));
                 plan = &ds.run_plans.back();
             }
@@ -1955,7 +1955,8 @@ namespace {
 // per step, a dataset uploaded again) probe once.  CYC_BATCH_CLUSTER skips
 // the tuner.
 struct TuneKey {
-    int model, K, J, F, G, precision, folds, fixed;
+    int model, K, J, F, G, precision, folds;
+    std::vector<int> fixed;
     long long nnz;
     bool operator<(const TuneKey& o) const {
         return std::tie(model, K, J, F, G, precision, folds, fixed, nnz) <
@@ -1972,10 +1973,10 @@ template <class T>
 float probe_cycle(Dataset& ds, cudaStream_t stream, int F, int G, int C, const cyc_prior& prior,
                   const cyc_fit_spec* specs, const std::vector<double>& beta, const std::vector<double>& hd,
                   const int* d_fold, int n_folds, const std::vector<int>* fit_fold, const cyc_control& ctl,
-                  int fixed_col) {
+                  const std::vector<int>& fixed_cols) {
     BatchRunner<T> r(ds, stream, F, G, C);
     if (d_fold) r.set_folds(d_fold, n_folds, *fit_fold);
-    r.setup(prior, specs, beta, hd, fixed_col);
+    r.setup(prior, specs, beta, hd, fixed_cols);
     cyc_control one = ctl;
     one.max_iterations = 1;
     float ms = 0.f;
@@ -1985,11 +1986,11 @@ float probe_cycle(Dataset& ds, cudaStream_t stream, int F, int G, int C, const c
 
 int tuned_cluster(Dataset& ds, cudaStream_t stream, int F, int G, const cyc_prior& prior, const cyc_fit_spec* specs,
                   const std::vector<double>& beta, const std::vector<double>& hd, const int* d_fold, int n_folds,
-                  const std::vector<int>* fit_fold, const cyc_control& ctl, int fixed_col) {
+                  const std::vector<int>* fit_fold, const cyc_control& ctl, const std::vector<int>& fixed_cols) {
     const int base = default_cluster(ds.K);
     const double work = (double)F * (double)(ds.nnz_idx + ds.nnz_val);
     if (std::getenv("CYC_BATCH_CLUSTER") || base <= 1 || F < 16 || work < 1e8) return base;
-    const TuneKey key{ds.model, ds.K, ds.J, F, G, ctl.precision, d_fold ? n_folds : 0, fixed_col, ds.nnz_idx};
+    const TuneKey key{ds.model, ds.K, ds.J, F, G, ctl.precision, d_fold ? n_folds : 0, fixed_cols, ds.nnz_idx};
     {
         std::lock_guard<std::mutex> lk(g_tune_mutex);
         auto it = tuned_sizes().find(key);
@@ -2000,9 +2001,9 @@ int tuned_cluster(Dataset& ds, cudaStream_t stream, int F, int G, const cyc_prio
     for (int c = base; c >= 1 && c >= base / 4; c /= 2) {
         const float ms = ctl.precision == CYC_MIXED
                              ? probe_cycle<float>(ds, stream, F, G, c, prior, specs, beta, hd, d_fold, n_folds,
-                                                  fit_fold, ctl, fixed_col)
+                                                  fit_fold, ctl, fixed_cols)
                              : probe_cycle<double>(ds, stream, F, G, c, prior, specs, beta, hd, d_fold, n_folds,
-                                                   fit_fold, ctl, fixed_col);
+                                                   fit_fold, ctl, fixed_cols);
         if (c == base || ms < best_ms) {
             best = c;
             best_ms = ms;
@@ -2031,9 +2032,25 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         CYC_REQUIRE(prior->exclude[i] >= 0 && prior->exclude[i] < ds.J, CYC_ERR_ARGUMENT, "exclude index out of range");
     for (int f = 0; f < F; ++f) {
         CYC_REQUIRE(out[f].beta, CYC_ERR_ARGUMENT, "null result buffer");
+        CYC_REQUIRE(specs[f].n_fixed >= 0 && (specs[f].n_fixed == 0 || specs[f].fixed), CYC_ERR_ARGUMENT,
+                    "bad fixed-column list");
         CYC_REQUIRE(prior->prior_type == CYC_PRIOR_NONE || specs[f].variance > 0, CYC_ERR_ARGUMENT,
                     "prior variance must be positive");
     }
+    // columns held fixed (besides the offset): the fits' shared fixed set and
+    // the profiled column
+    std::vector<int> fixed_cols(specs[0].fixed, specs[0].fixed + (specs[0].fixed ? specs[0].n_fixed : 0));
+    for (int j : fixed_cols) CYC_REQUIRE(j >= 0 && j < ds.J, CYC_ERR_ARGUMENT, "fixed column out of range");
+    std::sort(fixed_cols.begin(), fixed_cols.end());
+    for (int f = 1; f < F; ++f) {
+        std::vector<int> o(specs[f].fixed, specs[f].fixed + (specs[f].fixed ? specs[f].n_fixed : 0));
+        std::sort(o.begin(), o.end());
+        CYC_REQUIRE(o == fixed_cols, CYC_ERR_UNSUPPORTED, "the fits of one batched solve share their fixed columns");
+    }
+    if (fixed_col >= 0) fixed_cols.push_back(fixed_col);
+    std::sort(fixed_cols.begin(), fixed_cols.end());
+    fixed_cols.erase(std::unique(fixed_cols.begin(), fixed_cols.end()), fixed_cols.end());
+    if (ds.has_offset) fixed_cols.erase(std::remove(fixed_cols.begin(), fixed_cols.end(), 0), fixed_cols.end());
     CYC_CHECK_CUDA(cudaSetDevice(ds.device));
     cudaStream_t stream;
     CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
@@ -2089,7 +2106,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     int C;
     {
         NvtxRange range("cyclops batch: cluster tuner");
-        C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_col);
+        C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_cols);
     }
     int phase = 0;
     if (ctl->precision == CYC_MIXED) {
@@ -2097,7 +2114,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         NvtxRange range("cyclops batch: fp32 phase");
         BatchRunner<float> r32(ds, stream, F, G, C);
         if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
-        r32.setup(*prior, specs, beta, hd, fixed_col);
+        r32.setup(*prior, specs, beta, hd, fixed_cols);
         float ms = 0.f;
         r32.run(*ctl, std::max(ctl->polish_tolerance, ctl->tolerance), &ms);
         r32.results(beta, hd, iters, flags, ctr);
@@ -2108,7 +2125,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     NvtxRange range64("cyclops batch: fp64 phase");
     BatchRunner<double> r64(ds, stream, F, G, C);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
-    r64.setup(*prior, specs, beta, hd, fixed_col);
+    r64.setup(*prior, specs, beta, hd, fixed_cols);
     float ms = 0.f;
     r64.run(*ctl, ctl->tolerance, &ms);
     std::vector<int> it64;

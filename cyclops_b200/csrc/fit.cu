@@ -109,6 +109,11 @@ struct FitRunner {
         h_start.assign(J, 0.0);
         if (spec.start_beta) std::copy(spec.start_beta, spec.start_beta + J, h_start.begin());
         if (e.ds->has_offset) { fixb[0] = 1; h_start[0] = 1.0; }   // CCD init :218-221
+        CYC_REQUIRE(spec.n_fixed >= 0 && (spec.n_fixed == 0 || spec.fixed), CYC_ERR_ARGUMENT, "bad fixed-column list");
+        for (int i = 0; i < spec.n_fixed; ++i) {                 // setFixedBeta (fixedCoefficients)
+            CYC_REQUIRE(spec.fixed[i] >= 0 && spec.fixed[i] < J, CYC_ERR_ARGUMENT, "fixed column out of range");
+            fixb[spec.fixed[i]] = 1;
+        }
         base_fix = fixb;
         pt.assign(J, prior.prior_type);
         for (int i = 0; i < prior.n_exclude; ++i) {
@@ -551,6 +556,11 @@ static void host_loop_fit(Engine& e, const cyc_prior& prior, const cyc_fit_spec&
     std::vector<double> beta(J, 0.0);
     if (spec.start_beta) std::copy(spec.start_beta, spec.start_beta + J, beta.begin());
     if (e.ds->has_offset) { fixb[0] = 1; beta[0] = 1.0; }
+    CYC_REQUIRE(spec.n_fixed >= 0 && (spec.n_fixed == 0 || spec.fixed), CYC_ERR_ARGUMENT, "bad fixed-column list");
+    for (int i = 0; i < spec.n_fixed; ++i) {
+        CYC_REQUIRE(spec.fixed[i] >= 0 && spec.fixed[i] < J, CYC_ERR_ARGUMENT, "fixed column out of range");
+        fixb[spec.fixed[i]] = 1;
+    }
     const int conv = ctl.convergence_type;
     CYC_REQUIRE(conv >= CYC_CONV_GRADIENT && conv <= CYC_CONV_ZHANG_OLES, CYC_ERR_ARGUMENT,
                 "Unknown convergence criterion");
@@ -681,9 +691,12 @@ extern "C" int cyc_profile_bounds(cyc_dataset* ds, const cyc_prior* prior, const
         StreamScope scope(eng.stream);
         eng.set_weights(spec->weights, spec->weights != nullptr);
         FitRunner r(eng, *prior, *spec, *control);
-        for (int i = 0; i < n; ++i)                       // CcdInterface.cpp:297-302
+        for (int i = 0; i < n; ++i) {                     // CcdInterface.cpp:297-302, R/ModelFit.R:774-778
             CYC_REQUIRE(override_no_regularization || r.pt[columns[i]] == CYC_PRIOR_NONE, CYC_ERR_ARGUMENT,
                         "Variable " + std::to_string(columns[i]) + " is regularized.");
+            CYC_REQUIRE(!r.base_fix[columns[i]], CYC_ERR_ARGUMENT,
+                        "Cannot estimate confidence interval for a fixed coefficient");
+        }
         r.profile(columns, n, threshold, include_penalty != 0, lower, upper, evaluations, fit);
     });
 }
@@ -707,6 +720,7 @@ extern "C" int cyc_profile_log_likelihood(cyc_dataset* ds, const cyc_prior* prio
         StreamScope scope(eng.stream);
         eng.set_weights(spec->weights, spec->weights != nullptr);
         FitRunner r(eng, *prior, *spec, *control);
+        CYC_REQUIRE(!r.base_fix[column], CYC_ERR_ARGUMENT, "cannot profile a fixed coefficient");
         r.profile_points(column, points, n, include_penalty != 0, values);
     });
 }

@@ -205,7 +205,7 @@ struct ColView {
 // ---------------------------------------------------------------------------
 struct RunPlan {
     int C = 0, G = 0;
-    int fixed = -1;             // the column held fixed besides the offset (profile points), -1 none
+    std::vector<int> fixed;     // columns held fixed besides the offset (ascending)
     std::vector<int> len;       // J: columns in the batch starting here (1 = alone), 0 inside a batch
     std::vector<int> lvl;       // J: level of the column in its batch (1 + max level of earlier sharers)
     std::vector<int> dr0, nd;   // J (batch starts): its shared rows are drow[dr0, dr0 + nd)

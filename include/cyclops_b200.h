@@ -191,6 +191,11 @@ typedef struct {
     const double* weights;      /* K, or NULL */
     double variance;            /* prior variance (Laplace lambda = sqrt(2/variance)) */
     const double* start_beta;   /* J, or NULL (zeros; offset column 1) */
+    const int* fixed;           /* columns held at their start value (fitCyclopsModel's
+                                   fixedCoefficients, R/ModelFit.R:205-214 ->
+                                   setFixedBeta), or NULL; the fits of one batched
+                                   solve share one set */
+    int n_fixed;
 } cyc_fit_spec;
 
 typedef struct {

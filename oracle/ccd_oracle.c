@@ -629,6 +629,7 @@ static int ctx_init(Ctx* c, const ccd_problem* p) {
     c->col_groups = (int**)calloc(J, sizeof(int*));
     c->col_ngroups = (int*)calloc(J, sizeof(int));
     if (p->has_offset) { c->beta[0] = 1.0; c->fixb[0] = 1; }           /* CCD init :218-221 */
+    for (int i = 0; i < p->n_fixed; ++i) c->fixb[p->fixed[i]] = 1;     /* setFixedBeta (R/ModelFit.R:205-214) */
     if (c->cumulative) {
         set_pid_for_accumulation(c, NULL);                             /* initialize :1931-1932 */
     } else {

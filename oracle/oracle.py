@@ -32,6 +32,7 @@ class Problem(C.Structure):
         ("prior_type", C.c_int), ("variance", C.c_double),
         ("exclude", C.c_void_p), ("n_exclude", C.c_int),
         ("weights", C.c_void_p),
+        ("fixed", C.c_void_p), ("n_fixed", C.c_int),
     ]
 
 
@@ -63,8 +64,9 @@ def _ptr(a: Optional[np.ndarray]):
     return None if a is None else a.ctypes.data
 
 
-def make_problem(data, prior_type=1, variance=1.0, exclude=None, weights=None):
-    """Returns (Problem, keepalive) for a cyclops_b200.data.CyclopsData."""
+def make_problem(data, prior_type=1, variance=1.0, exclude=None, weights=None, fixed=None):
+    """Returns (Problem, keepalive) for a cyclops_b200.data.CyclopsData;
+    `fixed`: columns held at their start values."""
     if exclude is None:
         exclude = [1 if data.has_offset else 0] if data.has_intercept else []
     keep = {
@@ -78,6 +80,7 @@ def make_problem(data, prior_type=1, variance=1.0, exclude=None, weights=None):
         "cv": np.ascontiguousarray(data.col_val, np.float64),
         "ex": np.ascontiguousarray(exclude, np.int32),
         "w": None if weights is None else np.ascontiguousarray(weights, np.float64),
+        "fx": None if not fixed else np.ascontiguousarray(fixed, np.int32),
     }
     p = Problem(
         model=data.model, K=data.K, J=data.J, pid=_ptr(keep["pid"]), y=_ptr(keep["y"]),
@@ -85,7 +88,8 @@ def make_problem(data, prior_type=1, variance=1.0, exclude=None, weights=None):
         col_idx=_ptr(keep["ci"]), val_ptr=_ptr(keep["vp"]), col_val=_ptr(keep["cv"]),
         has_offset=int(data.has_offset), has_intercept=int(data.has_intercept),
         prior_type=prior_type, variance=variance, exclude=_ptr(keep["ex"]),
-        n_exclude=len(exclude), weights=_ptr(keep["w"]))
+        n_exclude=len(exclude), weights=_ptr(keep["w"]), fixed=_ptr(keep["fx"]),
+        n_fixed=0 if keep["fx"] is None else int(keep["fx"].size))
     return p, keep
 
 
@@ -140,8 +144,8 @@ class _Lib:
         return self._last_error().decode()
 
     def fit(self, data, prior_type=1, variance=1.0, control: Optional[Control] = None,
-            exclude=None, weights=None, start=None) -> Fit:
-        p, keep = make_problem(data, prior_type, variance, exclude, weights)
+            exclude=None, weights=None, start=None, fixed=None) -> Fit:
+        p, keep = make_problem(data, prior_type, variance, exclude, weights, fixed)
         c = control or make_control()
         beta = np.zeros(data.J)
         r = Result(beta=beta.ctypes.data)

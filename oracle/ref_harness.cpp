@@ -183,6 +183,7 @@ std::unique_ptr<Instance> build(const ref_problem* p, int device) {
         *inst->data, *inst->engine, joint,
         bsccs::make_shared<QuietLogger>(), bsccs::make_shared<ThrowingErrorHandler>()));
     inst->ccd->setNoiseLevel(SILENT);
+    for (int i = 0; i < p->n_fixed; ++i) inst->ccd->setFixedBeta(p->fixed[i], true);   // R/ModelFit.R:205-214
     if (p->weights) {
         std::vector<double> w(p->weights, p->weights + p->K);
         inst->ccd->setWeights(w.data());

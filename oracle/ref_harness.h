@@ -27,6 +27,8 @@ typedef struct {
     const int* exclude;      /* column indices with a flat prior */
     int n_exclude;
     const double* weights;   /* K weights or NULL */
+    const int* fixed;        /* columns held at their start (setFixedBeta), or NULL */
+    int n_fixed;
 } ref_problem;
 
 typedef struct {

@@ -194,3 +194,28 @@ def test_profile_bounds_agree_with_newton_profile(name, cols):
             ru = brentq(f, nb[j], up[i] + 0.5 * (up[i] - nb[j]), xtol=1e-12)
             rl = brentq(f, lo[i] - 0.5 * (nb[j] - lo[i]), nb[j], xtol=1e-12)
             assert abs(up[i] - ru) < 1e-3 and abs(lo[i] - rl) < 1e-3, (j, up[i] - ru, lo[i] - rl)
+
+
+def test_port_fixed_coefficients_match_reference():
+    """fixedCoefficients (R/ModelFit.R:205-214 -> setFixedBeta): the Dobson
+    design with outcome3 and treatment3 fixed as test-smallPoisson.R fixes
+    them (at 0, and at other starts), and a Laplace fit with two fixed
+    columns with and without the KKT swindle, against the reference run live."""
+    if not O.have_ref():
+        pytest.skip("reference engine not built here")
+    data, s = load_golden("small_pr_dense")
+    for start in (np.zeros(5), np.array([0.0, 0.3, 0.0, -0.2, 0.0])):
+        a = O.ref().fit(data, D.PRIOR_NONE, 1.0, exclude=[0], start=start, fixed=[1, 3])
+        b = O.port().fit(data, D.PRIOR_NONE, 1.0, exclude=[0], start=start, fixed=[1, 3])
+        assert a.beta[1] == start[1] and a.beta[3] == start[3]
+        assert a.iterations == b.iterations
+        np.testing.assert_allclose(b.beta, a.beta, rtol=1e-12, atol=1e-14)
+    data, s = load_golden("lr_laplace_small")
+    start = np.zeros(data.J)
+    start[[3, 7]] = [0.4, -0.25]
+    for sw in (0, 1):
+        ctl = O.make_control(use_kkt_swindle=sw)
+        a = O.ref().fit(data, D.PRIOR_LAPLACE, float(s["variance"]), control=ctl, start=start, fixed=[3, 7])
+        b = O.port().fit(data, D.PRIOR_LAPLACE, float(s["variance"]), control=ctl, start=start, fixed=[3, 7])
+        assert a.iterations == b.iterations
+        np.testing.assert_allclose(b.beta, a.beta, rtol=1e-12, atol=1e-14)
