@@ -126,6 +126,7 @@ class _Lib:
         if prefix == "ref_":
             sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
             sigs["fisher"] = [P(Problem), V, V, C.c_int, V, C.c_int]
+            sigs["predictive_estimates"] = [P(Problem), V, V, V]
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
             sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
                                P(Result), C.c_int]
@@ -217,6 +218,16 @@ class _Lib:
         if getattr(self.lib, self.prefix + "profile_points")(*args):
             raise RuntimeError(self.err())
         return vals
+
+    def predictive_estimates(self, data, beta, weights=None, fill=0.0):
+        """getPredictiveEstimates at `beta` (rows with zero weight keep `fill`)."""
+        p, keep = make_problem(data, 1, 1.0, None, None)
+        b = np.ascontiguousarray(beta, np.float64)
+        w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+        y = np.full(data.K, float(fill))
+        if self.lib.ref_predictive_estimates(C.byref(p), _ptr(b), _ptr(w), _ptr(y)):
+            raise RuntimeError(self.err())
+        return y
 
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)

@@ -306,6 +306,18 @@ int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n
     });
 }
 
+int ref_predictive_estimates(const ref_problem* p, const double* beta, const double* weights, double* y) {
+    return guarded([&] {
+        auto inst = build(p, 0);
+        std::vector<double> b(beta, beta + p->J);
+        inst->ccd->setBeta(b);
+        inst->ccd->getLogLikelihood();          // runs the lazy set-up (xbeta)
+        std::vector<double> w;
+        if (weights) w.assign(weights, weights + p->K);
+        inst->engine->getPredictiveEstimates(y, weights ? w.data() : nullptr);
+    });
+}
+
 int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int n, double* out, int device) {
     return guarded([&] {
         auto inst = build(p, device);

@@ -98,6 +98,10 @@ int ref_ingest(const ref_ingest_input* in, ref_ingest_output* out);
  * CyclicCoordinateDescent.cpp:1288-1300) at `beta` for `n` columns; out is
  * n x n row-major.  device 1 runs it through the CUDA adapter. */
 int ref_fisher(const ref_problem* p, const double* beta, const int* columns, int n, double* out, int device);
+/* AbstractModelSpecifics::getPredictiveEstimates (src/cyclops/engine/
+ * ModelSpecifics.hpp:693-707) at `beta`: y[k] for rows with nonzero weight
+ * (all rows when weights is NULL); other entries of y are left as given. */
+int ref_predictive_estimates(const ref_problem* p, const double* beta, const double* weights, double* y);
 void ref_ingest_free(ref_ingest_output* out);
 /* Profile-likelihood bounds (CcdInterface::profileModel, src/cyclops/
  * CcdInterface.cpp:262-420, one thread): fit, then for each column its upper

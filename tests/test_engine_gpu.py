@@ -82,6 +82,28 @@ def test_predictive_loglik_matches_oracle(cuda_lib):
         assert rel_err(got, want) < 1e-10, (name, got, want)
 
 
+def test_predictive_estimates_match_reference(cuda_lib):
+    """getPredictiveEstimates (ModelSpecifics.hpp:693-707): the logistic
+    probability, the Poisson mean, or xbeta, on the rows with nonzero weight;
+    the caller's other entries stay as they were."""
+    from cyclops_b200 import _native as N
+    from oracle import oracle as O
+    if not O.have_ref():
+        pytest.skip("reference engine not built here")
+    for name in ("lr_laplace_small", "pr_offset_normal", "clr_laplace", "cox_laplace"):
+        data, s = load_golden(name)
+        ds, e, use = _engine(data, None)
+        e.compute_xbeta(s["beta"])
+        e.compute_remaining_statistics()
+        w = (np.arange(data.K) % 4 != 0).astype(float)
+        want = O.ref().predictive_estimates(data, s["beta"], w, fill=-7.0)
+        y = np.full(data.K, -7.0)
+        N.check(N.lib().cyc_engine_get_predictive_estimates(e.handle, y.ctypes.data, w.ctypes.data))
+        np.testing.assert_allclose(y, want, rtol=1e-12, atol=1e-14)
+        np.testing.assert_allclose(e.get_predictive_estimates(), O.ref().predictive_estimates(data, s["beta"]),
+                                   rtol=1e-12, atol=1e-14)
+
+
 def test_gradient_before_statistics_is_a_state_error(cuda_lib):
     from cyclops_b200 import api, _native
     data, s = load_golden("lr_laplace_small")
