@@ -24,6 +24,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -77,8 +78,9 @@ class Clocks:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else "",
-                                 f".clocks_{os.getpid()}.csv")
+        # the raw samples go to CYCLOPS_CLOCKS_DIR when set (kept for inspection), else a temporary file
+        out_dir = os.environ.get("CYCLOPS_CLOCKS_DIR") or tempfile.gettempdir()
+        self.path = os.path.join(out_dir, f".clocks_{os.getpid()}.csv")
 
     def __enter__(self):
         try:
