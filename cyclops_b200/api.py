@@ -379,6 +379,35 @@ def profile_log_likelihood(data, column: int, points: Sequence[float], prior: Op
 
 
 @dataclasses.dataclass
+class CvAutoResult:
+    variance: float               # the variance the search settles on
+    expected: float               # the search's predicted held-out log likelihood there
+    tried: np.ndarray             # (steps, 3): variance, mean, stdev of each step
+
+
+def cv_auto_search(data, prior: PriorSpec, fold_of_row, n_folds: int, starting_variance: float = -1.0,
+                   control: Optional[ControlSpec] = None, device: int = 0) -> CvAutoResult:
+    """Auto-search cross-validation (createControl(cvType = "auto"), R's
+    default; AutoSearchCrossValidationDriver): one variance per step, every
+    fold refit on the GPU as one batched solve, the next variance proposed by
+    the reference's unimodal search.  `fold_of_row`: K fold ids, or
+    (repetitions, K)."""
+    ds = data if isinstance(data, Dataset) else Dataset(data, device)
+    control = control or create_control()
+    p, keep_ex = _prior_struct(ds.data, prior)
+    folds = np.ascontiguousarray(np.atleast_2d(fold_of_row), np.int32)
+    n_reps = folds.shape[0]
+    bv, val, n = C.c_double(), C.c_double(), C.c_int()
+    tv, tm, ts = np.zeros(64), np.zeros(64), np.zeros(64)
+    c = _control_struct(control)
+    N.check(N.lib().cyc_cv_auto_search(ds.handle, C.byref(p), _ptr(folds), int(n_folds), int(n_reps),
+                                       float(starting_variance), C.byref(c), C.byref(bv), C.byref(val), _ptr(tv),
+                                       _ptr(tm), _ptr(ts), 64, C.byref(n)))
+    k = min(n.value, 64)
+    return CvAutoResult(bv.value, val.value, np.stack([tv[:k], tm[:k], ts[:k]], axis=1))
+
+
+@dataclasses.dataclass
 class AsymptoticVariance:
     columns: np.ndarray           # the columns with a row / column in the matrices
     fisher: np.ndarray            # Fisher information (precision) matrix

@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -35,6 +36,7 @@
 
 #include "engine.cuh"
 #include "solver_common.cuh"
+#include "variance_search.h"
 
 namespace cg = cooperative_groups;
 
@@ -2247,5 +2249,119 @@ extern "C" int cyc_profile_log_likelihood_batch(cyc_dataset* dsh, const cyc_prio
         run_batch(ds, prior, specs.data(), n, ctl, out.data(), nullptr, 0, nullptr, nullptr, column);
         for (int i = 0; i < n; ++i)
             values[i] = out[i].log_likelihood + (include_penalty ? out[i].log_prior : 0.0);
+    });
+}
+
+// ---- auto-search cross-validation ---------------------------------------------
+//
+// AutoSearchCrossValidationDriver::doCrossValidationLoop
+// (src/cyclops/drivers/AutoSearchCrossValidationDriver.cpp:63-160): one
+// variance at a time, every fold (of every repetition) refit at it, the
+// held-out predictive log likelihoods' mean and standard deviation
+// (computePointEstimate / computeStDev, AbstractCrossValidationDriver.cpp:
+// 252-276) handed to UniModalSearch (src/utils/HParSearch.cpp), which
+// proposes the next variance.  Each step's folds are one batched solve here.
+// Every fit cold-starts (the reference's resetCoefficients).
+namespace {
+
+// getNormalBasedDefaultVar (ModelData.cpp:680-728): the summed squares of
+// the variable columns (those after the offset and intercept) / their
+// count / K
+double normal_based_default_variance(Dataset& ds) {
+    const int start = (ds.has_intercept ? 1 : 0) + (ds.has_offset ? 1 : 0);
+    CYC_REQUIRE(ds.J > start, CYC_ERR_ARGUMENT, "no variable columns");
+    std::vector<double> val(ds.nnz_val);
+    if (ds.nnz_val) {
+        CYC_CHECK_CUDA(cudaMemcpyAsync(val.data(), ds.d_val.get(), ds.nnz_val * sizeof(double),
+                                       cudaMemcpyDeviceToHost, ds.stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(ds.stream));
+    }
+    double total = 0.0;
+    for (int j = start; j < ds.J; ++j) {
+        const int f = ds.fmt[j];
+        if (f == CYC_INDICATOR) {
+            total += (double)(ds.col_ptr[j + 1] - ds.col_ptr[j]);
+        } else if (f == CYC_INTERCEPT) {
+            total += (double)ds.K;
+        } else {
+            double s = 0.0;
+            for (long long e = ds.val_ptr[j]; e < ds.val_ptr[j + 1]; ++e) s += val[e] * val[e];
+            total += s;
+        }
+    }
+    return total / (ds.J - start) / ds.K;
+}
+
+}  // namespace
+
+extern "C" int cyc_cv_auto_search(cyc_dataset* dsh, const cyc_prior* prior, const int* fold_of_row, int n_folds,
+                                  int n_reps, double starting_variance, const cyc_control* ctl,
+                                  double* best_variance, double* best_value, double* tried_variance,
+                                  double* tried_mean, double* tried_sd, int max_tried, int* n_tried) {
+    return guarded([&] {
+        NvtxRange range("cyc_cv_auto_search");
+        CYC_REQUIRE(dsh && prior && fold_of_row && ctl && best_variance && best_value && n_folds > 1 && n_reps > 0,
+                    CYC_ERR_ARGUMENT, "null argument");
+        CYC_REQUIRE(n_folds <= 127, CYC_ERR_ARGUMENT, "at most 127 folds");
+        CYC_REQUIRE(max_tried <= 0 || (tried_variance && tried_mean && tried_sd), CYC_ERR_ARGUMENT, "null argument");
+        Dataset& ds = dsh->ds;
+        for (long long k = 0; k < (long long)ds.K * n_reps; ++k)
+            CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
+        CYC_CHECK_CUDA(cudaSetDevice(ds.device));
+        StreamScope scope(ds.stream);
+        const int J = ds.J;
+        double x = starting_variance > 0 ? starting_variance : normal_based_default_variance(ds);
+        std::vector<DevBuf<int>> d_folds(n_reps);
+        for (int r = 0; r < n_reps; ++r) {
+            d_folds[r].alloc(ds.K);
+            CYC_CHECK_CUDA(cudaMemcpyAsync(d_folds[r].get(), fold_of_row + (size_t)r * ds.K, ds.K * sizeof(int),
+                                           cudaMemcpyHostToDevice, ds.stream));
+        }
+        CYC_CHECK_CUDA(cudaStreamSynchronize(ds.stream));
+        std::vector<int> fit_fold(n_folds);
+        for (int f = 0; f < n_folds; ++f) fit_fold[f] = f;
+        std::vector<double> betas((size_t)n_folds * J);
+        std::vector<cyc_fit_result> out(n_folds);
+        cyc::VarianceSearch search;
+        double value = 0.0;
+        int tried = 0;
+        for (int step = 0; step < 50; ++step) {            // MAX_STEPS, AutoSearchCrossValidationDriver.cpp:28
+            std::vector<double> pll_all;
+            for (int r = 0; r < n_reps; ++r) {
+                std::vector<cyc_fit_spec> specs(n_folds);
+                for (int f = 0; f < n_folds; ++f) {
+                    specs[f] = cyc_fit_spec{};
+                    specs[f].variance = x;
+                    out[f] = cyc_fit_result{};
+                    out[f].beta = betas.data() + (size_t)f * J;
+                }
+                std::vector<double> pll;
+                run_batch(ds, prior, specs.data(), n_folds, ctl, out.data(), d_folds[r].get(), n_folds, &fit_fold,
+                          &pll);
+                for (int f = 0; f < n_folds; ++f)
+                    pll_all.push_back(out[f].return_flag == CYC_SUCCESS ? pll[f] : std::nan(""));
+            }
+            double total = 0.0, inner = 0.0;
+            int count = 0;
+            for (double v : pll_all)
+                if (v == v) { total += v; ++count; }
+            const double mean = total / count;
+            for (double v : pll_all)
+                if (v == v) inner += v * v;
+            const double sd = std::sqrt(inner / count - mean * mean);
+            if (tried < max_tried) {
+                tried_variance[tried] = x;
+                tried_mean[tried] = mean;
+                tried_sd[tried] = sd;
+            }
+            ++tried;
+            search.tried(x, mean, sd);
+            bool go;
+            search.step(&go, &x, &value);
+            if (!go) break;
+        }
+        *best_variance = x;
+        *best_value = value;
+        if (n_tried) *n_tried = tried;
     });
 }

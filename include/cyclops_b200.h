@@ -269,6 +269,24 @@ int cyc_profile_log_likelihood_batch(cyc_dataset* ds, const cyc_prior* prior, co
                                      const cyc_control* control, int column, const double* points, int n,
                                      int include_penalty, double* values);
 
+/* Auto-search cross-validation (createControl(cvType = "auto"), R's
+ * default: AutoSearchCrossValidationDriver, src/cyclops/drivers/
+ * AutoSearchCrossValidationDriver.cpp:63-160, with the UniModalSearch of
+ * src/utils/HParSearch.cpp).  From `starting_variance` (<= 0: the
+ * normal-based default, ModelData.cpp:716-720) each step refits every fold
+ * of every repetition at one variance (one batched solve per repetition,
+ * cold starts: the reference's resetCoefficients), takes the mean and
+ * standard deviation of the held-out predictive log likelihoods (NaN folds
+ * left out) and lets the search propose the next variance; at most 50
+ * steps.  fold_of_row: n_reps x K fold ids (e.g. from cyc_cv_fold_weights).
+ * Returns the variance the search settles on and its expected value, and
+ * the first max_tried points tried (variance, mean, stdev; *n_tried counts
+ * all). */
+int cyc_cv_auto_search(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds, int n_reps,
+                       double starting_variance, const cyc_control* control, double* best_variance,
+                       double* best_value, double* tried_variance, double* tried_mean, double* tried_sd,
+                       int max_tried, int* n_tried);
+
 /* Cross-validation fold masks, `n_reps * folds` rows of K weights (0 = held
  * out), exactly as CrossValidationSelector draws them
  * (src/cyclops/drivers/CrossValidationSelector.cpp:21-116): by row

@@ -127,6 +127,8 @@ class _Lib:
             sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
             sigs["fisher"] = [P(Problem), V, V, C.c_int, V, C.c_int]
             sigs["predictive_estimates"] = [P(Problem), V, V, V]
+            sigs["cv_auto"] = [P(Problem), P(Control), C.c_int, C.c_int, C.c_long, C.c_int, C.c_double, C.c_int,
+                               P(C.c_double), P(C.c_double), V, V, V, C.c_int, P(C.c_int)]
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
             sigs["profile"] = [P(Problem), P(Control), V, V, C.c_int, C.c_double, C.c_int, C.c_int, V, V, V,
                                P(Result), C.c_int]
@@ -229,6 +231,23 @@ class _Lib:
             raise RuntimeError(self.err())
         return y
 
+    def cv_auto(self, data, prior_type, fold=10, n_reps=1, seed=123, by_row=True, starting_variance=-1.0,
+                reset_coefficients=True, control: Optional[Control] = None, exclude=None):
+        """AutoSearchCrossValidationDriver run by the reference (one thread).
+        Returns (best_variance, best_value, tried) with tried an (n, 3) array
+        of (variance, mean, stdev) as the driver logged them."""
+        p, keep = make_problem(data, prior_type, 1.0, exclude, None)
+        c = control or make_control()
+        bv, bval, n = C.c_double(), C.c_double(), C.c_int()
+        tv, tm, ts = np.zeros(64), np.zeros(64), np.zeros(64)
+        rc = ref_dyn().lib.ref_cv_auto(C.byref(p), C.byref(c), int(fold), int(n_reps), int(seed), int(by_row),
+                                  float(starting_variance), int(reset_coefficients), C.byref(bv), C.byref(bval),
+                                  _ptr(tv), _ptr(tm), _ptr(ts), 64, C.byref(n))
+        if rc:
+            raise RuntimeError(ref_dyn().err())
+        k = n.value
+        return bv.value, bval.value, np.stack([tv[:k], tm[:k], ts[:k]], axis=1)
+
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)
         b = np.ascontiguousarray(beta, np.float64)
@@ -249,6 +268,14 @@ def ref() -> _Lib:
     if "ref" not in _cache:
         _cache["ref"] = _Lib("libcyclops_ref.so", "ref_")
     return _cache["ref"]
+
+
+def ref_dyn() -> _Lib:
+    """The reference engine linked against the process's shared C++ runtime
+    (for the CV drivers, whose logging formats numbers through iostreams)."""
+    if "ref_dyn" not in _cache:
+        _cache["ref_dyn"] = _Lib("libcyclops_ref_dyn.so", "ref_")
+    return _cache["ref_dyn"]
 
 
 def port() -> _Lib:

@@ -18,6 +18,9 @@
 //   * CV fold masks     CrossValidationSelector  src/cyclops/drivers/CrossValidationSelector.cpp:21-116
 //   * engine probes     AbstractModelSpecifics virtuals, called directly on the
 //                       same engine object the CCD uses.
+//   * auto-search CV    AutoSearchCrossValidationDriver (drivers/, with
+//                       utils/HParSearch.cpp) as CcdInterface::runCrossValidation
+//                       drives it, src/cyclops/CcdInterface.cpp:731-790
 //   * profile points    CcdInterface::evaluateProfileModel with one thread
 //                       src/cyclops/CcdInterface.cpp:527-618
 //   * profile bounds    CcdInterface::profileModel with one thread
@@ -27,6 +30,7 @@
 //                       CcdInterface.cpp needs the R runtime).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -41,6 +45,8 @@
 #include "priors/JointPrior.h"
 #include "priors/CovariatePrior.h"
 #include "drivers/CrossValidationSelector.h"
+#include "drivers/AutoSearchCrossValidationDriver.h"
+#include "CcdInterface.h"
 #include "io/ProgressLogger.h"
 
 #include "utils/RZeroIn.h"
@@ -62,6 +68,14 @@ thread_local std::string g_error;
 class QuietLogger : public loggers::ProgressLogger {
 public:
     void writeLine(const std::ostringstream&) override {}
+    void yield() override {}
+};
+
+// keeps every line the drivers log (the auto search logs each point it tries)
+class RecordingLogger : public loggers::ProgressLogger {
+public:
+    std::vector<std::string> lines;
+    void writeLine(const std::ostringstream& s) override { lines.push_back(s.str()); }
     void yield() override {}
 };
 
@@ -423,6 +437,66 @@ int ref_profile_points(const ref_problem* p, const ref_control* c, const double*
             ProfileObjective eval{ccd, args, column, 0.0, 0.0, include_penalty != 0};
             values[i] = eval.objective(points[i]);
         }
+    });
+}
+
+}  // extern "C"
+
+namespace {
+// the auto-search driver with its result readable (maxPoint is protected)
+class AutoSearchProbe : public AutoSearchCrossValidationDriver {
+public:
+    using AutoSearchCrossValidationDriver::AutoSearchCrossValidationDriver;
+    MaxPoint best() const { return maxPoint; }
+};
+}  // namespace
+
+extern "C" {
+
+int ref_cv_auto(const ref_problem* p, const ref_control* c, int fold, int n_reps, long seed, int by_row,
+                double starting_variance, int reset_coefficients, double* best_variance, double* best_value,
+                double* tried_variance, double* tried_mean, double* tried_sd, int max_tried, int* n_tried) {
+    return guarded([&] {
+        auto inst = build(p, 0);
+        CCDArguments args = CCDArguments();   // value-initialised: the flags it leaves unset read as false / 0
+        args.modeFinding = toArguments(c);
+        args.threads = 1;
+        args.seed = seed;
+        args.resetCoefficients = reset_coefficients != 0;
+        args.useNormalPrior = p->prior_type == REF_PRIOR_NORMAL;
+        args.crossValidation.doCrossValidation = true;
+        args.crossValidation.useAutoSearchCV = true;
+        args.crossValidation.fold = fold;
+        args.crossValidation.foldToCompute = fold * n_reps;
+        args.crossValidation.startingVariance = starting_variance;
+        args.crossValidation.selectorType = by_row ? SelectorType::BY_ROW : SelectorType::BY_PID;
+        auto logger = bsccs::make_shared<RecordingLogger>();
+        auto err = bsccs::make_shared<ThrowingErrorHandler>();
+        std::vector<int> ids = inst->data->getPidVectorSTL();
+        CrossValidationSelector selector(fold, ids, args.crossValidation.selectorType, seed, logger, err,
+                                         nullptr, nullptr);
+        AutoSearchProbe driver(*inst->data, args, logger, err, nullptr);
+        driver.drive(*inst->ccd, selector, args);
+        const MaxPoint mp = driver.best();
+        *best_variance = mp.point[0];
+        *best_value = mp.value;
+        // the points tried, from the driver's log (6 significant digits)
+        int n = 0;
+        double m = 0, sd = 0;
+        for (const auto& line : logger->lines) {
+            const auto a = line.find("AvgPred = ");
+            if (a != std::string::npos) std::sscanf(line.c_str() + a, "AvgPred = %lf with stdev = %lf", &m, &sd);
+            const auto b = line.find("Completed at ");
+            if (b != std::string::npos && n < max_tried) {
+                double v = 0;
+                std::sscanf(line.c_str() + b, "Completed at %lf", &v);
+                tried_variance[n] = v;
+                tried_mean[n] = m;
+                tried_sd[n] = sd;
+                ++n;
+            }
+        }
+        *n_tried = n;
     });
 }
 

@@ -117,4 +117,16 @@ int ref_profile(const ref_problem* p, const ref_control* c, const double* start_
  * then one refit per point, each warm-started from the last. */
 int ref_profile_points(const ref_problem* p, const ref_control* c, const double* start_beta, int column,
                        const double* points, int n, int include_penalty, double* values, int device);
+/* Auto-search cross-validation (AutoSearchCrossValidationDriver,
+ * src/cyclops/drivers/AutoSearchCrossValidationDriver.cpp:63-160, with the
+ * UniModalSearch of src/utils/HParSearch.cpp) as CcdInterface::runCrossValidation
+ * runs it with one thread: `fold`-fold CV repeated n_reps times, selector by
+ * row or by stratum, seed, starting variance (<= 0: the normal-based
+ * default), cold starts when reset_coefficients.  Returns the chosen
+ * variance and its predicted value, and the points tried (variance, mean
+ * and stdev of the held-out predictive log likelihood; from the driver's
+ * log, 6 significant digits). */
+int ref_cv_auto(const ref_problem* p, const ref_control* c, int fold, int n_reps, long seed, int by_row,
+                double starting_variance, int reset_coefficients, double* best_variance, double* best_value,
+                double* tried_variance, double* tried_mean, double* tried_sd, int max_tried, int* n_tried);
 #endif

@@ -22,7 +22,7 @@ def golden_names():
     """The plain fit fixtures (not the CV folds, ingest tables or swindle fits)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
                   if not p.endswith("cv_folds.npz")
-                  and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_", "small_")))
+                  and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_", "small_", "cvauto_")))
 
 
 def small_names():
@@ -30,6 +30,11 @@ def small_names():
     test-smallBernoulli.R, test-smallPoisson.R) with the reference's fits and
     an independent Newton MLE."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "small_*.npz")))
+
+
+def cvauto_names():
+    """The reference's auto-search CV results on fit fixtures' data."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "cvauto_*.npz")))
 
 
 def profile_names():

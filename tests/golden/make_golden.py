@@ -367,6 +367,38 @@ def save_small():
               f"|tight-newton|={np.max(np.abs(tight.beta - nb)):.2e}")
 
 
+# (fixture, prior, by_row, starting variance (<= 0: the normal-based default))
+CV_AUTO_CASES = [("lr_laplace_small", D.PRIOR_LAPLACE, True, -1.0),
+                 ("lr_c1", D.PRIOR_LAPLACE, True, -1.0),
+                 ("clr_laplace", D.PRIOR_LAPLACE, False, -1.0),
+                 ("cpr_normal", D.PRIOR_NORMAL, False, -1.0),
+                 ("lr_zhang_oles", D.PRIOR_LAPLACE, True, 0.5)]
+
+
+def save_cv_auto():
+    """cvauto_<case>.npz: the reference's auto-search cross-validation
+    (AutoSearchCrossValidationDriver with UniModalSearch, one thread, cold
+    starts, 10 folds, seed 123) on a fit fixture's data: the chosen variance,
+    its predicted value and the points it tried."""
+    for name, prior, by_row, start in CV_AUTO_CASES:
+        d, _ = _load_fixture(name)
+        bv, bval, tried = O.ref().cv_auto(d, prior, fold=10, n_reps=1, seed=123, by_row=by_row,
+                                          starting_variance=start, reset_coefficients=True)
+        np.savez_compressed(os.path.join(HERE, "cvauto_" + name + ".npz"), base=name, prior=prior, fold=10,
+                            seed=123, by_row=int(by_row), starting_variance=start, best_variance=bv,
+                            best_value=bval, tried=tried)
+        print(f"cvauto_{name:20s} best={bv:.6g} value={bval:.6g} steps={len(tried)}")
+
+
+def _load_fixture(name):
+    z = np.load(os.path.join(HERE, name + ".npz"))
+    data = D.CyclopsData(model=int(z["model"]), y=z["y"], col_format=z["col_format"], col_ptr=z["col_ptr"],
+                         col_idx=z["col_idx"], val_ptr=z["val_ptr"], col_val=z["col_val"],
+                         pid=z["pid"] if z["pid"].size else None, time=z["time"] if z["time"].size else None,
+                         has_offset=bool(z["has_offset"]), has_intercept=bool(z["has_intercept"]))
+    return data, z
+
+
 def main(parts):
     if not O.have_ref():
         O.build()
@@ -383,8 +415,10 @@ def main(parts):
         save_profile()
     if "small" in parts:
         save_small()
+    if "cvauto" in parts:
+        save_cv_auto()
 
 
 if __name__ == "__main__":
-    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile] [small]   (default: all)
-    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile", "small"])
+    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile] [small] [cvauto]
+    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile", "small", "cvauto"])
