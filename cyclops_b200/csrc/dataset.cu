@@ -139,7 +139,7 @@ void Dataset::ensure_csr() {
 using namespace cyc;
 
 extern "C" const char* cyc_last_error(void) { return g_last_error.c_str(); }
-extern "C" int cyc_version(void) { return 1; }
+extern "C" int cyc_version(void) { return CYC_ABI_VERSION; }
 extern "C" long long cyc_launch_count(void) { return g_launches.load(); }
 
 extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_dataset** out) {

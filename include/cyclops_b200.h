@@ -101,6 +101,10 @@ typedef struct cyc_dataset cyc_dataset;
 typedef struct cyc_engine cyc_engine;
 
 const char* cyc_last_error(void);
+/* ABI revision: 2 since cyc_control gained use_kkt_swindle, cyc_fit_spec
+ * gained fixed / n_fixed and cyc_run_stats gained cluster_ctas (fields
+ * appended; zero-initialise these structs, e.g. `cyc_fit_spec s = {0};`). */
+#define CYC_ABI_VERSION 2
 int cyc_version(void);
 
 /* Copy a dataset to device `device`.  Replaces the host-side ModelData the

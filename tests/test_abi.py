@@ -103,3 +103,10 @@ def test_struct_mirrors_match_the_header(tmp_path):
         st = getattr(N, pyname)
         want = ctypes.sizeof(st) if field == "size" else getattr(st, field).offset
         assert int(value) == want, (pyname, field, int(value), want)
+
+
+def test_library_reports_the_header_abi_version(cuda_lib):
+    import re
+    txt = open(os.path.join(ROOT, "include", "cyclops_b200.h")).read()
+    want = int(re.search(r"#define CYC_ABI_VERSION (\d+)", txt).group(1))
+    assert cuda_lib.cyc_version() == want
