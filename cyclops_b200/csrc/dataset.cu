@@ -152,8 +152,9 @@ extern "C" int cyc_dataset_create(const cyc_data_desc* d, int device, cyc_datase
         CYC_REQUIRE(d->y && d->col_format && d->col_ptr && d->val_ptr, CYC_ERR_ARGUMENT, "missing arrays");
         CYC_REQUIRE(d->model != CYC_COX || d->time, CYC_ERR_ARGUMENT, "cox needs survival times");
         // a NaN or an infinity among the outcomes, times or covariate values
-        // leaves every fit undefined (the reference engine runs into it with
-        // no defined result), so such data is refused before any device work
+        // leaves every fit undefined (the reference's fit on such data comes
+        // back ILLCONDITIONED with NaN coefficients), so such data is refused
+        // before any device work
         auto finite = [](const double* a, long long n) {
             for (long long i = 0; i < n; ++i)
                 if (!std::isfinite(a[i])) return false;
