@@ -481,9 +481,12 @@ class CvGridResult:
 
 
 def cv_grid_fit(data, prior: PriorSpec, fold_of_row, n_folds: int, variances: Sequence[float],
-                control: Optional[ControlSpec] = None, device: int = 0) -> CvGridResult:
+                control: Optional[ControlSpec] = None, device: int = 0, weights=None) -> CvGridResult:
     """Cross-validation over a prior-variance grid as one batched GPU solve
-    (GridSearchCrossValidationDriver + AbstractCrossValidationDriver)."""
+    (GridSearchCrossValidationDriver + AbstractCrossValidationDriver).
+    `weights` (K observation weights) trains each fold at those weights and
+    scores the held-out rows at theirs, as the reference's selector does
+    with the fit's weights."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     control = control or create_control()
     p, keep_ex = _prior_struct(ds.data, prior)
@@ -497,8 +500,13 @@ def cv_grid_fit(data, prior: PriorSpec, fold_of_row, n_folds: int, variances: Se
     pll = np.zeros(F)
     gm = np.zeros(var.size)
     c = _control_struct(control)
-    N.check(N.lib().cyc_cv_grid_fit(ds.handle, C.byref(p), _ptr(fold), int(n_folds), _ptr(var), int(var.size),
-                                    C.byref(c), results, _ptr(pll), _ptr(gm)))
+    if weights is None:
+        N.check(N.lib().cyc_cv_grid_fit(ds.handle, C.byref(p), _ptr(fold), int(n_folds), _ptr(var), int(var.size),
+                                        C.byref(c), results, _ptr(pll), _ptr(gm)))
+    else:
+        w = np.ascontiguousarray(weights, np.float64)
+        N.check(N.lib().cyc_cv_grid_fit_weighted(ds.handle, C.byref(p), _ptr(fold), int(n_folds), _ptr(w), _ptr(var),
+                                                 int(var.size), C.byref(c), results, _ptr(pll), _ptr(gm)))
     fits = [FitResult(betas[f].copy(), results[f].log_likelihood, results[f].log_prior,
                       results[f].iterations, results[f].return_flag) for f in range(F)]
     best = int(np.nanargmax(gm)) if np.any(np.isfinite(gm)) else -1

@@ -2365,3 +2365,73 @@ extern "C" int cyc_cv_auto_search(cyc_dataset* dsh, const cyc_prior* prior, cons
         if (n_tried) *n_tried = tried;
     });
 }
+
+// Cross-validation with observation weights (CrossValidationSelector with
+// wtsOriginal, src/cyclops/drivers/CrossValidationSelector.cpp:72-124, as
+// CcdInterface::runCrossValidation passes the fit's weights, :738-754): fit
+// (variance v, fold f) trains with the original weight on rows outside fold
+// f and 0 on it, and is scored on fold f's rows at their original weights
+// (getComplement).  The fits run as one batched solve with per-fit weights;
+// each held-out predictive log likelihood is one engine evaluation at the
+// fit's coefficients (getNewPredictiveLogLikelihood, CyclicCoordinateDescent
+// .cpp:319-353).  Cold starts, as cyc_cv_grid_fit.
+extern "C" int cyc_cv_grid_fit_weighted(cyc_dataset* dsh, const cyc_prior* prior, const int* fold_of_row,
+                                        int n_folds, const double* row_weights, const double* variances, int n_var,
+                                        const cyc_control* ctl, cyc_fit_result* out, double* pred_loglik,
+                                        double* grid_mean) {
+    return guarded([&] {
+        NvtxRange range("cyc_cv_grid_fit_weighted");
+        CYC_REQUIRE(dsh && prior && fold_of_row && row_weights && variances && ctl && out && n_folds > 1 && n_var > 0,
+                    CYC_ERR_ARGUMENT, "null argument");
+        Dataset& ds = dsh->ds;
+        const int K = ds.K;
+        for (int k = 0; k < K; ++k) {
+            CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
+            CYC_REQUIRE(std::isfinite(row_weights[k]) && row_weights[k] >= 0, CYC_ERR_ARGUMENT,
+                        "weights must be finite and nonnegative");
+        }
+        CYC_CHECK_CUDA(cudaSetDevice(ds.device));
+        const int F = n_folds * n_var;
+        std::vector<double> train((size_t)n_folds * K), held((size_t)n_folds * K);
+        for (int f = 0; f < n_folds; ++f)
+            for (int k = 0; k < K; ++k) {
+                const bool out_f = fold_of_row[k] == f;
+                train[(size_t)f * K + k] = out_f ? 0.0 : row_weights[k];
+                held[(size_t)f * K + k] = out_f ? row_weights[k] : 0.0;
+            }
+        std::vector<cyc_fit_spec> specs(F);
+        for (int i = 0; i < F; ++i) {
+            specs[i] = cyc_fit_spec{};
+            specs[i].weights = train.data() + (size_t)(i % n_folds) * K;
+            specs[i].variance = variances[i / n_folds];
+        }
+        run_batch(ds, prior, specs.data(), F, ctl, out, nullptr, 0, nullptr, nullptr);
+        std::vector<double> pll(F);
+        {
+            Engine eng(&ds);
+            StreamScope scope(eng.stream);
+            for (int i = 0; i < F; ++i) {
+                if (out[i].return_flag != CYC_SUCCESS) {       // AbstractCrossValidationDriver.cpp:236-240
+                    pll[i] = std::nan("");
+                    continue;
+                }
+                const int f = i % n_folds;
+                eng.set_weights(train.data() + (size_t)f * K, true);
+                eng.compute_xbeta(out[i].beta);
+                eng.remaining_statistics(true);
+                pll[i] = eng.predictive_log_likelihood(held.data() + (size_t)f * K);
+            }
+        }
+        if (pred_loglik) std::copy(pll.begin(), pll.end(), pred_loglik);
+        if (grid_mean)
+            for (int v = 0; v < n_var; ++v) {
+                double tot = 0.0;
+                int cnt = 0;
+                for (int f = 0; f < n_folds; ++f) {
+                    const double x = pll[v * n_folds + f];
+                    if (x == x) { tot += x; ++cnt; }
+                }
+                grid_mean[v] = tot / cnt;
+            }
+    });
+}

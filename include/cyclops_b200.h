@@ -273,6 +273,16 @@ int cyc_profile_log_likelihood_batch(cyc_dataset* ds, const cyc_prior* prior, co
                                      const cyc_control* control, int column, const double* points, int n,
                                      int include_penalty, double* values);
 
+/* cyc_cv_grid_fit with observation weights (the fit's weights handed to
+ * the CV selector, CrossValidationSelector.cpp:72-124): fit (variance v,
+ * fold f) trains on the rows outside fold f at their weights and is scored
+ * on fold f's rows at their weights (getComplement).  lr, pr, clr, cpr;
+ * cold starts; outputs as cyc_cv_grid_fit. */
+int cyc_cv_grid_fit_weighted(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds,
+                             const double* row_weights, const double* variances, int n_var,
+                             const cyc_control* control, cyc_fit_result* out, double* pred_loglik,
+                             double* grid_mean);
+
 /* Auto-search cross-validation (createControl(cvType = "auto"), R's
  * default: AutoSearchCrossValidationDriver, src/cyclops/drivers/
  * AutoSearchCrossValidationDriver.cpp:63-160, with the UniModalSearch of

@@ -13,7 +13,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import exclude_for, load_golden, rel_err
 from cyclops_b200 import data as D
 
 pytestmark = pytest.mark.gpu
@@ -110,3 +110,36 @@ def test_cluster_sizes_agree(cuda_lib, cluster_size):
         out[c] = np.array([f.beta for f in api.cv_grid_fit(data, prior, folds, 4, variances, ctl).fits])
     for c in (2, 5, 8):
         assert np.max(np.abs(out[c] - out[1]) / np.maximum(np.abs(out[1]), 1.0)) < 1e-6, c
+
+
+@pytest.mark.parametrize("name", ["lr_normal_weighted", "pr_offset_normal", "clr_normal_weighted"])
+def test_weighted_cv_grid_matches_oracle(cuda_lib, name):
+    """Observation weights in CV (CrossValidationSelector with the fit's
+    weights): each fold trains at the weights outside it and is scored at
+    the weights inside it; fits and held-out log likelihoods against the
+    restatement oracle run on the same masks."""
+    from cyclops_b200 import api
+    from oracle import oracle as O
+    data, s = load_golden(name)
+    base = np.ones(data.K) if s["weights"] is None else np.asarray(s["weights"], float)
+    w = base * (1.0 + (np.arange(data.K) % 3))                              # non-0/1 weights
+    n_folds = 5
+    fold = (np.arange(data.K) * 7 % n_folds).astype(np.int32)
+    variances = [float(s["variance"]), 2.0 * float(s["variance"])]
+    prior = api.PriorSpec(int(s["prior"]), 1.0, exclude_for(data))
+    ctl = api.create_control()
+    res = api.cv_grid_fit(data, prior, fold, n_folds, variances, ctl, weights=w)
+    octl = O.make_control()
+    for i, fit in enumerate(res.fits):
+        v, f = variances[i // n_folds], i % n_folds
+        train = np.where(fold == f, 0.0, w)
+        held = np.where(fold == f, w, 0.0)
+        ref = O.port().fit(data, int(s["prior"]), v, control=octl, weights=train)
+        assert fit.return_flag == ref.return_flag
+        assert abs(fit.iterations - ref.iterations) <= 1
+        if ref.return_flag != 0:                     # not converged: NaN, as the reference's driver records
+            assert np.isnan(res.pred_loglik[i])
+            continue
+        np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
+        want = O.port().predictive_loglik(data, ref.beta, held, weights=train)
+        assert abs(res.pred_loglik[i] - want) <= 1e-8 * abs(want), (i, res.pred_loglik[i], want)
