@@ -112,7 +112,7 @@ def test_cluster_sizes_agree(cuda_lib, cluster_size):
         assert np.max(np.abs(out[c] - out[1]) / np.maximum(np.abs(out[1]), 1.0)) < 1e-6, c
 
 
-@pytest.mark.parametrize("name", ["lr_normal_weighted", "pr_offset_normal", "clr_normal_weighted"])
+@pytest.mark.parametrize("name", ["lr_normal_weighted", "lr_laplace_small", "cpr_normal", "clr_normal_weighted"])
 def test_weighted_cv_grid_matches_oracle(cuda_lib, name):
     """Observation weights in CV (CrossValidationSelector with the fit's
     weights): each fold trains at the weights outside it and is scored at
