@@ -2158,6 +2158,15 @@ extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc
     return guarded([&] {
         NvtxRange range("cyc_batch_fit");
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
+        if (ctl->use_kkt_swindle) {
+            // every fit carries its own active set, which one batch kernel
+            // cannot share: each runs as cyc_fit
+            for (int f = 0; f < F; ++f) {
+                const int rc = cyc_fit(dsh, prior, &specs[f], ctl, &out[f]);
+                CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
+            }
+            return;
+        }
         run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, 0, nullptr, nullptr);
     });
 }
@@ -2173,6 +2182,13 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
         Dataset& ds = dsh->ds;
         for (int k = 0; k < ds.K; ++k)
             CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
+        if (ctl->use_kkt_swindle) {          // per-fit active sets: the per-fit path, unit weights
+            std::vector<double> ones(ds.K, 1.0);
+            const int rc = cyc_cv_grid_fit_weighted(dsh, prior, fold_of_row, n_folds, ones.data(), variances, n_var,
+                                                    ctl, out, pred_loglik, grid_mean);
+            CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
+            return;
+        }
         CYC_CHECK_CUDA(cudaSetDevice(ds.device));
         const int F = n_folds * n_var;
         std::vector<cyc_fit_spec> specs(F);
@@ -2405,7 +2421,14 @@ extern "C" int cyc_cv_grid_fit_weighted(cyc_dataset* dsh, const cyc_prior* prior
             specs[i].weights = train.data() + (size_t)(i % n_folds) * K;
             specs[i].variance = variances[i / n_folds];
         }
-        run_batch(ds, prior, specs.data(), F, ctl, out, nullptr, 0, nullptr, nullptr);
+        if (ctl->use_kkt_swindle) {          // per-fit active sets: each fit as cyc_fit
+            for (int i = 0; i < F; ++i) {
+                const int rc = cyc_fit(dsh, prior, &specs[i], ctl, &out[i]);
+                CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
+            }
+        } else {
+            run_batch(ds, prior, specs.data(), F, ctl, out, nullptr, 0, nullptr, nullptr);
+        }
         std::vector<double> pll(F);
         {
             Engine eng(&ds);

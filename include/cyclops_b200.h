@@ -177,8 +177,11 @@ typedef struct {
     int use_kkt_swindle;        /* useKktSwindle (CcdInterface.h:77): the active-set
                                    passes of CyclicCoordinateDescent::kktSwindle
                                    (CyclicCoordinateDescent.cpp:636-814) under a
-                                   Laplace prior; cyc_fit only, the batched
-                                   solvers return CYC_ERR_UNSUPPORTED */
+                                   Laplace prior.  Every fit keeps its own
+                                   active set, so cyc_batch_fit and the CV
+                                   grids run such fits one by one as cyc_fit;
+                                   cyc_cv_auto_search returns
+                                   CYC_ERR_UNSUPPORTED */
 } cyc_control;
 
 /* the prior: one default prior for every column, a flat prior on `exclude`

@@ -76,13 +76,45 @@ def test_swindle_warm_start_and_pass_limit(cuda_lib):
         np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
 
 
-def test_swindle_rejected_by_batched_solvers(cuda_lib):
-    from cyclops_b200 import api, _native
-    data, s = load_golden("lr_laplace_small")
+@pytest.mark.parametrize("name", ["swindle_lr_laplace_small", "swindle_clr_laplace"])
+def test_swindle_in_batched_fits(cuda_lib, name):
+    """cyc_batch_fit with the swindle runs each fit's own active-set passes
+    (one by one): every fit equals the reference's swindle fit."""
+    from cyclops_b200 import api
+    data, s = load_golden(name)
     prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    ctl = api.create_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                             use_kkt_swindle=True)
+    for fit in api.batch_fit(data, prior, [float(s["variance"])] * 2, control=ctl):
+        assert fit.return_flag == int(s["return_flag"])
+        assert abs(fit.iterations - int(s["iterations"])) <= 1
+        np.testing.assert_array_equal(fit.beta != 0, s["beta"] != 0)
+        err = np.abs(fit.beta - s["beta"]) / np.maximum(np.abs(s["beta"]), 1.0)
+        assert err.max() < 1e-4
+
+
+def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
+    """The CV grid with the swindle: each fold's fit and held-out log
+    likelihood as the restatement computes them with the swindle; the auto
+    search refuses the swindle."""
+    from cyclops_b200 import api, _native
+    from oracle import oracle as O
+    data, s = load_golden("swindle_lr_laplace_small")
+    prior = api.PriorSpec(int(s["prior"]), 1.0, exclude_for(data))
     ctl = api.create_control(use_kkt_swindle=True)
+    fold = (np.arange(data.K) % 4).astype(np.int32)
+    variances = [float(s["variance"])]
+    res = api.cv_grid_fit(data, prior, fold, 4, variances, ctl)
+    for f, fit in enumerate(res.fits):
+        train = (fold != f).astype(float)
+        ref = O.port().fit(data, int(s["prior"]), variances[0], control=O.make_control(use_kkt_swindle=1),
+                           weights=train)
+        assert abs(fit.iterations - ref.iterations) <= 1
+        np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
+        want = O.port().predictive_loglik(data, ref.beta, 1.0 - train, weights=train)
+        assert abs(res.pred_loglik[f] - want) <= 1e-8 * abs(want)
     with pytest.raises(_native.CyclopsError) as ei:
-        api.batch_fit(data, prior, [float(s["variance"])] * 2, control=ctl)
+        api.cv_auto_search(data, prior, fold, 4, control=ctl)
     assert ei.value.status == 4
 
 
