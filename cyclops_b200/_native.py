@@ -112,7 +112,7 @@ _SIGS = {
                                          C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p],
     "cyc_cv_grid_fit_weighted": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                  C.POINTER(Control), C.POINTER(FitResult), C.c_void_p, C.c_void_p],
-    "cyc_cv_auto_search": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_int, C.c_double,
+    "cyc_cv_auto_search": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double,
                            C.POINTER(Control), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_int, C.POINTER(C.c_int)],
     "cyc_profile_bounds": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_void_p,

@@ -386,12 +386,12 @@ class CvAutoResult:
 
 
 def cv_auto_search(data, prior: PriorSpec, fold_of_row, n_folds: int, starting_variance: float = -1.0,
-                   control: Optional[ControlSpec] = None, device: int = 0) -> CvAutoResult:
+                   control: Optional[ControlSpec] = None, device: int = 0, weights=None) -> CvAutoResult:
     """Auto-search cross-validation (createControl(cvType = "auto"), R's
     default; AutoSearchCrossValidationDriver): one variance per step, every
     fold refit on the GPU as one batched solve, the next variance proposed by
     the reference's unimodal search.  `fold_of_row`: K fold ids, or
-    (repetitions, K)."""
+    (repetitions, K); `weights`: K observation weights (as cv_grid_fit)."""
     ds = data if isinstance(data, Dataset) else Dataset(data, device)
     control = control or create_control()
     p, keep_ex = _prior_struct(ds.data, prior)
@@ -400,7 +400,8 @@ def cv_auto_search(data, prior: PriorSpec, fold_of_row, n_folds: int, starting_v
     bv, val, n = C.c_double(), C.c_double(), C.c_int()
     tv, tm, ts = np.zeros(64), np.zeros(64), np.zeros(64)
     c = _control_struct(control)
-    N.check(N.lib().cyc_cv_auto_search(ds.handle, C.byref(p), _ptr(folds), int(n_folds), int(n_reps),
+    w = None if weights is None else np.ascontiguousarray(weights, np.float64)
+    N.check(N.lib().cyc_cv_auto_search(ds.handle, C.byref(p), _ptr(folds), int(n_folds), int(n_reps), _ptr(w),
                                        float(starting_variance), C.byref(c), C.byref(bv), C.byref(val), _ptr(tv),
                                        _ptr(tm), _ptr(ts), 64, C.byref(n)))
     k = min(n.value, 64)

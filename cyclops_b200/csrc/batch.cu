@@ -2311,7 +2311,8 @@ double normal_based_default_variance(Dataset& ds) {
 }  // namespace
 
 extern "C" int cyc_cv_auto_search(cyc_dataset* dsh, const cyc_prior* prior, const int* fold_of_row, int n_folds,
-                                  int n_reps, double starting_variance, const cyc_control* ctl,
+                                  int n_reps, const double* row_weights, double starting_variance,
+                                  const cyc_control* ctl,
                                   double* best_variance, double* best_value, double* tried_variance,
                                   double* tried_mean, double* tried_sd, int max_tried, int* n_tried) {
     return guarded([&] {
@@ -2338,12 +2339,28 @@ extern "C" int cyc_cv_auto_search(cyc_dataset* dsh, const cyc_prior* prior, cons
         for (int f = 0; f < n_folds; ++f) fit_fold[f] = f;
         std::vector<double> betas((size_t)n_folds * J);
         std::vector<cyc_fit_result> out(n_folds);
+        std::vector<double> ones(row_weights ? 0 : ds.K, 1.0);
         cyc::VarianceSearch search;
         double value = 0.0;
         int tried = 0;
         for (int step = 0; step < 50; ++step) {            // MAX_STEPS, AutoSearchCrossValidationDriver.cpp:28
             std::vector<double> pll_all;
             for (int r = 0; r < n_reps; ++r) {
+                if (row_weights || ctl->use_kkt_swindle) {
+                    // observation weights or per-fit active sets: the weighted grid path
+                    std::vector<double> w(row_weights ? row_weights : ones.data(),
+                                          (row_weights ? row_weights : ones.data()) + ds.K);
+                    std::vector<double> pll(n_folds);
+                    for (int f = 0; f < n_folds; ++f) {
+                        out[f] = cyc_fit_result{};
+                        out[f].beta = betas.data() + (size_t)f * J;
+                    }
+                    const int rc = cyc_cv_grid_fit_weighted(dsh, prior, fold_of_row + (size_t)r * ds.K, n_folds,
+                                                            w.data(), &x, 1, ctl, out.data(), pll.data(), nullptr);
+                    CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
+                    pll_all.insert(pll_all.end(), pll.begin(), pll.end());
+                    continue;
+                }
                 std::vector<cyc_fit_spec> specs(n_folds);
                 for (int f = 0; f < n_folds; ++f) {
                     specs[f] = cyc_fit_spec{};

@@ -295,12 +295,16 @@ int cyc_cv_grid_fit_weighted(cyc_dataset* ds, const cyc_prior* prior, const int*
  * cold starts: the reference's resetCoefficients), takes the mean and
  * standard deviation of the held-out predictive log likelihoods (NaN folds
  * left out) and lets the search propose the next variance; at most 50
- * steps.  fold_of_row: n_reps x K fold ids (e.g. from cyc_cv_fold_weights).
+ * steps.  fold_of_row: n_reps x K fold ids (e.g. from cyc_cv_fold_weights);
+ * row_weights: K observation weights (NULL: all 1), used as
+ * cyc_cv_grid_fit_weighted uses them; with use_kkt_swindle the folds run
+ * one by one as cyc_fit.
  * Returns the variance the search settles on and its expected value, and
  * the first max_tried points tried (variance, mean, stdev; *n_tried counts
  * all). */
 int cyc_cv_auto_search(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds, int n_reps,
-                       double starting_variance, const cyc_control* control, double* best_variance,
+                       const double* row_weights, double starting_variance, const cyc_control* control,
+                       double* best_variance,
                        double* best_value, double* tried_variance, double* tried_mean, double* tried_sd,
                        int max_tried, int* n_tried);
 

@@ -31,3 +31,25 @@ def test_auto_search_matches_reference(cuda_lib, name):
     np.testing.assert_allclose(res.variance, float(z["best_variance"]), rtol=1e-6)
     np.testing.assert_allclose(res.expected, float(z["best_value"]), rtol=1e-6)
     np.testing.assert_allclose(res.tried, z["tried"], rtol=1e-5)
+
+
+def test_weighted_auto_search_matches_restatement(cuda_lib):
+    """Observation weights in the auto search: each step's folds train and
+    score at the weights (the selector's original weights)."""
+    from cyclops_b200 import api
+    from oracle import cv_auto
+    data, s = load_golden("lr_laplace_small")
+    w = 1.0 + (np.arange(data.K) % 3)
+    fold = (np.arange(data.K) * 7 % 5).astype(np.int32)
+    W = np.stack([np.where(fold == f, 0.0, w) for f in range(5)])
+
+    def fits(v, train, held_unit):
+        f = O.port().fit(data, int(s["prior"]), v, weights=train)
+        held = np.where(train == 0, w, 0.0)
+        return float("nan") if f.return_flag != 0 else O.port().predictive_loglik(data, f.beta, held, weights=train)
+
+    x, value, trail = cv_auto.auto_search(data, fits, 5, W)
+    prior = api.PriorSpec(int(s["prior"]), 1.0, exclude_for(data))
+    got = api.cv_auto_search(data, prior, fold, 5, weights=w)
+    np.testing.assert_allclose(got.variance, x, rtol=1e-6)
+    np.testing.assert_allclose(got.tried, np.array(trail), rtol=1e-6)

@@ -94,9 +94,9 @@ def test_swindle_in_batched_fits(cuda_lib, name):
 
 
 def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
-    """The CV grid with the swindle: each fold's fit and held-out log
-    likelihood as the restatement computes them with the swindle; the auto
-    search refuses the swindle."""
+    """The CV grid and the auto search with the swindle: each fold's fit and
+    held-out log likelihood as the restatement computes them with the
+    swindle."""
     from cyclops_b200 import api, _native
     from oracle import oracle as O
     data, s = load_golden("swindle_lr_laplace_small")
@@ -113,9 +113,19 @@ def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
         np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
         want = O.port().predictive_loglik(data, ref.beta, 1.0 - train, weights=train)
         assert abs(res.pred_loglik[f] - want) <= 1e-8 * abs(want)
-    with pytest.raises(_native.CyclopsError) as ei:
-        api.cv_auto_search(data, prior, fold, 4, control=ctl)
-    assert ei.value.status == 4
+    # the auto search with the swindle against the restated search over the
+    # restatement's swindle fits
+    from oracle import cv_auto
+    W = np.stack([(fold != f).astype(float) for f in range(4)])
+
+    def fits(v, w, held):
+        f = O.port().fit(data, int(s["prior"]), v, control=O.make_control(use_kkt_swindle=1), weights=w)
+        return float("nan") if f.return_flag != 0 else O.port().predictive_loglik(data, f.beta, held, weights=w)
+
+    x, value, trail = cv_auto.auto_search(data, fits, 4, W)
+    got = api.cv_auto_search(data, prior, fold, 4, control=ctl)
+    np.testing.assert_allclose(got.variance, x, rtol=1e-6)
+    np.testing.assert_allclose(got.tried, np.array(trail), rtol=1e-6)
 
 
 @pytest.mark.skipif(not os.path.exists(ADAPTER), reason="adapter harness not built (needs the reference sources)")
