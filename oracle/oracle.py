@@ -127,6 +127,8 @@ class _Lib:
             sigs["cv_weights"] = [C.c_int, V, C.c_int, C.c_long, C.c_int, C.c_int, V]
             sigs["fisher"] = [P(Problem), V, V, C.c_int, V, C.c_int]
             sigs["predictive_estimates"] = [P(Problem), V, V, V]
+            sigs["cv_grid"] = [P(Problem), P(Control), C.c_int, C.c_long, C.c_int, C.c_double, C.c_double, C.c_int,
+                               C.c_int, V, V, V]
             sigs["cv_auto"] = [P(Problem), P(Control), C.c_int, C.c_int, C.c_long, C.c_int, C.c_double, C.c_int,
                                P(C.c_double), P(C.c_double), V, V, V, C.c_int, P(C.c_int)]
             sigs["fit_device"] = [P(Problem), P(Control), V, P(Result), C.c_int]
@@ -247,6 +249,22 @@ class _Lib:
             raise RuntimeError(ref_dyn().err())
         k = n.value
         return bv.value, bval.value, np.stack([tv[:k], tm[:k], ts[:k]], axis=1)
+
+    def cv_grid(self, data, prior_type, fold=10, seed=123, by_row=True, lower=0.01, upper=20.0, grid_steps=10,
+                reset_coefficients=True, control: Optional[Control] = None, exclude=None, weights=None):
+        """GridSearchCrossValidationDriver run by the reference (one thread),
+        with `weights` as the fit's weights.  Returns (points, values,
+        fold_pred[grid_steps, fold])."""
+        p, keep = make_problem(data, prior_type, 1.0, exclude, weights)
+        c = control or make_control()
+        pts, vals = np.zeros(grid_steps), np.zeros(grid_steps)
+        fp = np.full(grid_steps * fold, np.nan)
+        rc = ref_dyn().lib.ref_cv_grid(C.byref(p), C.byref(c), int(fold), int(seed), int(by_row), float(lower),
+                                       float(upper), int(grid_steps), int(reset_coefficients), _ptr(pts), _ptr(vals),
+                                       _ptr(fp))
+        if rc:
+            raise RuntimeError(ref_dyn().err())
+        return pts, vals, fp.reshape(grid_steps, fold)
 
     def predictive_loglik(self, data, beta, held_out, weights=None):
         p, keep = make_problem(data, 1, 1.0, None, weights)

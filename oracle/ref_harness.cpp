@@ -46,6 +46,7 @@
 #include "priors/CovariatePrior.h"
 #include "drivers/CrossValidationSelector.h"
 #include "drivers/AutoSearchCrossValidationDriver.h"
+#include "drivers/GridSearchCrossValidationDriver.h"
 #include "CcdInterface.h"
 #include "io/ProgressLogger.h"
 
@@ -449,6 +450,14 @@ public:
     using AutoSearchCrossValidationDriver::AutoSearchCrossValidationDriver;
     MaxPoint best() const { return maxPoint; }
 };
+
+// the grid-search driver with its grid readable (protected members)
+class GridSearchProbe : public GridSearchCrossValidationDriver {
+public:
+    using GridSearchCrossValidationDriver::GridSearchCrossValidationDriver;
+    const std::vector<double>& points() const { return gridPoint; }
+    const std::vector<double>& values() const { return gridValue; }
+};
 }  // namespace
 
 extern "C" {
@@ -497,6 +506,52 @@ int ref_cv_auto(const ref_problem* p, const ref_control* c, int fold, int n_reps
             }
         }
         *n_tried = n;
+    });
+}
+
+int ref_cv_grid(const ref_problem* p, const ref_control* c, int fold, long seed, int by_row, double lower,
+                double upper, int grid_steps, int reset_coefficients, double* points, double* values,
+                double* fold_pred) {
+    return guarded([&] {
+        auto inst = build(p, 0);
+        CCDArguments args = CCDArguments();
+        args.modeFinding = toArguments(c);
+        args.threads = 1;
+        args.seed = seed;
+        args.resetCoefficients = reset_coefficients != 0;
+        args.useNormalPrior = p->prior_type == REF_PRIOR_NORMAL;
+        args.crossValidation.doCrossValidation = true;
+        args.crossValidation.useAutoSearchCV = false;
+        args.crossValidation.fold = fold;
+        args.crossValidation.foldToCompute = fold;
+        args.crossValidation.lowerLimit = lower;
+        args.crossValidation.upperLimit = upper;
+        args.crossValidation.gridSteps = grid_steps;
+        args.crossValidation.selectorType = by_row ? SelectorType::BY_ROW : SelectorType::BY_PID;
+        auto logger = bsccs::make_shared<RecordingLogger>();
+        auto err = bsccs::make_shared<ThrowingErrorHandler>();
+        // the fit's weights become the selector's original weights
+        // (CcdInterface::runCrossValidation, CcdInterface.cpp:738-754)
+        std::vector<double> original;
+        if (p->weights) original.assign(p->weights, p->weights + p->K);
+        std::vector<int> ids = inst->data->getPidVectorSTL();
+        CrossValidationSelector selector(fold, ids, args.crossValidation.selectorType, seed, logger, err, nullptr,
+                                         p->weights ? &original : nullptr);
+        GridSearchProbe driver(args, logger, err, nullptr);
+        driver.drive(*inst->ccd, selector, args);
+        for (int i = 0; i < grid_steps; ++i) {
+            points[i] = driver.points()[i];
+            values[i] = driver.values()[i];
+        }
+        // per-fold held-out log likelihoods from the driver's log (6 digits), NaN if not computed
+        int n = 0;
+        for (const auto& line : logger->lines) {
+            const auto a = line.find("pred log like = ");
+            if (a == std::string::npos || n >= grid_steps * fold) continue;
+            double v = NAN;
+            if (std::sscanf(line.c_str() + a, "pred log like = %lf", &v) != 1) v = NAN;
+            fold_pred[n++] = v;
+        }
     });
 }
 

@@ -129,4 +129,14 @@ int ref_profile_points(const ref_problem* p, const ref_control* c, const double*
 int ref_cv_auto(const ref_problem* p, const ref_control* c, int fold, int n_reps, long seed, int by_row,
                 double starting_variance, int reset_coefficients, double* best_variance, double* best_value,
                 double* tried_variance, double* tried_mean, double* tried_sd, int max_tried, int* n_tried);
+/* Grid-search cross-validation (GridSearchCrossValidationDriver,
+ * src/cyclops/drivers/GridSearchCrossValidationDriver.cpp:79-103) as
+ * CcdInterface::runCrossValidation runs it with one thread: grid_steps
+ * variances log-spaced over [lower, upper]; the problem's weights, when
+ * given, become the selector's original weights.  points / values: the grid
+ * and its mean held-out predictive log likelihood; fold_pred: grid_steps x
+ * fold per-fold values from the driver's log (6 significant digits). */
+int ref_cv_grid(const ref_problem* p, const ref_control* c, int fold, long seed, int by_row, double lower,
+                double upper, int grid_steps, int reset_coefficients, double* points, double* values,
+                double* fold_pred);
 #endif
