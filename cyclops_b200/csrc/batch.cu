@@ -1556,7 +1556,11 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
     P.dr0.assign(J, 0);
     P.nd.assign(J, 0);
     P.de_ptr.assign(J + 1, 0);
-    std::vector<int> stamp(K, -1), rlvl(K, 0), dslot(K, -1), first_w(K, 0), first_e(K, 0);
+    // per row: the batch that last touched it, its level, its shared-row slot
+    // and its first (column, entry) in that batch -- one struct per row, so
+    // the random row lookups of a column touch one cache line each
+    struct RowState { int stamp = -1, rlvl = 0, dslot = -1, first_w = 0, first_e = 0; };
+    std::vector<RowState> rs(K);
     struct Ent { int w, d, e; };
     std::vector<Ent> ents;
     std::vector<int> shared;            // row ids in order of their slots
@@ -1605,9 +1609,9 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
         int fresh = 0, level = 1;
         if (start >= 0)
             for (int e = 0; e < n; ++e)
-                if (stamp[rows[e]] == run_id) {
-                    fresh += dslot[rows[e]] < 0;
-                    level = std::max(level, rlvl[rows[e]] + 1);
+                if (rs[rows[e]].stamp == run_id) {
+                    fresh += rs[rows[e]].dslot < 0;
+                    level = std::max(level, rs[rows[e]].rlvl + 1);
                 }
         if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > kLevelMax)) {
             close();
@@ -1620,20 +1624,20 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
         const int w = len;
         for (int e = 0; e < n; ++e) {
             const int r = rows[e];
-            if (stamp[r] == run_id) {
-                if (dslot[r] < 0) {
-                    dslot[r] = (int)shared.size();
+            if (rs[r].stamp == run_id) {
+                if (rs[r].dslot < 0) {
+                    rs[r].dslot = (int)shared.size();
                     shared.push_back(r);
-                    ents.push_back({first_w[r], dslot[r], first_e[r]});
+                    ents.push_back({rs[r].first_w, rs[r].dslot, rs[r].first_e});
                 }
-                ents.push_back({w, dslot[r], e});
+                ents.push_back({w, rs[r].dslot, e});
             } else {
-                stamp[r] = run_id;
-                dslot[r] = -1;
-                first_w[r] = w;
-                first_e[r] = e;
+                rs[r].stamp = run_id;
+                rs[r].dslot = -1;
+                rs[r].first_w = w;
+                rs[r].first_e = e;
             }
-            rlvl[r] = level;
+            rs[r].rlvl = level;
         }
         P.len[j] = 0;
         P.lvl[j] = level;
