@@ -147,7 +147,10 @@ struct FitRunner {
 
     void set_beta(const std::vector<double>& b) {
         CYC_CHECK_CUDA(cudaMemcpyAsync(beta.get(), b.data(), J * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-        e.compute_xbeta_device(beta.get());
+        // all zero (a cold start without an offset): xbeta is zero, and the
+        // row-major copy the general case reads need not be built
+        if (std::all_of(b.begin(), b.end(), [](double v) { return v == 0.0; })) e.zero_xbeta();
+        else e.compute_xbeta_device(beta.get());
         e.sync();
     }
 
