@@ -365,7 +365,10 @@ int cyc_fit_host_loop(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spe
  *   stream: a cudaStream_t (NULL = the default stream).
  * At most 4,194,304 column entries per call; larger columns are rejected.
  * Runs on the calling thread's current device; the first call on a device
- * looks up the scratch address there, so make it before any stream capture.
+ * looks up the scratch address there, so make it before any stream capture,
+ * and during set-up, before the caller's own pool takes the GPU's memory:
+ * with lazy module loading that lookup can load the library's device code,
+ * which takes device memory.  Later calls allocate nothing.
  * Calls share the scratch: calls that overlap on the GPU race. */
 int cyc_gradient_hessian_noalloc(int model, int format, long long n, const int* rows,
                                  const double* values, const double* exb, const double* denom,

@@ -1,6 +1,7 @@
 import glob
 import os
 import sys
+import types
 
 import numpy as np
 import pytest
@@ -75,3 +76,35 @@ def rel_err(a, b, floor=1e-12):
     a = np.asarray(a, float)
     b = np.asarray(b, float)
     return np.abs(a - b) / np.maximum(np.abs(b), floor)
+
+
+# The precision contract of an FP64 path against an FP64 oracle run with the
+# same prior, variance, tolerance and convergence rule: the same return flag
+# and cycle count, the same zero pattern, beta within 1e-6 relative (1e-9
+# absolute around zero) and log likelihood within 1e-9 relative.
+BETA_RTOL = 1e-6
+BETA_ATOL = 1e-9
+LL_RTOL = 1e-9
+
+
+def golden_fit(s):
+    """The reference's fit stored in a fixture, as a fit record."""
+    return types.SimpleNamespace(beta=np.asarray(s["beta"], float), log_likelihood=float(s["log_likelihood"]),
+                                 iterations=int(s["iterations"]), return_flag=int(s["return_flag"]))
+
+
+def assert_contract(got, want, iterations=True, log_likelihood=True, what=""):
+    """`got` (beta, log_likelihood, iterations, return_flag) against `want`
+    under the precision contract; `iterations=False` drops the cycle count
+    (a path whose reported cycles are one phase's), `log_likelihood=False`
+    the likelihood (a record that carries none)."""
+    assert got.return_flag == want.return_flag, (what, got.return_flag, want.return_flag)
+    if iterations:
+        assert got.iterations == want.iterations, (what, got.iterations, want.iterations)
+    b, w = np.asarray(got.beta, float), np.asarray(want.beta, float)
+    np.testing.assert_array_equal(b != 0, w != 0, err_msg=str(what))
+    ok = np.abs(b - w) <= BETA_RTOL * np.abs(w) + BETA_ATOL
+    assert ok.all(), (what, float(np.max(np.abs(b - w) / (np.abs(w) + BETA_ATOL / BETA_RTOL))))
+    if log_likelihood:
+        assert rel_err(got.log_likelihood, want.log_likelihood) < LL_RTOL, (what, got.log_likelihood,
+                                                                             want.log_likelihood)

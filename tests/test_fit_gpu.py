@@ -1,20 +1,15 @@
 """Device-resident CCD (cyc_fit) and the drop-in adapter (the reference's
 own CyclicCoordinateDescent driving the CUDA engine) against the reference."""
 import os
+import types
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, exclude_for, golden_names, load_golden, rel_err
+from conftest import ROOT, assert_contract, exclude_for, golden_fit, golden_names, load_golden
 from cyclops_b200 import data as D
 
 pytestmark = pytest.mark.gpu
-
-# the precision contract: beta within 1e-6 relative (absolute 1e-9 around
-# zero; exact zeros must match as a support set), log likelihood 1e-9 relative
-BETA_RTOL = 1e-6
-BETA_ATOL = 1e-9
-LL_RTOL = 1e-9
 
 
 def _gpu_fit(data, s, tolerance=None, convergence=None, max_iterations=1000):
@@ -28,17 +23,10 @@ def _gpu_fit(data, s, tolerance=None, convergence=None, max_iterations=1000):
 
 @pytest.mark.parametrize("name", golden_names())
 def test_device_fit_matches_reference_fit(cuda_lib, name):
-    """Same prior, tolerance and convergence rule as the reference run."""
+    """Same prior, tolerance and convergence rule as the reference run: the
+    precision contract, cycle for cycle."""
     data, s = load_golden(name)
-    fit = _gpu_fit(data, s)
-    assert fit.return_flag == int(s["return_flag"])
-    assert abs(fit.iterations - int(s["iterations"])) <= 1
-    ref = s["beta"]
-    nz = ref != 0
-    np.testing.assert_array_equal(fit.beta != 0, nz)
-    err = np.abs(fit.beta - ref) / np.maximum(np.abs(ref), 1.0)
-    assert err.max() < 1e-4, err.max()
-    assert rel_err(fit.log_likelihood, float(s["log_likelihood"])) < 1e-6
+    assert_contract(_gpu_fit(data, s), golden_fit(s), what=name)
 
 
 @pytest.mark.parametrize("name", ["lr_c1", "pr_offset_normal", "clr_laplace", "cpr_normal",
@@ -51,11 +39,7 @@ def test_device_fit_tight_contract(cuda_lib, name):
     ctl = O.make_control(tolerance=1e-12, convergence_type=D.CONV_MITTAL, max_iterations=5000)
     ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
     fit = _gpu_fit(data, s, tolerance=1e-12, convergence=D.CONV_MITTAL, max_iterations=5000)
-    assert fit.iterations == ref.iterations
-    np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
-    ok = np.abs(fit.beta - ref.beta) <= BETA_RTOL * np.abs(ref.beta) + BETA_ATOL
-    assert ok.all(), np.max(np.abs(fit.beta - ref.beta) / (np.abs(ref.beta) + 1e-3))
-    assert rel_err(fit.log_likelihood, ref.log_likelihood) < LL_RTOL
+    assert_contract(fit, ref, what=name)
 
 
 ADAPTER = os.path.join(ROOT, "oracle", "_ref", "libcyclops_ref_cuda.so")
@@ -79,9 +63,6 @@ def test_reference_ccd_drives_cuda_engine(cuda_lib, name):
     r = O.Result(beta=beta.ctypes.data)
     rc = lib.ref_fit_device(C.byref(p), C.byref(ctl), None, C.byref(r), 1)
     assert rc == 0, lib.ref_last_error()
-    assert r.return_flag == int(s["return_flag"])
-    assert abs(r.iterations - int(s["iterations"])) <= 1
-    ref = s["beta"]
-    np.testing.assert_array_equal(beta != 0, ref != 0)
-    err = np.abs(beta - ref) / np.maximum(np.abs(ref), 1.0)
-    assert err.max() < 1e-4, err.max()
+    got = types.SimpleNamespace(beta=beta, log_likelihood=r.log_likelihood, iterations=r.iterations,
+                                return_flag=r.return_flag)
+    assert_contract(got, golden_fit(s), what=name)

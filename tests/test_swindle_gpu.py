@@ -6,11 +6,12 @@ the reference made, the restatement oracle at a tight tolerance, and the
 reference's own swindle driving the CUDA engine through the adapter."""
 import ctypes as C
 import os
+import types
 
 import numpy as np
 import pytest
 
-from conftest import ROOT, exclude_for, load_golden, rel_err, swindle_names
+from conftest import ROOT, assert_contract, exclude_for, golden_fit, load_golden, swindle_names
 from cyclops_b200 import data as D
 
 pytestmark = pytest.mark.gpu
@@ -32,14 +33,7 @@ def test_swindle_matches_reference_fixture(cuda_lib, name):
     """Same prior, tolerance and convergence rule as the reference's swindle
     run: flag, iterations of the last findMode, zero pattern, coefficients."""
     data, s = load_golden(name)
-    fit = _gpu_fit(data, s)
-    assert fit.return_flag == int(s["return_flag"])
-    assert abs(fit.iterations - int(s["iterations"])) <= 1
-    ref = s["beta"]
-    np.testing.assert_array_equal(fit.beta != 0, ref != 0)
-    err = np.abs(fit.beta - ref) / np.maximum(np.abs(ref), 1.0)
-    assert err.max() < 1e-4, err.max()
-    assert rel_err(fit.log_likelihood, float(s["log_likelihood"])) < 1e-6
+    assert_contract(_gpu_fit(data, s), golden_fit(s), what=name)
 
 
 @pytest.mark.parametrize("name", ["swindle_lr_c1", "swindle_pr_laplace_weighted", "swindle_clr_laplace",
@@ -52,12 +46,7 @@ def test_swindle_tight_contract(cuda_lib, name):
     ctl = O.make_control(tolerance=1e-12, convergence_type=D.CONV_MITTAL, max_iterations=5000, use_kkt_swindle=1)
     ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, weights=s["weights"])
     fit = _gpu_fit(data, s, tolerance=1e-12, convergence=D.CONV_MITTAL, max_iterations=5000)
-    assert fit.iterations == ref.iterations
-    assert fit.return_flag == ref.return_flag
-    np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
-    ok = np.abs(fit.beta - ref.beta) <= 1e-6 * np.abs(ref.beta) + 1e-9
-    assert ok.all(), np.max(np.abs(fit.beta - ref.beta) / (np.abs(ref.beta) + 1e-3))
-    assert rel_err(fit.log_likelihood, ref.log_likelihood) < 1e-9
+    assert_contract(fit, ref, what=name)
 
 
 def test_swindle_warm_start_and_pass_limit(cuda_lib):
@@ -70,10 +59,7 @@ def test_swindle_warm_start_and_pass_limit(cuda_lib):
         ctl = O.make_control(tolerance=1e-8, max_iterations=max_it, use_kkt_swindle=1)
         ref = O.port().fit(data, int(s["prior"]), float(s["variance"]), control=ctl, start=start)
         fit = _gpu_fit(data, s, tolerance=1e-8, max_iterations=max_it, start=start)
-        assert fit.return_flag == ref.return_flag
-        assert fit.iterations == ref.iterations
-        np.testing.assert_array_equal(fit.beta != 0, ref.beta != 0)
-        np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
+        assert_contract(fit, ref, what=max_it)
 
 
 @pytest.mark.parametrize("name", ["swindle_lr_laplace_small", "swindle_clr_laplace"])
@@ -86,11 +72,7 @@ def test_swindle_in_batched_fits(cuda_lib, name):
     ctl = api.create_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
                              use_kkt_swindle=True)
     for fit in api.batch_fit(data, prior, [float(s["variance"])] * 2, control=ctl):
-        assert fit.return_flag == int(s["return_flag"])
-        assert abs(fit.iterations - int(s["iterations"])) <= 1
-        np.testing.assert_array_equal(fit.beta != 0, s["beta"] != 0)
-        err = np.abs(fit.beta - s["beta"]) / np.maximum(np.abs(s["beta"]), 1.0)
-        assert err.max() < 1e-4
+        assert_contract(fit, golden_fit(s), what=name)
 
 
 def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
@@ -109,8 +91,7 @@ def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
         train = (fold != f).astype(float)
         ref = O.port().fit(data, int(s["prior"]), variances[0], control=O.make_control(use_kkt_swindle=1),
                            weights=train)
-        assert abs(fit.iterations - ref.iterations) <= 1
-        np.testing.assert_allclose(fit.beta, ref.beta, rtol=1e-6, atol=1e-9)
+        assert_contract(fit, ref, what=f)
         want = O.port().predictive_loglik(data, ref.beta, 1.0 - train, weights=train)
         assert abs(res.pred_loglik[f] - want) <= 1e-8 * abs(want)
     # the auto search with the swindle against the restated search over the
@@ -144,9 +125,6 @@ def test_reference_swindle_drives_cuda_engine(cuda_lib, name):
     beta = np.zeros(data.J)
     r = O.Result(beta=beta.ctypes.data)
     assert lib.ref_fit_device(C.byref(p), C.byref(ctl), None, C.byref(r), 1) == 0, lib.ref_last_error()
-    assert r.return_flag == int(s["return_flag"])
-    assert abs(r.iterations - int(s["iterations"])) <= 1
-    ref = s["beta"]
-    np.testing.assert_array_equal(beta != 0, ref != 0)
-    err = np.abs(beta - ref) / np.maximum(np.abs(ref), 1.0)
-    assert err.max() < 1e-4, err.max()
+    got = types.SimpleNamespace(beta=beta, log_likelihood=r.log_likelihood, iterations=r.iterations,
+                                return_flag=r.return_flag)
+    assert_contract(got, golden_fit(s), what=name)
