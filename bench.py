@@ -63,9 +63,22 @@ def workload(quick: bool):
 
 
 def fold_ids(K: int, seed: int) -> np.ndarray:
+    """Fold id per row, drawn by this library's restatement of the
+    reference's CrossValidationSelector (bit-exact with it)."""
     from cyclops_b200 import api
     masks = api.cv_fold_weights(K, N_FOLDS, seed)
     return api.fold_ids_from_weights(masks)
+
+
+def ref_fold_ids(K: int, seed: int) -> np.ndarray:
+    """The same fold ids drawn by the reference's own CrossValidationSelector
+    (the reference engine compiled from its sources), so that the reference
+    arm loads nothing of this library."""
+    from oracle import oracle as O
+    masks = O.ref_cv_weights(K, np.arange(K, dtype=np.int32), N_FOLDS, seed)
+    held = masks == 0
+    assert np.all(held.sum(axis=0) == 1)
+    return np.argmax(held, axis=0).astype(np.int32)
 
 
 class Clocks:
@@ -233,7 +246,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     data, lambdas, variances, desc, _ = workload(args.quick)
-    folds = fold_ids(data.K, FOLD_SEED)
+    folds = ref_fold_ids(data.K, FOLD_SEED)
     threads = os.cpu_count() or 1
     ids = sample_ids(threads)
     # warm-up steps run two cycles per fit (page-in, thread start-up); timed
@@ -262,6 +275,198 @@ def run_reference(args):
     }
     print(json.dumps(line))
     return 0
+
+
+# --------------------------------------------------------------------------
+# further measurements at N = 1 (rank 0 only, after the timed region): the
+# single-fit denominators, the mixed-precision scheme, the Poisson and Cox
+# workloads and the request stream.  Each is bounded in time and reports its
+# own sample; none of it enters `value`.
+# --------------------------------------------------------------------------
+
+def roofline_of(bytes_, ms, kernel, note=None):
+    peak, kind = peaks()
+    gbs = bytes_ / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+    out = {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+           "peak_source": kind, "kernel": kernel, "algorithmic_bytes": bytes_, "ms": ms}
+    if note:
+        out["note"] = note
+    return out
+
+
+def cpu_ref():
+    from oracle import oracle as O
+    return (O.ref(), "reference") if O.have_ref() else (O.port(), "port")
+
+
+def leg_single_fits(api, ds, folds, variances, mean_cycles, value):
+    """The single-fit denominators of the batched grid, on one fit of it (the
+    middle of the lambda grid, fold 0): the plain FP64 host-driven CCD
+    (cyc_fit_host_loop, 2 cycles timed) and the device-resident CCD (cyc_fit,
+    one whole fit timed).  Both are put on the batch's footing as fits/s =
+    1 / (seconds per cycle x the batch's mean cycles per fit)."""
+    i0 = (N_LAMBDA // 2) * N_FOLDS
+    w = (folds != (i0 % N_FOLDS)).astype(np.float64)
+    pr = api.PriorSpec(D.PRIOR_LAPLACE, float(variances[i0 // N_FOLDS]), [0])
+    out = {}
+    t0 = time.perf_counter()
+    api.fit_cyclops_model(ds, pr, api.create_control(max_iterations=2), weights=w, host_loop=True)
+    per_cycle = (time.perf_counter() - t0) / 2.0
+    plain = 1.0 / (per_cycle * mean_cycles)
+    out["plain_fp64_gpu_ccd"] = {"fits_per_s": plain, "seconds_per_cycle": per_cycle,
+                                 "sample": "1 fit of the grid (middle lambda, fold 0), 2 cycles timed, "
+                                           "scaled by the batch's mean cycles per fit"}
+    out["speedup_vs_plain_fp64_gpu_ccd"] = value / plain
+    api.fit_cyclops_model(ds, pr, api.create_control(max_iterations=1), weights=w)       # warm-up
+    t0 = time.perf_counter()
+    fit = api.fit_cyclops_model(ds, pr, api.create_control(), weights=w)
+    wall = time.perf_counter() - t0
+    st = api.last_run_stats()
+    spc = wall / max(1, fit.iterations)
+    dev = 1.0 / (spc * mean_cycles)
+    out["device_single_fit_ccd"] = {
+        "fits_per_s": dev, "seconds_per_fit": wall, "cycles": fit.iterations, "seconds_per_cycle": spc,
+        "raw_fits_per_s": 1.0 / wall,
+        "roofline": roofline_of(st["phase_bytes"][0], st["kernel_ms"], "cyc_fit: every kernel of the fit"),
+        "sample": "1 whole fit of the grid (middle lambda, fold 0) through cyc_fit: the CCD loop on the device, "
+                  "kernels per coordinate replayed as CUDA graphs; fits_per_s scaled by the batch's mean cycles"}
+    out["speedup_vs_device_single_fit_ccd"] = value / dev
+    return out
+
+
+def leg_mixed(api, ds, prior, folds, variances, control, res64):
+    """The precision scheme of the target: FP32 linear predictors with
+    compensated sums to a relative objective change of 1e-4, then the FP64
+    polish to the requested tolerance; one grid solve after one warm-up."""
+    ctl = api.create_control(tolerance=control.tolerance, precision="mixed", polish_tolerance=1e-4,
+                             max_iterations=control.max_iterations)
+    api.cv_grid_fit(ds, prior, folds, N_FOLDS, variances, ctl)
+    t0 = time.perf_counter()
+    r = api.cv_grid_fit(ds, prior, folds, N_FOLDS, variances, ctl)
+    wall = time.perf_counter() - t0
+    st = api.last_run_stats()
+    F = N_FOLDS * N_LAMBDA
+    err = max(float(np.max(np.abs(a.beta - b.beta) / np.maximum(np.abs(b.beta), 1.0)))
+              for a, b in zip(r.fits, res64.fits))
+    out = {"fits_per_s": F / wall, "seconds_per_step": wall, "kernel_ms": st["kernel_ms"],
+           "phase_ms": st["phase_ms"][:st["phases"]],
+           "mean_cycles_fp64_phase": float(np.mean([f.iterations for f in r.fits])),
+           "converged": int(sum(f.return_flag == 0 for f in r.fits)),
+           "max_rel_err_beta_vs_fp64_grid": err}
+    for p, name in zip(range(st["phases"]), ("fp32_phase", "fp64_phase")):
+        kern = f"k_batch<{'float' if st['phase_state_bytes'][p] == 4 else 'double'},LR,8>"
+        out["roofline_" + name] = roofline_of(st["phase_bytes"][p], st["phase_ms"][p], kern)
+    return out
+
+
+def leg_poisson(api):
+    """Poisson regression at full size: K = 1M rows, an offset log(t)
+    (t ~ Exp(1)), an intercept, 10 dense N(0,1) columns and 100k indicator
+    columns with 50 distinct Zipf(1.1)-ranked columns per row (50M entries),
+    normal prior of variance 1, default control.  One fit through the
+    persistent solver (cyc_batch_fit, one fit) to convergence or a 90 s cap,
+    2 cycles of cyc_fit, and 2 cycles of the reference engine on one host
+    thread."""
+    t0 = time.perf_counter()
+    data = D.synth_poisson()
+    gen = time.perf_counter() - t0
+    ds = api.Dataset(data, 0)
+    prior = api.PriorSpec(D.PRIOR_NORMAL, 1.0, None)
+    out = {"workload": "poisson: K=1,000,000, J=100,012 (offset log t, intercept, 10 dense N(0,1), 100k indicators "
+                       "Zipf(1.1) 50 per row), normal prior variance 1, seed 2",
+           "stored_entries": data.nnz, "generation_s": gen}
+    api.batch_fit(ds, prior, [1.0], None, api.create_control(max_iterations=1))
+    c1 = api.last_run_stats()["kernel_ms"]
+    cap = int(min(1000, max(2, 90_000.0 / max(c1, 1e-3))))
+    t0 = time.perf_counter()
+    fit = api.batch_fit(ds, prior, [1.0], None, api.create_control(max_iterations=cap))[0]
+    wall = time.perf_counter() - t0
+    st = api.last_run_stats()
+    out["persistent_fit"] = {
+        "cycles": fit.iterations, "return_flag": fit.return_flag, "cycle_cap": cap, "seconds": wall,
+        "kernel_ms": st["kernel_ms"], "seconds_per_cycle": st["kernel_ms"] / 1000.0 / max(1, fit.iterations),
+        "roofline": roofline_of(st["phase_bytes"][0], st["phase_ms"][0], "k_batch<double,PR,1> (one fit)")}
+    api.fit_cyclops_model(ds, prior, api.create_control(max_iterations=1))
+    f2 = api.fit_cyclops_model(ds, prior, api.create_control(max_iterations=2))
+    st2 = api.last_run_stats()
+    out["cyc_fit"] = {"seconds_per_cycle": st2["kernel_ms"] / 1000.0 / max(1, f2.iterations),
+                      "roofline": roofline_of(st2["phase_bytes"][0], st2["kernel_ms"],
+                                              "cyc_fit: every kernel of 2 cycles")}
+    lib, kind = cpu_ref()
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    lib.fit(data, D.PRIOR_NORMAL, 1.0, control=O.make_control(max_iterations=2), exclude=[1])
+    cpu = (time.perf_counter() - t0) / 2.0
+    out["cpu_baseline"] = {"seconds_per_cycle": cpu, "cores": 1, "kind": kind,
+                           "sample": "2 cycles of the same fit from beta 0 (includes the engine's set-up)"}
+    out["speedup_per_cycle_vs_cpu"] = cpu / out["persistent_fit"]["seconds_per_cycle"]
+    ds.close()
+    return out
+
+
+def leg_cox(api, n_strata=0):
+    """Breslow Cox at full size: K = 2M rows sorted by descending time, 50k
+    sparse N(0,1) columns at 0.05 % (50M entries), Weibull(1.2) times, 70 %
+    censoring, Laplace rate 0.1 (variance 200), default control; one whole
+    fit through cyc_fit after a 1-cycle warm-up.  The reference engine's
+    cycle costs O(N) per coordinate (about 2M x 50k); it is timed for one
+    cycle on the first 500 columns (same rows, one host thread) and scaled
+    by the column count."""
+    t0 = time.perf_counter()
+    data = D.synth_cox(n_strata=n_strata)
+    gen = time.perf_counter() - t0
+    ds = api.Dataset(data, 0)
+    var = D.laplace_variance(0.1)
+    prior = api.PriorSpec(D.PRIOR_LAPLACE, var, [])
+    out = {"workload": (f"breslow cox: K=2,000,000, J=50,000 sparse N(0,1) at 0.05%, Weibull(1.2), 70% censored, "
+                        f"{n_strata or 'no'} strata, laplace lambda 0.1 (variance 200), seed 3"),
+           "stored_entries": data.nnz, "generation_s": gen}
+    api.fit_cyclops_model(ds, prior, api.create_control(max_iterations=1))
+    t0 = time.perf_counter()
+    fit = api.fit_cyclops_model(ds, prior, api.create_control())
+    wall = time.perf_counter() - t0
+    st = api.last_run_stats()
+    spc = st["kernel_ms"] / 1000.0 / max(1, fit.iterations)
+    out["device_fit"] = {"cycles": fit.iterations, "return_flag": fit.return_flag, "seconds": wall,
+                         "kernel_ms": st["kernel_ms"], "seconds_per_cycle": spc,
+                         "update_entries": st["update_entries"],
+                         "roofline": roofline_of(st["phase_bytes"][0], st["kernel_ms"],
+                                                 "cyc_fit cox kernels (numerator, gradient, update, risk-set rescans)")}
+    sub = 500
+    from cyclops_b200.data import CyclopsData
+    sd = CyclopsData(model=data.model, y=data.y, col_format=data.col_format[:sub], col_ptr=data.col_ptr[:sub + 1],
+                     col_idx=data.col_idx[:int(data.col_ptr[sub])], val_ptr=data.val_ptr[:sub + 1],
+                     col_val=data.col_val[:int(data.val_ptr[sub])], pid=data.pid, time=data.time)
+    lib, kind = cpu_ref()
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    lib.fit(sd, D.PRIOR_LAPLACE, var, control=O.make_control(max_iterations=1), exclude=[])
+    cpu = (time.perf_counter() - t0) * data.J / sub
+    out["cpu_baseline"] = {"seconds_per_cycle": cpu, "cores": 1, "kind": kind,
+                           "sample": f"1 cycle over the first {sub} columns (all 2M rows), scaled by J/{sub}"}
+    out["speedup_per_cycle_vs_cpu"] = cpu / spc
+    ds.close()
+    return out
+
+
+def leg_serving():
+    """The request stream (2,000 requests at 50/s in full), bounded: its first
+    120 requests (about 2.4 s of arrivals), admitted for at most 60 s, stored
+    entries capped at 4M per request (density scaled down above that)."""
+    from cyclops_b200 import serving
+    n, window = 120, 60.0
+    t0 = time.perf_counter()
+    reqs = serving.request_stream(n, 50.0, seed=7, max_entries=4_000_000)
+    gen = time.perf_counter() - t0
+    server = serving.Server(slots=16)
+    t0 = time.monotonic()
+    res = server.run(reqs, realtime=True, deadline=window)
+    wall = time.monotonic() - t0
+    out = serving.summarize(res, wall)
+    out.update({"offered": n, "admitted": n - out["not_admitted"], "rate_per_s": 50.0, "admission_window_s": window,
+                "max_entries_per_request": 4_000_000, "generation_s": gen,
+                "sample": f"first {n} requests of the 2,000-request stream (seed 7)"})
+    return out
 
 
 # --------------------------------------------------------------------------
@@ -376,8 +581,10 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-            "config": dict(desc, precision=args.precision, mean_cycles_per_fit=mean_cycles,
-                           converged=int(sum(f.return_flag == 0 for f in res.fits))),
+            "config": desc,
+            "run": {"precision": args.precision, "mean_cycles_per_fit": mean_cycles,
+                    "max_cycles_per_fit": int(max(f.iterations for f in res.fits)),
+                    "converged": int(sum(f.return_flag == 0 for f in res.fits))},
             "clocks": clocks,
             "e2e": {"value": e2e, "unit": "fits/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
@@ -388,18 +595,7 @@ def run_ours(args):
         }
     rep.barrier()
     if rank == 0 and world == 1 and not args.no_baselines:
-        # plain FP64 single-fit GPU CCD (host-driven loop): 2 cycles of one fit
-        i0 = sample_ids(1)[0]
-        w = (folds != (i0 % N_FOLDS)).astype(np.float64)
-        ctl2 = api.create_control(tolerance=1e-6, max_iterations=2)
-        pr = api.PriorSpec(D.PRIOR_LAPLACE, float(variances[i0 // N_FOLDS]), [0])
-        t0 = time.perf_counter()
-        api.fit_cyclops_model(ds, pr, ctl2, weights=w, host_loop=True)
-        per_cycle = (time.perf_counter() - t0) / 2.0
-        plain = 1.0 / (per_cycle * mean_cycles)
-        line["plain_fp64_gpu_ccd"] = {"fits_per_s": plain, "seconds_per_cycle": per_cycle,
-                                      "sample": "1 fit, 2 cycles timed, scaled by the batch's mean cycles per fit"}
-        line["speedup_vs_plain_fp64_gpu_ccd"] = value / plain
+        line.update(leg_single_fits(api, ds, folds, variances, mean_cycles, value))
         # CPU baseline on a bounded sample; checks our fits against it
         threads = os.cpu_count() or 1
         ids = sample_ids(min(threads, 16))
@@ -411,6 +607,29 @@ def run_ours(args):
         line["cpu_baseline"] = {"value": len(ids) / dt, "unit": "fits/s", "cores": min(threads, 16), "kind": kind,
                                 "sample": f"{len(ids)} fits of the grid, one per thread"}
         line["check"] = {"fits_compared": len(ids), "max_rel_err_beta_vs_cpu": err}
+    if rank == 0 and world == 1 and args.extras != "none":
+        legs = args.extras.split(",") if args.extras != "all" else \
+            ["mixed", "poisson", "cox", "cox_strata", "serving"]
+        extra = {}
+        t_extra = time.perf_counter()
+        for leg in legs:
+            t_leg = time.perf_counter()
+            try:
+                if leg == "mixed":
+                    extra[leg] = leg_mixed(api, ds, prior, folds, variances, control, res)
+                elif leg == "poisson":
+                    extra[leg] = leg_poisson(api)
+                elif leg in ("cox", "cox_strata"):
+                    extra[leg] = leg_cox(api, n_strata=10_000 if leg == "cox_strata" else 0)
+                elif leg == "serving":
+                    extra[leg] = leg_serving()
+                else:
+                    extra[leg] = {"error": "unknown leg"}
+            except Exception as e:     # a failed leg is reported; the line still prints
+                extra[leg] = {"error": f"{type(e).__name__}: {e}"}
+            extra[leg]["leg_wall_s"] = round(time.perf_counter() - t_leg, 1)
+        line["workloads"] = extra
+        line["workloads_wall_s"] = round(time.perf_counter() - t_extra, 1)
     if rank == 0:
         print(json.dumps(line))
     rep.close()
@@ -432,6 +651,9 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true", help="device-resident timing only (profiling runs)")
     ap.add_argument("--max-iterations", type=int, default=1000,
                     help="cap on CCD cycles per fit (the reference default is 1000)")
+    ap.add_argument("--extras", default="all",
+                    help="further measurements at N=1: all, none, or a comma list of "
+                         "mixed,poisson,cox,cox_strata,serving")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

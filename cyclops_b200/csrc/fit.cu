@@ -32,7 +32,10 @@ __global__ void k_step(int j, const double* __restrict__ gh, StepState st) {
     delta = apply_bounds(st.hdelta + j, delta);
     if (delta != 0.0) st.beta[j] = beta + delta;
     *st.delta = delta;
-    if (delta != 0.0) atomicAdd(st.n_updates, 1ull);
+    if (delta != 0.0) {
+        atomicAdd(st.n_updates, 1ull);
+        if (st.col_updates) st.col_updates[j] += 1u;
+    }
 }
 
 // performCheckConvergence (CyclicCoordinateDescent.cpp:839-906) for the
@@ -96,6 +99,7 @@ struct FitRunner {
     DevBuf<double> beta, hdelta, gh, delta, obj, last;
     DevBuf<int> ptype, flags;
     DevBuf<unsigned long long> n_updates;
+    DevBuf<unsigned> col_updates;        // per column: coordinate steps that moved beta
     double variance;
     PinnedBlock h_block;                 // two flags read back per cycle (pinned, pooled)
     int* h_flags = h_block.as<int>();
@@ -121,9 +125,10 @@ struct FitRunner {
             pt[prior.exclude[i]] = CYC_PRIOR_NONE;
         }
         beta.alloc(J); hdelta.alloc(J); gh.alloc(2); delta.alloc(1); obj.alloc(1); last.alloc(1);
-        ptype.alloc(J); flags.alloc(2); n_updates.alloc(1);
+        ptype.alloc(J); flags.alloc(2); n_updates.alloc(1); col_updates.alloc(J);
         CYC_CHECK_CUDA(cudaMemcpyAsync(ptype.get(), pt.data(), J * sizeof(int), cudaMemcpyHostToDevice, e.stream));
         CYC_CHECK_CUDA(cudaMemsetAsync(n_updates.get(), 0, sizeof(unsigned long long), e.stream));
+        CYC_CHECK_CUDA(cudaMemsetAsync(col_updates.get(), 0, J * sizeof(unsigned), e.stream));
         CYC_CHECK_CUDA(cudaEventCreate(&ev0));
         CYC_CHECK_CUDA(cudaEventCreate(&ev1));
         e.sync();
@@ -142,6 +147,7 @@ struct FitRunner {
         s.prior_type = ptype.get();
         s.variance = variance;
         s.n_updates = n_updates.get();
+        s.col_updates = col_updates.get();
         return s;
     }
 
@@ -359,6 +365,50 @@ struct FitRunner {
         out->return_flag = flag;
     }
 
+    // Algorithmic bytes of the coordinate loop (the bytes the algorithm must
+    // move; FP64 state s = 8, s_x = 8 for real-valued columns and 0 for
+    // indicators, w = 8 with row weights), per column j with nnz_j entries:
+    //   lr / pr   gradient nnz_j (4 + s_x + s + w), update nnz_j (4 + s_x + 3 s);
+    //   clr / cpr the same plus 16 B per stratum the column touches (at most
+    //             one per entry) for the gradient and for an update;
+    //   cox       numerator scatter nnz_j (4 + s_x + s + w) + 16 g_j, gradient
+    //             32 g_j (the two double-double prefix sums at the g_j groups
+    //             the column touches), update nnz_j (4 + s_x + 3 s + w)
+    //             + 16 g_j and the rescan of the groups from the column's first
+    //             to N at 56 B a group (denominator and group weight read; the
+    //             accumulated denominator and two double-double prefix sums
+    //             written).
+    // Gradients count once per cycle for every column not fixed, updates once
+    // per step that moved beta; each convergence check reads K (2 s + 8).
+    double algorithmic_bytes(int iters, const std::vector<unsigned>& upd) const {
+        const Dataset& ds = *e.ds;
+        const int K = ds.K;
+        const double w = e.use_w ? 8.0 : 0.0;
+        double bytes = (double)(iters + 1) * K * (2 * 8.0 + 8.0);
+        for (int j = 0; j < J; ++j) {
+            if (fixb[j]) continue;
+            const int f = ds.fmt[j];
+            const bool dense = (f == CYC_DENSE || f == CYC_INTERCEPT);
+            const double n = dense ? (double)K : (double)(ds.col_ptr[j + 1] - ds.col_ptr[j]);
+            const double sx = (f == CYC_INDICATOR || f == CYC_INTERCEPT) ? 0.0 : 8.0;
+            const double si = dense ? 0.0 : 4.0;
+            double grad, upd_b;
+            if (model_cumulative(ds.model)) {
+                const double g = (double)(e.h_glist_ptr[j + 1] - e.h_glist_ptr[j]);
+                grad = n * (si + sx + 8.0 + w) + 16.0 * g + 32.0 * g;
+                upd_b = n * (si + sx + 24.0 + w) + 16.0 * g + 56.0 * (double)std::max(0, e.N - e.first_group(j));
+            } else if (model_grouped(ds.model)) {
+                grad = n * (si + sx + 8.0 + w) + 16.0 * n;
+                upd_b = n * (si + sx + 24.0) + 16.0 * n;
+            } else {
+                grad = n * (si + sx + 8.0 + w);
+                upd_b = n * (si + sx + 24.0);
+            }
+            bytes += (double)iters * grad + (double)upd[j] * upd_b;
+        }
+        return bytes;
+    }
+
     void run(cyc_fit_result* out) {
         prepare();
         CYC_CHECK_CUDA(cudaEventRecord(ev0, e.stream));
@@ -368,6 +418,10 @@ struct FitRunner {
         results(out, flag, iters);
         float ms = 0.f;
         CYC_CHECK_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        std::vector<unsigned> upd(J);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(upd.data(), col_updates.get(), J * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                       e.stream));
+        e.sync();
         cyc_run_stats st{};
         st.kernel_ms = ms;
         st.coordinate_steps = (double)iters * J;
@@ -375,6 +429,17 @@ struct FitRunner {
         st.phases = 1;
         st.phase_ms[0] = ms;
         st.phase_state_bytes[0] = 8;
+        // the swindle's passes run findMode over changing active sets: not counted
+        st.algorithmic_bytes = swindle ? 0.0 : algorithmic_bytes(iters, upd);
+        st.phase_bytes[0] = st.algorithmic_bytes;
+        for (int j = 0; j < J; ++j) {
+            if (fixb[j]) continue;
+            const int f = e.ds->fmt[j];
+            const double n = (f == CYC_DENSE || f == CYC_INTERCEPT) ? (double)e.ds->K
+                                                                    : (double)(e.ds->col_ptr[j + 1] - e.ds->col_ptr[j]);
+            st.gradient_entries += (double)iters * n;
+            st.update_entries += (double)upd[j] * n;
+        }
         set_last_stats(st);
     }
 

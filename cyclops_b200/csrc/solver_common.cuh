@@ -12,6 +12,7 @@ struct StepState {
     const int* prior_type;           // J (flat prior on excluded columns)
     double variance;
     unsigned long long* n_updates;   // steps with delta != 0
+    unsigned* col_updates;           // J: steps with delta != 0 per column (null: not counted)
 };
 
 __host__ __device__ inline int sgn(double x) { return x == 0 ? 0 : (x < 0 ? -1 : 1); }
