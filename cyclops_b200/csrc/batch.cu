@@ -542,6 +542,136 @@ __device__ __forceinline__ void batch_update(T* xbg, const int* idx, const doubl
     }
 }
 
+// The batch cache: a batch of short columns whose entries in this CTA's rows
+// number at most kRows (the planner caps batches so) is gathered once into
+// shared memory -- every entry's row of linear predictors (all G fits, by
+// 16-byte cp.async), its row id, value and fold id -- with all copies in
+// flight at once, so the batch pays one memory round trip; the gradient
+// partials then read shared memory and the update writes the new values from
+// it without reading global memory again.  It occupies the bytes the
+// cp.async row slots of the single-column path use (kAsyncBytes).
+template <class T, int G>
+struct BatchCache {
+    static constexpr int kPieces = (int)(G * sizeof(T)) / 16;          // 16-byte pieces of a row
+    static constexpr int kEntryBytes = (int)(G * sizeof(T) + sizeof(int) + sizeof(T) + 1);
+    static constexpr int kRows = (kAsyncBytes / kEntryBytes) / 32 * 32;
+    static_assert(kPieces >= 1 && (G * sizeof(T)) % 16 == 0, "rows are whole 16-byte pieces");
+    static_assert(kRows * kEntryBytes <= kAsyncBytes, "the batch cache exceeds its shared memory");
+    T* v;                  // [kRows][G] linear predictors at the batch's start
+    int* row;              // [kRows] row ids
+    T* x;                  // [kRows] values (1 for indicators)
+    unsigned char* fold;   // [kRows] fold ids (CV grid)
+    __device__ explicit BatchCache(void* base) {
+        unsigned char* b = static_cast<unsigned char*>(base);
+        v = reinterpret_cast<T*>(b);
+        row = reinterpret_cast<int*>(b + (size_t)kRows * G * sizeof(T));
+        x = reinterpret_cast<T*>(b + (size_t)kRows * (G * sizeof(T) + sizeof(int)));
+        fold = b + (size_t)kRows * (G * sizeof(T) + sizeof(int) + sizeof(T));
+    }
+};
+
+// Gather the batch's entries in this CTA's rows (columns q .. q+L-1, entry
+// offsets boff[0..L]) into the cache; returns after every copy has landed
+// and the CTA has synchronised.
+template <class T, int G, int WM>
+__device__ __forceinline__ void batch_gather(const BatchCache<T, G>& bc, const T* xbg, const int* idx,
+                                             const double* val, const signed char* fold, const int* sidx,
+                                             const long long* cp, const long long* vp, const int* e0,
+                                             const int* off, const int* fmt, int q, const int* boff, int L) {
+    constexpr int P = BatchCache<T, G>::kPieces;
+    constexpr int PV = 16 / (int)sizeof(T);
+    const int E = boff[L];
+    for (int i = threadIdx.x; i < E * P; i += kBT) {
+        const int e = i / P, p = i % P;
+        int w = 0;
+        while (e >= boff[w + 1]) ++w;
+        const int qq = q + w, el = e - boff[w];
+        const int k = off[qq] >= 0 ? sidx[off[qq] + el] : __ldg(idx + cp[qq] + e0[qq] + el);
+        cp_async16(bc.v + (size_t)e * G + p * PV, xbg + (size_t)k * G + p * PV);
+    }
+    cp_async_commit();
+    for (int e = threadIdx.x; e < E; e += kBT) {
+        int w = 0;
+        while (e >= boff[w + 1]) ++w;
+        const int qq = q + w, el = e - boff[w];
+        const int k = off[qq] >= 0 ? sidx[off[qq] + el] : __ldg(idx + cp[qq] + e0[qq] + el);
+        bc.row[e] = k;
+        bc.x[e] = fmt[qq] == CYC_SPARSE ? (T)__ldg(val + vp[qq] + e0[qq] + el) : T(1);
+        if (WM == 1) bc.fold[e] = (unsigned char)__ldg(fold + k);
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+}
+
+// Gradient and Hessian terms of the group's fits over cache entries
+// [b0, b1) (one column of the batch) by the 32 lanes of a warp: lane t takes
+// entries b0 + t / TPR, b0 + t / TPR + 32 / TPR, ... and fits part t % TPR
+// of each -- the entries and order rows_gh gives a warp, so the sums are the
+// same.
+template <class T, int MODEL, int G, int WM>
+__device__ __forceinline__ void cache_gh(const BatchCache<T, G>& bc, int b0, int b1, bool ind, const T* wg,
+                                         const unsigned char* wmask, unsigned done,
+                                         double (&g)[RowLayout<T, G, false>::FPT],
+                                         double (&h)[RowLayout<T, G, false>::FPT]) {
+    using Lay = RowLayout<T, G, false>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, RS = 32 / TPR;
+    const int lane = threadIdx.x & 31;
+    const int f0 = (lane % TPR) * FPT;
+    const unsigned dn = done >> f0;
+    Kahan<T> ag[FPT], ah[FPT];
+    for (int e = b0 + lane / TPR; e < b1; e += RS) {
+        T v[FPT];
+        load_row<T, FPT>(bc.v + (size_t)e * G + f0, v);
+        const T x = bc.x[e];
+        T w[FPT];
+        if (WM == 0) load_row<T, FPT>(wg + (size_t)bc.row[e] * G + f0, w);
+        const unsigned wm = (WM == 1) ? (unsigned)wmask[bc.fold[e]] >> f0 : 0u;
+        #pragma unroll
+        for (int f = 0; f < FPT; ++f) {
+            if ((dn >> f) & 1u) continue;
+            const T wt = (WM == 1) ? (((wm >> f) & 1u) ? T(1) : T(0)) : w[f];
+            row_gh<T, MODEL>(v[f], x, wt, ind, ag[f], ah[f]);
+        }
+    }
+    #pragma unroll
+    for (int f = 0; f < FPT; ++f) { g[f] = ag[f].value(); h[f] = ah[f].value(); }
+}
+
+// updateXBeta of a cached batch over this CTA's rows: each (entry, part) of a
+// column with a step writes its new values from the cache; entries on the
+// batch's shared rows (`drow`, nd of them) are left to their owner.  No two
+// items touch the same (row, part): a row outside `drow` is in one column.
+template <class T, int G>
+__device__ __forceinline__ void cache_update(const BatchCache<T, G>& bc, T* xbg, const int* boff, int L,
+                                             const double (*dr)[G], const int* drow, int nd) {
+    using Lay = RowLayout<T, G, false>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR;
+    unsigned bloom = 0;
+    for (int d = 0; d < nd; ++d) bloom |= 1u << (drow[d] & 31);
+    const int items = boff[L] * TPR;
+    for (int i = threadIdx.x; i < items; i += kBT) {
+        const int e = i / TPR, f0 = (i % TPR) * FPT;
+        int w = 0;
+        while (e >= boff[w + 1]) ++w;
+        bool moved = false;                 // a part whose fits all kept their coefficients stays
+        #pragma unroll
+        for (int f = 0; f < FPT; ++f) moved |= (dr[w][f0 + f] != 0.0);
+        if (!moved) continue;
+        const int k = bc.row[e];
+        if ((bloom >> (k & 31)) & 1u) {
+            bool sh = false;
+            for (int d = 0; d < nd; ++d) sh |= (drow[d] == k);
+            if (sh) continue;
+        }
+        T v[FPT];
+        load_row<T, FPT>(bc.v + (size_t)e * G + f0, v);
+        const T x = bc.x[e];
+        #pragma unroll
+        for (int f = 0; f < FPT; ++f) v[f] = upd_fma((T)dr[w][f0 + f], x, v[f]);
+        store_row<T, FPT>(xbg + (size_t)k * G + f0, v);
+    }
+}
+
 // Items of one coordinate a thread keeps in registers between the gradient
 // and the update: columns with at most kRegItems * (kBT / G) entries in this
 // CTA's rows take this path (one load round trip, no reload for the update);
@@ -631,6 +761,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     __shared__ unsigned char s_dwm[kDirtyMax];
     __shared__ int s_drow[kDirtyMax];
     __shared__ int s_boff[kRunMax + 1];
+    __shared__ int s_cbo[kRunMax + 1];     // the open batch's columns in the batch cache
     // the current chunk of coordinates
     __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk], c_run[kChunk];
     __shared__ int c_lvl[kChunk], c_nd[kChunk], c_dr0[kChunk], c_de0[kChunk + 1];
@@ -650,6 +781,8 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     // groups of independent-rows models, each thread's cp.async row slots
     T* s_sx = reinterpret_cast<T*>(dyn_smem + 3 * kChunk * G * sizeof(double) + kStage * sizeof(int));
     T* s_abuf = s_sx + (size_t)threadIdx.x * LayB::D * LayB::FPT;
+    // the batch cache (8-fit groups of independent-rows models) shares those bytes
+    const BatchCache<T, kRowStream ? G : 8> bcache(s_sx);
     // shared rows of the open batch: as pushed by their owners (by parity; the
     // replay then moves this CTA's copy of the current parity in place), their
     // model means at the batch's start and now, and their weights
@@ -832,13 +965,29 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                     s_bde_d[t] = __ldg(A.de_d + de0 + t) & 0xff;
                     s_bde_x[t] = __ldg(A.de_x + de0 + t);
                 }
+                // the batch's entries in my rows, column by column (cache offsets)
+                if (threadIdx.x <= L) {
+                    int o = 0;
+                    for (int w = 0; w < (int)threadIdx.x; ++w) o += c_e1[q + w] - c_e0[q + w];
+                    s_cbo[threadIdx.x] = o;
+                }
+                __syncthreads();
+                const bool cached = s_cbo[L] <= BatchCache<T, G>::kRows;
+                if (cached)
+                    batch_gather<T, G, WM>(bcache, xbg, A.idx, A.val, A.fold, s_sidx, c_cp, c_vp, c_e0, c_off, c_fmt,
+                                           q, s_cbo, L);
                 // gradient partials of every column from the state at the batch's start
                 if (warp < L) {
                     const int qq = q + warp, so = c_off[qq];
-                    const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
-                                        nullptr, c_e0[qq], c_e1[qq], false, c_fmt[qq] == CYC_INDICATOR};
                     double g[LayW::FPT], h[LayW::FPT];
-                    rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
+                    if (cached) {
+                        cache_gh<T, MODEL, G, WM>(bcache, s_cbo[warp], s_cbo[warp + 1], c_fmt[qq] == CYC_INDICATOR, wg,
+                                                  s_wmask, done_m, g, h);
+                    } else {
+                        const ColRows<T> cr{A.idx + c_cp[qq], A.val + c_vp[qq], so >= 0 ? s_sidx + so : nullptr,
+                                            nullptr, c_e0[qq], c_e1[qq], false, c_fmt[qq] == CYC_INDICATOR};
+                        rows_gh<T, MODEL, G, WM, 32>(cr, lane, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
+                    }
                     int fit;
                     bool is_h, holder;
                     const double v = warp_reduce_rows<LayW::FPT, LayW::TPR>(g, h, fit, is_h, holder);
@@ -925,20 +1074,25 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 // threads, flat): a row that one column of the batch touches gets
                 // that column's step; a row the batch shares gets its replayed
                 // value, written by its owner.  Columns whose fits all kept their
-                // coefficients are skipped.
-                if (threadIdx.x == 0) {
-                    int o = 0;
-                    for (int w = 0; w < L; ++w) {
-                        s_boff[w] = o;
-                        bool any = false;
-                        for (int f = 0; f < G; ++f) any |= (s_dr[w][f] != 0.0);
-                        if (any) o += c_e1[q + w] - c_e0[q + w];
+                // coefficients are skipped.  A cached batch writes the new values
+                // from the cache.
+                if (cached) {
+                    cache_update<T, G>(bcache, xbg, s_cbo, L, s_dr, s_drow, nd);
+                } else {
+                    if (threadIdx.x == 0) {
+                        int o = 0;
+                        for (int w = 0; w < L; ++w) {
+                            s_boff[w] = o;
+                            bool any = false;
+                            for (int f = 0; f < G; ++f) any |= (s_dr[w][f] != 0.0);
+                            if (any) o += c_e1[q + w] - c_e0[q + w];
+                        }
+                        s_boff[L] = o;
                     }
-                    s_boff[L] = o;
+                    __syncthreads();
+                    batch_update<T, G>(xbg, A.idx, A.val, s_sidx, nullptr, c_cp, c_vp, c_e0, c_off, c_fmt, q, L,
+                                       s_boff, s_dr, s_drow, nd);
                 }
-                __syncthreads();
-                batch_update<T, G>(xbg, A.idx, A.val, s_sidx, nullptr, c_cp, c_vp, c_e0, c_off, c_fmt, q, L, s_boff,
-                                   s_dr, s_drow, nd);
                 for (int t = threadIdx.x; t < nd * G; t += kBT) {
                     const int d = t / G, k = s_drow[d];
                     if (k >= r0 && k < r1) xbg[(size_t)k * G + t % G] = s_dst[par][d][t % G];
@@ -1547,8 +1701,10 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
 // rows.  Each shared row gets a slot, and every entry on a shared row is
 // listed with (slot, column within the batch, position in the column).
 // dmax = 0 gives the conflict-free runs used with one fit per group.
+// `batch_rows` > 0 also closes a batch before its entries in any one CTA's
+// rows would exceed that many (the batch cache holds them all).
 static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const std::vector<int>& fixb, int cap,
-                         bool allow, int dmax) {
+                         bool allow, int dmax, int batch_rows = 0) {
     const int J = ds.J, K = ds.K, C = (int)rpart.size() - 1;
     RunPlan P;
     P.len.assign(J, 1);
@@ -1565,7 +1721,9 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
     std::vector<Ent> ents;
     std::vector<int> shared;            // row ids in order of their slots
     int run_id = -1, start = -1, len = 0;
+    std::vector<int> bsum(C, 0);        // the open batch's entries per CTA
     auto close = [&] {
+        std::fill(bsum.begin(), bsum.end(), 0);
         if (start < 0) return;
         P.len[start] = len;
         P.dr0[start] = (int)P.drow.size();
@@ -1613,10 +1771,14 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
                     fresh += rs[rows[e]].dslot < 0;
                     level = std::max(level, rs[rows[e]].rlvl + 1);
                 }
-        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > kLevelMax)) {
+        bool full = false;
+        if (batch_rows > 0)
+            for (int r = 0; r < C; ++r) full |= bsum[r] + cnt[r] > batch_rows;
+        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > kLevelMax || full)) {
             close();
             level = 1;
         }
+        for (int r = 0; r < C; ++r) bsum[r] += cnt[r];
         if (start < 0) {
             start = j;
             ++run_id;
@@ -1761,14 +1923,16 @@ struct BatchRunner {
         d_fixb.alloc(J); d_ptype.alloc(J); d_active.alloc(Fp); d_var.alloc(Fp);
         {
             const RunPlan* plan = nullptr;
+            const bool rows8 = (G == 8) && model_independent(ds.model);
+            const int brows = rows8 ? BatchCache<T, 8>::kRows : 0;
             for (auto& pl : ds.run_plans)
-                if (pl.C == C && pl.G == G && pl.fixed == fixed_cols) plan = &pl;
+                if (pl.C == C && pl.G == G && pl.batch_rows == brows && pl.fixed == fixed_cols) plan = &pl;
             if (!plan) {
-                const bool rows8 = (G == 8) && model_independent(ds.model);
                 RunPlan pl = plan_runs(ds, rpart, fixb, rows8 ? kBatchCap : (32 / G) * kRunItems,
-                                       model_independent(ds.model), rows8 ? kDirtyMax : 0);
+                                       model_independent(ds.model), rows8 ? kDirtyMax : 0, brows);
                 pl.C = C;
                 pl.G = G;
+                pl.batch_rows = brows;
                 pl.fixed = fixed_cols;
                 ds.run_plans.push_back(std::move(pl));
                 plan = &ds.run_plans.back();

@@ -205,6 +205,7 @@ struct ColView {
 // ---------------------------------------------------------------------------
 struct RunPlan {
     int C = 0, G = 0;
+    int batch_rows = 0;         // cap on a batch's entries in any one CTA's rows (0: none)
     std::vector<int> fixed;     // columns held fixed besides the offset (ascending)
     std::vector<int> len;       // J: columns in the batch starting here (1 = alone), 0 inside a batch
     std::vector<int> lvl;       // J: level of the column in its batch (1 + max level of earlier sharers)
