@@ -44,15 +44,20 @@ struct SharedDataset {
     ~SharedDataset() { if (ds) cyc_dataset_destroy(ds); }
 };
 
-class CudaModelSpecifics : public bsccs::AbstractModelSpecifics {
+// RealType is the ModelData's: double, or float for the reference's
+// floatingPoint = 32 data (src/RcppModelData.cpp:724-728), whose values,
+// outcomes and times are widened to double at upload; the engine computes
+// in FP64 on those values either way.
+template <class RealType>
+class CudaModelSpecificsT : public bsccs::AbstractModelSpecifics {
 public:
-    CudaModelSpecifics(const bsccs::ModelData<double>& data, int cycModel, int device = 0)
+    CudaModelSpecificsT(const bsccs::ModelData<RealType>& data, int cycModel, int device = 0)
         : bsccs::AbstractModelSpecifics(data), data_(data), model_(cycModel), device_(device),
           shared_(std::make_shared<SharedDataset>()) {
         upload();
     }
 
-    ~CudaModelSpecifics() override {
+    ~CudaModelSpecificsT() override {
         if (engine_) cyc_engine_destroy(engine_);
     }
 
@@ -127,7 +132,7 @@ public:
     void printTiming() override {}
 
     bsccs::AbstractModelSpecifics* clone() const override {
-        return new CudaModelSpecifics(*this, CloneTag());
+        return new CudaModelSpecificsT(*this, CloneTag());
     }
 
     const std::vector<double> getXBeta() override {
@@ -155,7 +160,7 @@ protected:
 
 private:
     struct CloneTag {};
-    CudaModelSpecifics(const CudaModelSpecifics& other, CloneTag)
+    CudaModelSpecificsT(const CudaModelSpecificsT& other, CloneTag)
         : bsccs::AbstractModelSpecifics(other.data_), data_(other.data_), model_(other.model_),
           device_(other.device_), shared_(other.shared_) {}
 
@@ -176,19 +181,19 @@ private:
                 const size_t n = X.getNumberOfEntries(j);
                 idx.insert(idx.end(), r, r + n);
                 if (f == bsccs::SPARSE) {
-                    const double* v = X.getDataVector(j);
+                    const RealType* v = X.getDataVector(j);
                     val.insert(val.end(), v, v + n);
                 }
             } else if (f == bsccs::DENSE) {
-                const double* v = X.getDataVector(j);
+                const RealType* v = X.getDataVector(j);
                 val.insert(val.end(), v, v + K0);
             }
             cp[j + 1] = (long long)idx.size();
             vp[j + 1] = (long long)val.size();
         }
         const auto& pid = data_.getPidVectorRef();
-        const auto& y = data_.getYVectorRef();
-        const auto& t = data_.getTimeVectorRef();
+        const std::vector<double> y(data_.getYVectorRef().begin(), data_.getYVectorRef().end());
+        const std::vector<double> t(data_.getTimeVectorRef().begin(), data_.getTimeVectorRef().end());
         cyc_data_desc d{};
         d.model = model_;
         d.K = K0;
@@ -206,7 +211,7 @@ private:
         check(cyc_dataset_create(&d, device_, &shared_->ds));
     }
 
-    const bsccs::ModelData<double>& data_;
+    const bsccs::ModelData<RealType>& data_;
     int model_;
     int device_;
     std::shared_ptr<SharedDataset> shared_;
@@ -217,12 +222,18 @@ private:
 // (src/cyclops/engine/AbstractModelSpecifics.cpp:32-35): nullptr for model
 // types this engine does not offer, which the caller reports as
 // "Invalid model type." (src/RcppCyclopsInterface.cpp:890-892).
+using CudaModelSpecifics = CudaModelSpecificsT<double>;
+
 inline bsccs::AbstractModelSpecifics* makeCudaModelSpecifics(bsccs::ModelType type,
                                                              const bsccs::AbstractModelData& data,
                                                              int device = 0) {
     const int m = toCycModel(type);
-    if (m < 0 || data.getPrecisionType() != bsccs::PrecisionType::FP64) return nullptr;
-    return new CudaModelSpecifics(static_cast<const bsccs::ModelData<double>&>(data), m, device);
+    if (m < 0) return nullptr;
+    if (data.getPrecisionType() == bsccs::PrecisionType::FP64)
+        return new CudaModelSpecificsT<double>(static_cast<const bsccs::ModelData<double>&>(data), m, device);
+    if (data.getPrecisionType() == bsccs::PrecisionType::FP32)
+        return new CudaModelSpecificsT<float>(static_cast<const bsccs::ModelData<float>&>(data), m, device);
+    return nullptr;
 }
 
 }  // namespace cyclops_b200

@@ -88,12 +88,15 @@ public:
 };
 
 // ModelData subclass that takes plain arrays, in the ingest order of
-// RcppModelData (src/RcppModelData.cpp:751-900).
-class HarnessModelData : public ModelData<double> {
+// RcppModelData (src/RcppModelData.cpp:751-900); RealType float is the
+// reference's floatingPoint = 32 data (RcppModelData.cpp:724-728), the
+// arrays rounded to float as they are copied in.
+template <class RealType>
+class HarnessModelDataT : public ModelData<RealType> {
 public:
-    HarnessModelData(ModelType type, const ref_problem* p,
-                     std::vector<int> pid, std::vector<double> y, std::vector<double> time)
-        : ModelData<double>(type, pid, y, std::vector<double>(), time,
+    HarnessModelDataT(ModelType type, const ref_problem* p,
+                      std::vector<int> pid, std::vector<double> y, std::vector<double> time)
+        : ModelData<RealType>(type, pid, y, std::vector<double>(), time,
                             bsccs::make_shared<QuietLogger>(),
                             bsccs::make_shared<ThrowingErrorHandler>()) {
         const int K = p->K;
@@ -103,30 +106,30 @@ public:
             const long long vb = p->val_ptr[j];
             switch (p->col_format[j]) {
             case REF_DENSE:
-                X.push_back((int*)nullptr, (int*)nullptr, p->col_val + vb, p->col_val + vb + K, DENSE);
+                this->X.push_back((int*)nullptr, (int*)nullptr, p->col_val + vb, p->col_val + vb + K, DENSE);
                 break;
             case REF_SPARSE:
-                X.push_back(p->col_idx + b, p->col_idx + e, p->col_val + vb, p->col_val + vb + (e - b), SPARSE);
+                this->X.push_back(p->col_idx + b, p->col_idx + e, p->col_val + vb, p->col_val + vb + (e - b), SPARSE);
                 break;
             case REF_INDICATOR:
-                X.push_back(p->col_idx + b, p->col_idx + e, (double*)nullptr, (double*)nullptr, INDICATOR);
+                this->X.push_back(p->col_idx + b, p->col_idx + e, (double*)nullptr, (double*)nullptr, INDICATOR);
                 break;
             case REF_INTERCEPT:
-                X.push_back((int*)nullptr, (int*)nullptr, (double*)nullptr, (double*)nullptr, INTERCEPT);
+                this->X.push_back((int*)nullptr, (int*)nullptr, (double*)nullptr, (double*)nullptr, INTERCEPT);
                 break;
             default:
                 throw std::runtime_error("unknown column format");
             }
-            X.getColumn(X.getNumberOfColumns() - 1).add_label(j);
+            this->X.getColumn(this->X.getNumberOfColumns() - 1).add_label(j);
         }
-        X.nRows = K;
-        if (p->has_offset) setHasOffsetCovariate(true);
-        if (p->has_intercept) setHasInterceptCovariate(true);
+        this->X.nRows = K;
+        if (p->has_offset) this->setHasOffsetCovariate(true);
+        if (p->has_intercept) this->setHasInterceptCovariate(true);
         // pid renumbering by runs (RcppModelData.cpp:878-900)
-        std::vector<int>& cpid = getPidVectorRef();
+        std::vector<int>& cpid = this->getPidVectorRef();
         if (cpid.empty()) {
             for (int i = 0; i < K; ++i) cpid.push_back(i);
-            nPatients = K;
+            this->nPatients = K;
         } else {
             int current = 0;
             int last = cpid[0];
@@ -135,10 +138,12 @@ public:
                 if (cpid[i] != last) { ++current; last = cpid[i]; }
                 cpid[i] = current;
             }
-            nPatients = current + 1;
+            this->nPatients = current + 1;
         }
     }
 };
+
+using HarnessModelData = HarnessModelDataT<double>;
 
 ModelType toModelType(int m) {
     switch (m) {
@@ -161,13 +166,13 @@ priors::PriorPtr makeCovariatePrior(int type, double variance) {
 }
 
 struct Instance {
-    std::unique_ptr<HarnessModelData> data;
+    std::unique_ptr<AbstractModelData> data;
     std::unique_ptr<AbstractModelSpecifics> engine;
     std::unique_ptr<CyclicCoordinateDescent> ccd;
     bool useWeights = false;
 };
 
-std::unique_ptr<Instance> build(const ref_problem* p, int device) {
+std::unique_ptr<Instance> build(const ref_problem* p, int device, bool fp32 = false) {
     std::vector<int> pid;
     if (p->pid) pid.assign(p->pid, p->pid + p->K);
     std::vector<double> y(p->y, p->y + p->K);
@@ -175,7 +180,8 @@ std::unique_ptr<Instance> build(const ref_problem* p, int device) {
     if (p->time) time.assign(p->time, p->time + p->K);
 
     auto inst = std::unique_ptr<Instance>(new Instance());
-    inst->data.reset(new HarnessModelData(toModelType(p->model), p, pid, y, time));
+    if (fp32) inst->data.reset(new HarnessModelDataT<float>(toModelType(p->model), p, pid, y, time));
+    else inst->data.reset(new HarnessModelData(toModelType(p->model), p, pid, y, time));
     if (device == 0) {
         inst->engine.reset(AbstractModelSpecifics::factory(
             toModelType(p->model), *inst->data, DeviceType::CPU, ""));
@@ -244,9 +250,9 @@ void fillResult(Instance& inst, int J, ref_result* out) {
 }
 
 int fitWithDevice(const ref_problem* p, const ref_control* c, const double* start, ref_result* out,
-                  int device) {
+                  int device, bool fp32 = false) {
     return guarded([&] {
-        auto inst = build(p, device);
+        auto inst = build(p, device, fp32);
         if (start) {
             std::vector<double> b(start, start + p->J);
             inst->ccd->setBeta(b);
@@ -269,6 +275,11 @@ int ref_fit(const ref_problem* p, const ref_control* c, const double* start_beta
 int ref_fit_device(const ref_problem* p, const ref_control* c, const double* start_beta,
                    ref_result* out, int device) {
     return fitWithDevice(p, c, start_beta, out, device);
+}
+
+int ref_fit_fp32(const ref_problem* p, const ref_control* c, const double* start_beta, ref_result* out,
+                 int device) {
+    return fitWithDevice(p, c, start_beta, out, device, true);
 }
 
 int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient, double* hessian,

@@ -52,6 +52,11 @@ const char* ref_last_error(void);
 int ref_fit(const ref_problem* p, const ref_control* c, const double* start_beta, ref_result* out);
 int ref_fit_device(const ref_problem* p, const ref_control* c, const double* start_beta,
                    ref_result* out, int device);
+/* The same on ModelData<float> (the reference's floatingPoint = 32 data,
+ * RcppModelData.cpp:724-728): device 0 the reference's float CPU engine,
+ * device 1 the CUDA engine through the adapter. */
+int ref_fit_fp32(const ref_problem* p, const ref_control* c, const double* start_beta, ref_result* out,
+                 int device);
 int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient, double* hessian,
                      double* xbeta, double* log_likelihood);
 int ref_predictive_loglik(const ref_problem* p, const double* beta, const double* held_out,

@@ -66,3 +66,22 @@ def test_reference_ccd_drives_cuda_engine(cuda_lib, name):
     got = types.SimpleNamespace(beta=beta, log_likelihood=r.log_likelihood, iterations=r.iterations,
                                 return_flag=r.return_flag)
     assert_contract(got, golden_fit(s), what=name)
+
+
+@pytest.mark.skipif(not os.path.exists(ADAPTER), reason="adapter harness not built (needs the reference sources)")
+@pytest.mark.parametrize("name", ["small_lr_dense", "lr_normal_weighted", "pr_offset_normal", "cox_laplace",
+                                  "clr_laplace"])
+def test_reference_ccd_drives_cuda_engine_on_float_data(cuda_lib, name):
+    """ModelData<float> (the reference's floatingPoint = 32) behind the
+    drop-in: the adapter widens the float values to double at upload, so the
+    fit is the reference FP64 engine's on the float-rounded data, under the
+    precision contract."""
+    import ctypes as C
+    from oracle import oracle as O
+    from test_oracle import _float_rounded, ref_fit_fp32
+    data, s = load_golden(name)
+    got = ref_fit_fp32(C.CDLL(ADAPTER), data, s, 1)
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]))
+    want = O.ref().fit(_float_rounded(data), int(s["prior"]), float(s["variance"]), control=ctl,
+                       weights=s["weights"])
+    assert_contract(got, want, what=name)

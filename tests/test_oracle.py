@@ -1,5 +1,7 @@
 """The CPU oracles, pinned against the golden fixtures made by the reference
 engine (tests/golden/make_golden.py).  No GPU."""
+import os
+
 import numpy as np
 import pytest
 
@@ -219,3 +221,42 @@ def test_port_fixed_coefficients_match_reference():
         b = O.port().fit(data, D.PRIOR_LAPLACE, float(s["variance"]), control=ctl, start=start, fixed=[3, 7])
         assert a.iterations == b.iterations
         np.testing.assert_allclose(b.beta, a.beta, rtol=1e-12, atol=1e-14)
+
+
+def _float_rounded(data):
+    """The data as ModelData<float> holds it: outcomes, times and values
+    rounded to float, widened back to double."""
+    from cyclops_b200.data import CyclopsData
+    r = lambda a: None if a is None else np.asarray(a, np.float32).astype(np.float64)
+    return CyclopsData(model=data.model, y=r(data.y), col_format=data.col_format, col_ptr=data.col_ptr,
+                       col_idx=data.col_idx, val_ptr=data.val_ptr, col_val=r(data.col_val), pid=data.pid,
+                       time=r(data.time), has_offset=data.has_offset, has_intercept=data.has_intercept)
+
+
+def ref_fit_fp32(lib, data, s, device):
+    """ref_fit_fp32 of a harness library: the reference's CCD on
+    ModelData<float> (device 0: its float CPU engine; 1: the CUDA engine)."""
+    import ctypes as C
+    lib.ref_fit_fp32.argtypes = [C.POINTER(O.Problem), C.POINTER(O.Control), C.c_void_p, C.POINTER(O.Result),
+                                 C.c_int]
+    lib.ref_last_error.restype = C.c_char_p
+    p, keep = O.make_problem(data, int(s["prior"]), float(s["variance"]), None, s["weights"])
+    ctl = O.make_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]))
+    beta = np.zeros(data.J)
+    r = O.Result(beta=beta.ctypes.data)
+    assert lib.ref_fit_fp32(C.byref(p), C.byref(ctl), None, C.byref(r), device) == 0, lib.ref_last_error()
+    return O.Fit(beta, r.log_likelihood, r.log_prior, r.iterations, r.return_flag)
+
+
+def test_reference_float_data_fit():
+    """The reference's own FP32 path (floatingPoint = 32) on the binomial bid
+    design of test-floatingPoint.R fits the FP64 coefficients to the
+    reference test's own bound (1e-3, against glm there)."""
+    import ctypes as C
+    if not O.have_ref():
+        pytest.skip("reference engine not built")
+    data, s = load_golden("small_lr_dense")
+    lib = C.CDLL(os.path.join(O.REF_DIR, "libcyclops_ref.so"))
+    f32 = ref_fit_fp32(lib, data, s, 0)
+    assert f32.return_flag == 0
+    np.testing.assert_allclose(f32.beta, s["beta"], rtol=1e-3)
