@@ -99,6 +99,7 @@ _SIGS = {
                       C.POINTER(FitResult)],
     "cyc_last_run_stats": [C.POINTER(RunStats)],
     "cyc_cv_fold_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_int, C.c_int, C.c_void_p],
+    "cyc_bootstrap_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_void_p],
     "cyc_launch_count": [],
     "cyc_gradient_hessian_noalloc": [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p],

@@ -532,6 +532,22 @@ def cv_fold_weights(K: int, folds: int, seed: int, ids=None, n_reps: int = 1) ->
     return out
 
 
+def bootstrap_weights(K: int, n_replicates: int, seed: int, ids=None, unit_exclude=None) -> np.ndarray:
+    """(n_replicates, K) bootstrap weights drawn exactly as the reference's
+    BootstrapSelector draws them for BootstrapDriver: each replicate resamples
+    the units (`ids`, one per row by default) with replacement; a row's
+    weight is its unit's draw count.  Fit the replicates together with
+    batch_fit(data, prior, [variance] * n_replicates, weights).  The
+    reference's driver warm-starts each replicate from the previous one's
+    coefficients; batch_fit starts every replicate from `starts` (zero by
+    default), so fits agree with the driver's to the convergence tolerance."""
+    out = np.zeros((n_replicates, K))
+    idv = None if ids is None else np.ascontiguousarray(ids, np.int32)
+    ex = None if unit_exclude is None else np.ascontiguousarray(unit_exclude, np.float64)
+    N.check(N.lib().cyc_bootstrap_weights(int(K), _ptr(idv), int(n_replicates), int(seed), _ptr(ex), _ptr(out)))
+    return out
+
+
 def last_run_stats() -> dict:
     s = N.RunStats()
     N.check(N.lib().cyc_last_run_stats(C.byref(s)))

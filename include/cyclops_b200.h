@@ -315,6 +315,18 @@ int cyc_cv_auto_search(cyc_dataset* ds, const cyc_prior* prior, const int* fold_
 int cyc_cv_fold_weights(int K, const int* ids, int folds, long seed, int by_row, int n_reps,
                         double* out);
 
+/* Bootstrap replicate weights, `n_replicates` rows of K weights, exactly as
+ * BootstrapSelector draws them for BootstrapDriver
+ * (src/cyclops/drivers/BootstrapSelector.cpp:15-88,
+ * src/cyclops/drivers/BootstrapDriver.cpp:47-64): units are the ids
+ * 0..N-1 (`ids` K per-row unit ids, NULL = one unit per row); each replicate
+ * draws as many units with replacement from the units whose `unit_exclude`
+ * weight is 0 (NULL = all), and weights row k by the draws of its unit.
+ * Seed -1 = the engine's default state.  Feed the rows to cyc_batch_fit as
+ * per-fit weights. */
+int cyc_bootstrap_weights(int K, const int* ids, int n_replicates, long seed, const double* unit_exclude,
+                          double* out);
+
 /* Statistics of the last cyc_batch_fit / cyc_fit on this thread, for
  * roofline accounting: kernel milliseconds (CUDA events), column entries
  * visited by gradients, entries visited by updates, coordinate steps. */

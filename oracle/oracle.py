@@ -340,6 +340,35 @@ def ref_cv_weights(K, ids, fold, seed, by_row=True, n_reps=1) -> np.ndarray:
     return np.frombuffer(p.stdout, dtype=np.float64).reshape(n_reps * fold, K).copy()
 
 
+_BOOT_SCRIPT = r"""
+import ctypes as C, sys
+L = C.CDLL(sys.argv[1])
+f = L.ref_bootstrap_weights
+f.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_void_p]
+K, reps, seed = map(int, sys.argv[2:5])
+raw = sys.stdin.buffer.read()
+ids = (C.c_int * K).from_buffer_copy(raw)
+out = (C.c_double * (K * reps))()
+if f(K, C.addressof(ids), reps, seed, C.addressof(out)):
+    sys.exit(3)
+sys.stdout.buffer.write(bytes(out))
+"""
+
+
+def ref_bootstrap_weights(K, ids, n_replicates, seed) -> np.ndarray:
+    """Replicate weights from the reference's BootstrapSelector (by unit id,
+    one permute per replicate as BootstrapDriver does), in a child
+    interpreter for the same reason as ref_cv_weights."""
+    path = os.path.join(REF_DIR, "libcyclops_ref.so")
+    if not os.path.exists(path):
+        build()
+    ids = np.ascontiguousarray(ids, np.int32)
+    import sys
+    p = subprocess.run([sys.executable, "-c", _BOOT_SCRIPT, path, str(K), str(n_replicates), str(seed)],
+                       input=ids.tobytes(), capture_output=True, check=True)
+    return np.frombuffer(p.stdout, dtype=np.float64).reshape(n_replicates, K).copy()
+
+
 class IngestInput(C.Structure):
     _fields_ = [("model", C.c_int), ("n_outcomes", C.c_longlong), ("stratum_id", C.c_void_p),
                 ("row_id", C.c_void_p), ("y", C.c_void_p), ("time", C.c_void_p),

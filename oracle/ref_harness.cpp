@@ -45,6 +45,7 @@
 #include "priors/JointPrior.h"
 #include "priors/CovariatePrior.h"
 #include "drivers/CrossValidationSelector.h"
+#include "drivers/BootstrapSelector.h"
 #include "drivers/AutoSearchCrossValidationDriver.h"
 #include "drivers/GridSearchCrossValidationDriver.h"
 #include "CcdInterface.h"
@@ -328,6 +329,23 @@ int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n
             if (f == 0) sel.permute();
             sel.getWeights(f, w);
             std::memcpy(out + (size_t)task * K, w.data(), sizeof(double) * K);
+        }
+    });
+}
+
+// BootstrapSelector (by unit id) as BootstrapDriver::drive uses it: one
+// permute per replicate, then the weights of batch 0.
+int ref_bootstrap_weights(int K, const int* ids, int n_replicates, long seed, double* out /* n_replicates x K */) {
+    return guarded([&] {
+        std::vector<int> idv(ids, ids + K);
+        auto logger = bsccs::make_shared<QuietLogger>();
+        auto err = bsccs::make_shared<ThrowingErrorHandler>();
+        BootstrapSelector sel(n_replicates, idv, SelectorType::BY_PID, seed, logger, err, nullptr);
+        std::vector<double> w;
+        for (int r = 0; r < n_replicates; ++r) {
+            sel.permute();
+            sel.getWeights(0, w);
+            std::memcpy(out + (size_t)r * K, w.data(), sizeof(double) * K);
         }
     });
 }

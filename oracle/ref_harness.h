@@ -62,6 +62,7 @@ int ref_engine_probe(const ref_problem* p, const double* beta, double* gradient,
 int ref_predictive_loglik(const ref_problem* p, const double* beta, const double* held_out,
                           double* out);
 int ref_cv_weights(int K, const int* ids, int fold, long seed, int by_row, int n_reps, double* out);
+int ref_bootstrap_weights(int K, const int* ids, int n_replicates, long seed, double* out);
 
 /* The reference's own data loader on tables already in the reference's
  * sort order (the R layer sorts, R/NewDataConversion.R:125-176):

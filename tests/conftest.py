@@ -104,7 +104,8 @@ def assert_contract(got, want, iterations=True, log_likelihood=True, what=""):
     b, w = np.asarray(got.beta, float), np.asarray(want.beta, float)
     np.testing.assert_array_equal(b != 0, w != 0, err_msg=str(what))
     ok = np.abs(b - w) <= BETA_RTOL * np.abs(w) + BETA_ATOL
-    assert ok.all(), (what, float(np.max(np.abs(b - w) / (np.abs(w) + BETA_ATOL / BETA_RTOL))))
+    j = int(np.argmin(ok)) if not ok.all() else -1
+    assert ok.all(), (what, "column", j, float(b[j]), float(w[j]), "abs", float(abs(b[j] - w[j])))
     if log_likelihood:
         assert rel_err(got.log_likelihood, want.log_likelihood) < LL_RTOL, (what, got.log_likelihood,
                                                                              want.log_likelihood)

@@ -122,6 +122,19 @@ def save_cv():
     print("cv_folds", by_row.shape, by_pid.shape)
 
 
+def save_bootstrap():
+    """BootstrapSelector's replicate weights (by unit id), per row and with
+    matched strata of 5 rows as the units."""
+    K = 1003
+    ids = np.arange(K, dtype=np.int32)
+    by_row = O.ref_bootstrap_weights(K, ids, 8, 123)
+    pid = np.repeat(np.arange(201, dtype=np.int32), 5)[:K]
+    by_pid = O.ref_bootstrap_weights(K, pid, 4, 77)
+    np.savez_compressed(os.path.join(HERE, "bootstrap_weights.npz"), K=K, by_row=by_row, pid=pid, by_pid=by_pid,
+                        seed_row=123, seed_pid=77)
+    print("bootstrap_weights", by_row.shape, by_pid.shape)
+
+
 def ingest_tables(model_type, seed, with_values=True, n=80, m=400):
     """Unsorted long-format tables with the awkward cases: rowIds in random
     order, covariate rows without an outcome, zero values, columns that start
@@ -407,6 +420,8 @@ def main(parts):
             save_case(name, spec)
     if "cv" in parts:
         save_cv()
+    if "bootstrap" in parts:
+        save_bootstrap()
     if "ingest" in parts:
         save_ingest()
     if "swindle" in parts:
@@ -420,5 +435,5 @@ def main(parts):
 
 
 if __name__ == "__main__":
-    # python tests/golden/make_golden.py [fits] [cv] [ingest] [swindle] [profile] [small] [cvauto]
-    main(sys.argv[1:] or ["fits", "cv", "ingest", "swindle", "profile", "small", "cvauto"])
+    # python tests/golden/make_golden.py [fits] [cv] [bootstrap] [ingest] [swindle] [profile] [small] [cvauto]
+    main(sys.argv[1:] or ["fits", "cv", "bootstrap", "ingest", "swindle", "profile", "small", "cvauto"])

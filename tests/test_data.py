@@ -79,3 +79,15 @@ def test_library_fold_masks_equal_reference_selector(cuda_lib):
     K = int(z["K"])
     np.testing.assert_array_equal(api.cv_fold_weights(K, 10, int(z["seed_row"]), n_reps=2), z["by_row"])
     np.testing.assert_array_equal(api.cv_fold_weights(K, 5, int(z["seed_pid"]), ids=z["pid"]), z["by_pid"])
+
+
+def test_library_bootstrap_weights_equal_reference_selector(cuda_lib):
+    """cyc_bootstrap_weights is host code: bit-exact against the replicate
+    weights the reference's BootstrapSelector drew (one permute in its
+    constructor, one per replicate), per row and by matched stratum."""
+    from cyclops_b200 import api
+    z = np.load(GOLDEN + "/bootstrap_weights.npz")
+    K = int(z["K"])
+    np.testing.assert_array_equal(api.bootstrap_weights(K, 8, int(z["seed_row"])), z["by_row"])
+    np.testing.assert_array_equal(api.bootstrap_weights(K, 4, int(z["seed_pid"]), ids=z["pid"]), z["by_pid"])
+    assert np.all(z["by_row"].sum(axis=1) == K)          # K draws with replacement per replicate
