@@ -99,3 +99,19 @@ def test_batch_rejects_cox(cuda_lib):
     with pytest.raises(_native.CyclopsError) as ei:
         api.batch_fit(data, api.create_prior("laplace", 1.0), [1.0, 2.0])
     assert ei.value.status == 4
+
+
+@pytest.mark.parametrize("name", ["lr_laplace_small", "clr_laplace", "pr_laplace_weighted"])
+def test_bootstrap_replicates_as_one_batch(cuda_lib, name):
+    """Bootstrap replicates (BootstrapSelector's weights: per row, or per
+    matched stratum for clr) fitted as one batched solve; each replicate is
+    the oracle's fit at its weights (a cold start, as every fit of a batch)."""
+    from cyclops_b200 import api
+    data, s = load_golden(name)
+    ids = data.strata() if data.model in (D.CLR, D.CPR) else None
+    W = api.bootstrap_weights(data.K, 6, 42, ids=ids)
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    fits = api.batch_fit(data, prior, [float(s["variance"])] * 6, list(W), api.create_control())
+    for r, fit in enumerate(fits):
+        ref = _ref_fit(data, int(s["prior"]), float(s["variance"]), W[r])
+        assert_contract(fit, ref, what=(name, r))
