@@ -856,20 +856,23 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             if (dl != 0.0) c_beta[qq][f] = b + dl;
             return dl;
         };
-        // work counters of L columns from chunk coordinate q0 (deltas in s_dr)
+        // work counters of L columns from chunk coordinate q0 (deltas in s_dr),
+        // kept by thread 0 of every CTA over the CTA's own entries of each
+        // column (shared memory only: the counters stay off the loads); the
+        // CTAs' counts add up to the group's, the steps are counted by rank 0
         auto count_run = [&](int q0, int L) {
             int act = 0;
             for (int f = 0; f < G; ++f) act += !s_done[f];
             for (int w = 0; w < L; ++w) {
                 int upd = 0;
                 for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
-                const int j = j0 + q0 + w, fm = c_fmt[q0 + w];
+                const int fm = c_fmt[q0 + w];
                 const bool dn = (fm == CYC_DENSE || fm == CYC_INTERCEPT);
                 const bool in = (fm == CYC_INDICATOR || fm == CYC_INTERCEPT);
-                const long long nn = dn ? A.K : A.col_ptr[j + 1] - A.col_ptr[j];
+                const long long nn = c_e1[q0 + w] - c_e0[q0 + w];
                 n_grad += (unsigned long long)(act * nn);
                 n_upd += (unsigned long long)(upd * nn);
-                n_steps += act;
+                if (rank == 0) n_steps += act;
                 n_idx += (unsigned long long)(nn * ((dn ? 0 : 4) + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
             }
         };
@@ -1098,7 +1101,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                     if (k >= r0 && k < r1) xbg[(size_t)k * G + t % G] = s_dst[par][d][t % G];
                 }
                 __syncthreads();
-                if (rank == 0 && threadIdx.x == 0) count_run(q, L);
+                if (threadIdx.x == 0) count_run(q, L);
                 par ^= 1;
                 q += L;
                 continue;
@@ -1129,7 +1132,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 bool any = false;
                 #pragma unroll
                 for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[0][f]; any |= (s_dr[0][f] != 0.0); }
-                if (rank == 0 && threadIdx.x == 0) count_run(q, 1);
+                if (threadIdx.x == 0) count_run(q, 1);
                 if (any) rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd, s_abuf);
                 __syncthreads();
                 par ^= 1;
@@ -1205,20 +1208,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                       }
                   }
                   __syncthreads();
-                  if (rank == 0 && threadIdx.x == 0) {
-                      int act = 0;
-                      for (int f = 0; f < G; ++f) act += !s_done[f];
-                      for (int w = 0; w < L; ++w) {
-                          int upd = 0;
-                          for (int f = 0; f < G; ++f) upd += (s_dr[w][f] != 0.0);
-                          const long long nn = A.col_ptr[j0 + q + w + 1] - A.col_ptr[j0 + q + w];
-                          const bool in = (c_fmt[q + w] == CYC_INDICATOR);
-                          n_grad += (unsigned long long)(act * nn);
-                          n_upd += (unsigned long long)(upd * nn);
-                          n_steps += act;
-                          n_idx += (unsigned long long)(nn * (4 + (in ? 0 : 8)) * (1 + (upd ? 1 : 0)));
-                      }
-                  }
+                  if (threadIdx.x == 0) count_run(q, L);
                   par ^= 1;
                   q += L;
                   continue;
@@ -1329,15 +1319,14 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
               }
               __syncthreads();
               const double dl = s_delta[fl];
-              if (rank == 0 && threadIdx.x == 0) {
+              if (threadIdx.x == 0) {
+                  // as count_run, over this CTA's entries of the column
                   int act = 0, upd = 0;
                   for (int f = 0; f < G; ++f) { act += !s_done[f]; upd += (s_delta[f] != 0.0); }
-                  const long long nn = dense ? A.K : c_cp[q + 1 < jn ? q + 1 : q] - c_cp[q];
-                  const long long nnc = dense ? A.K : A.col_ptr[j0 + q + 1] - A.col_ptr[j0 + q];
-                  (void)nn;
+                  const long long nnc = e1 - e0;
                   n_grad += (unsigned long long)(act * nnc);
                   n_upd += (unsigned long long)(upd * nnc);
-                  n_steps += act;
+                  if (rank == 0) n_steps += act;
                   // the column streamed by this group: row ids (not for dense) and
                   // values (sparse, dense), once for the gradient, again for an update
                   const long long cb = nnc * ((dense ? 0 : 4) + (ind ? 0 : 8));
@@ -1458,10 +1447,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         A.out_flag[f] = s_flag[threadIdx.x];
         A.out_obj[f] = s_last[threadIdx.x];
     }
-    if (rank == 0 && threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
         atomicAdd(A.counters + 0, n_grad);
         atomicAdd(A.counters + 1, n_upd);
-        atomicAdd(A.counters + 2, n_steps);
+        if (rank == 0) atomicAdd(A.counters + 2, n_steps);
         atomicAdd(A.counters + 3 + grp, n_idx);
     }
 }

@@ -22,7 +22,7 @@ def pytest_configure(config):
 def golden_names():
     """The plain fit fixtures (not the CV folds, ingest tables or swindle fits)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz"))
-                  if not p.endswith("cv_folds.npz")
+                  if not p.endswith(("cv_folds.npz", "bootstrap_weights.npz"))
                   and not os.path.basename(p).startswith(("ingest_", "swindle_", "profile_", "small_", "cvauto_")))
 
 
