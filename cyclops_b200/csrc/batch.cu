@@ -204,6 +204,8 @@ __device__ __forceinline__ void row_terms(T v, T x, T wt, bool ind, T& gi, T& hi
     mean_terms<T, MODEL>(row_mean<T, MODEL>(v), x, wt, ind, gi, hi);
 }
 
+// (callers skip rows of weight zero: their terms are exactly zero, and the
+// exp() they would cost is the FP64 pipe's largest load)
 template <class T, int MODEL>
 __device__ __forceinline__ void row_gh(T v, T x, T wt, bool ind, Kahan<T>& ag, Kahan<T>& ah) {
     T gi, hi;
@@ -420,7 +422,7 @@ __device__ __forceinline__ void rows_gh(const ColRows<T>& c, int t0, const T* xb
                 for (int f = 0; f < FPT; ++f) {
                     if ((dn >> f) & 1u) continue;
                     const T wt = (WM == 1) ? (((wm >> f) & 1u) ? T(1) : T(0)) : w[s][f];
-                    row_gh<T, MODEL>(v[f], x[s], wt, c.ind, ag[f], ah[f]);
+                    if (wt != T(0)) row_gh<T, MODEL>(v[f], x[s], wt, c.ind, ag[f], ah[f]);
                 }
             }
             issue(s);
@@ -630,7 +632,7 @@ __device__ __forceinline__ void cache_gh(const BatchCache<T, G>& bc, int b0, int
         for (int f = 0; f < FPT; ++f) {
             if ((dn >> f) & 1u) continue;
             const T wt = (WM == 1) ? (((wm >> f) & 1u) ? T(1) : T(0)) : w[f];
-            row_gh<T, MODEL>(v[f], x, wt, ind, ag[f], ah[f]);
+            if (wt != T(0)) row_gh<T, MODEL>(v[f], x, wt, ind, ag[f], ah[f]);
         }
     }
     #pragma unroll
@@ -1167,7 +1169,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                       Kahan<T> ag, ah;
                       #pragma unroll
                       for (int r = 0; r < kRunItems; ++r)
-                          if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+                          if (kk[r] >= 0 && ww[r] != T(0)) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
                       double g = ag.value(), h = ah.value();
                       for (int o = G; o < 32; o <<= 1) {
                           g += __shfl_xor_sync(0xffffffffu, g, o);
@@ -1241,7 +1243,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                   }
                   #pragma unroll
                   for (int r = 0; r < kRegItems; ++r)
-                      if (kk[r] >= 0) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
+                      if (kk[r] >= 0 && ww[r] != T(0)) row_gh<T, MODEL>(vv[r], xx[r], ww[r], ind, ag, ah);
               } else if (!grouped) {
                   if (!done_l) {
                       // long column: batches of kRegItems entries per thread, loads first
@@ -1261,7 +1263,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                           }
                           #pragma unroll
                           for (int r = 0; r < kRegItems; ++r)
-                              if (k2[r] >= 0) row_gh<T, MODEL>(v2[r], x2[r], w2[r], ind, ag, ah);
+                              if (k2[r] >= 0 && w2[r] != T(0)) row_gh<T, MODEL>(v2[r], x2[r], w2[r], ind, ag, ah);
                       }
                   }
               } else {
