@@ -606,18 +606,19 @@ __device__ __forceinline__ void batch_gather(const BatchCache<T, G>& bc, const T
 }
 
 // Gradient and Hessian terms of the group's fits over cache entries
-// [b0, b1) (one column of the batch) by the 32 lanes of a warp: lane t takes
-// entries b0 + t / TPR, b0 + t / TPR + 32 / TPR, ... and fits part t % TPR
-// of each -- the entries and order rows_gh gives a warp, so the sums are the
+// [b0, b1) (one column) by STRIDE threads (a warp taking one column of a
+// batch, or the CTA taking a column alone): thread t takes entries
+// b0 + t / TPR, b0 + t / TPR + STRIDE / TPR, ... and fits part t % TPR of
+// each -- the entries and order rows_gh gives them, so the sums are the
 // same.
-template <class T, int MODEL, int G, int WM>
+template <class T, int MODEL, int G, int WM, int STRIDE = 32>
 __device__ __forceinline__ void cache_gh(const BatchCache<T, G>& bc, int b0, int b1, bool ind, const T* wg,
                                          const unsigned char* wmask, unsigned done,
-                                         double (&g)[RowLayout<T, G, false>::FPT],
-                                         double (&h)[RowLayout<T, G, false>::FPT]) {
-    using Lay = RowLayout<T, G, false>;
-    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, RS = 32 / TPR;
-    const int lane = threadIdx.x & 31;
+                                         double (&g)[RowLayout<T, G, STRIDE == kBT>::FPT],
+                                         double (&h)[RowLayout<T, G, STRIDE == kBT>::FPT]) {
+    using Lay = RowLayout<T, G, STRIDE == kBT>;
+    constexpr int FPT = Lay::FPT, TPR = Lay::TPR, RS = STRIDE / TPR;
+    const int lane = STRIDE == kBT ? (int)threadIdx.x : (int)(threadIdx.x & 31);
     const int f0 = (lane % TPR) * FPT;
     const unsigned dn = done >> f0;
     Kahan<T> ag[FPT], ah[FPT];
@@ -1115,7 +1116,19 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 const ColRows<T> cr{A.idx + c_cp[q], A.val + c_vp[q], so >= 0 ? s_sidx + so : nullptr, nullptr,
                                     c_e0[q], c_e1[q], dense, fmt == CYC_INDICATOR || fmt == CYC_INTERCEPT};
                 double g[LayB::FPT], h[LayB::FPT];
-                rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
+                // a column whose entries in my rows fit the batch cache is
+                // gathered once and updated from the cache
+                const int n1 = c_e1[q] - c_e0[q];
+                const bool cached1 = !dense && n1 <= BatchCache<T, G>::kRows;
+                if (cached1) {
+                    if (threadIdx.x <= 1) s_cbo[threadIdx.x] = threadIdx.x ? n1 : 0;
+                    __syncthreads();
+                    batch_gather<T, G, WM>(bcache, xbg, A.idx, A.val, A.fold, s_sidx, c_cp, c_vp, c_e0, c_off,
+                                           c_fmt, q, s_cbo, 1);
+                    cache_gh<T, MODEL, G, WM, kBT>(bcache, 0, n1, cr.ind, wg, s_wmask, done_m, g, h);
+                } else {
+                    rows_gh<T, MODEL, G, WM, kBT>(cr, threadIdx.x, xbg, wg, A.fold, s_wmask, done_m, s_abuf, g, h);
+                }
                 block_reduce_rows<G, LayB::FPT, LayB::TPR>(g, h, s_red, reinterpret_cast<double*>(s_scr));
                 if (threadIdx.x < G)
                     for (int r = 0; r < C; ++r) *cluster.map_shared_rank(&s_part[par][rank][0][threadIdx.x], r) = s_red[threadIdx.x];
@@ -1135,7 +1148,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                 #pragma unroll
                 for (int f = 0; f < G; ++f) { dd[f] = (T)s_dr[0][f]; any |= (s_dr[0][f] != 0.0); }
                 if (threadIdx.x == 0) count_run(q, 1);
-                if (any) rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd, s_abuf);
+                if (any) {
+                    if (cached1) cache_update<T, G>(bcache, xbg, s_cbo, 1, s_dr, s_drow, 0);
+                    else rows_update<T, G, kBT>(cr, threadIdx.x, xbg, dd, s_abuf);
+                }
                 __syncthreads();
                 par ^= 1;
                 ++q;
@@ -1915,7 +1931,9 @@ struct BatchRunner {
         {
             const RunPlan* plan = nullptr;
             const bool rows8 = (G == 8) && model_independent(ds.model);
-            const int brows = rows8 ? BatchCache<T, 8>::kRows : 0;
+            // batches are planned without regard to the cache: those whose
+            // entries fit it in every CTA take the cached path, the rest stream
+            const int brows = 0;
             for (auto& pl : ds.run_plans)
                 if (pl.C == C && pl.G == G && pl.batch_rows == brows && pl.fixed == fixed_cols) plan = &pl;
             if (!plan) {
