@@ -101,7 +101,6 @@ _SIGS = {
     "cyc_cv_fold_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_int, C.c_int, C.c_void_p],
     "cyc_bootstrap_weights": [C.c_int, C.c_void_p, C.c_int, C.c_long, C.c_void_p, C.c_void_p],
     "cyc_launch_count": [],
-    "cyc_model_mean": [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p],
     "cyc_gradient_hessian_noalloc": [C.c_int, C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p],
     "cyc_cv_grid_fit": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_void_p, C.c_int,

@@ -36,7 +36,6 @@
 
 #include "engine.cuh"
 #include "solver_common.cuh"
-#include "fast_math.cuh"
 #include "variance_search.h"
 
 namespace cg = cooperative_groups;
@@ -182,13 +181,8 @@ __device__ __forceinline__ double objective_partial(const BatchArgs& A, int grp,
 // the row's mean under the model: the logistic probability, or exp(xb)
 template <class T, int MODEL>
 __device__ __forceinline__ T row_mean(T v) {
-    if constexpr (sizeof(T) == 8) {         // FP64: the table-driven exp and Newton reciprocal
-        if (MODEL == CYC_LR) return logistic_mean(v);
-        return exp_table(v);
-    } else {
-        if (MODEL == CYC_LR) return T(1) / (T(1) + fexp(-v));
-        return fexp(v);
-    }
+    if (MODEL == CYC_LR) return T(1) / (T(1) + fexp(-v));
+    return fexp(v);
 }
 
 // (gradient, Hessian) terms of one entry from its row's mean
@@ -2713,37 +2707,5 @@ extern "C" int cyc_cv_grid_fit_weighted(cyc_dataset* dsh, const cyc_prior* prior
                 }
                 grid_mean[v] = tot / cnt;
             }
-    });
-}
-
-// ---- the model means as the batched solver evaluates them ------------------
-
-namespace cyc {
-template <int MODEL>
-__global__ void k_model_mean(long long n, const double* __restrict__ v, double* __restrict__ out) {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        out[i] = row_mean<double, MODEL>(v[i]);
-}
-}  // namespace cyc
-
-extern "C" int cyc_model_mean(int model, long long n, const double* v, double* out) {
-    return guarded([&] {
-        CYC_REQUIRE(model == CYC_LR || model == CYC_PR, CYC_ERR_UNSUPPORTED, "model means cover lr and pr");
-        CYC_REQUIRE(n >= 0 && (n == 0 || (v && out)), CYC_ERR_ARGUMENT, "bad argument");
-        if (n == 0) return;
-        cudaStream_t s;
-        CYC_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-        struct StreamGuard { cudaStream_t s; ~StreamGuard() { cudaStreamDestroy(s); } } sg{s};
-        StreamScope scope(s);
-        DevBuf<double> dv, dout;
-        dv.alloc(n);
-        dout.alloc(n);
-        CYC_CHECK_CUDA(cudaMemcpyAsync(dv.get(), v, n * sizeof(double), cudaMemcpyHostToDevice, s));
-        const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
-        if (model == CYC_LR) launch(k_model_mean<CYC_LR>, blocks, 256, 0, s, n, (const double*)dv.get(), dout.get());
-        else launch(k_model_mean<CYC_PR>, blocks, 256, 0, s, n, (const double*)dv.get(), dout.get());
-        CYC_CHECK_LAUNCH();
-        CYC_CHECK_CUDA(cudaMemcpyAsync(out, dout.get(), n * sizeof(double), cudaMemcpyDeviceToHost, s));
-        CYC_CHECK_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -348,13 +348,6 @@ typedef struct {
 } cyc_run_stats;
 int cyc_last_run_stats(cyc_run_stats* out);
 
-/* The model means the batched solvers evaluate in FP64 -- the logistic
- * probability 1 / (1 + exp(v)^-1) (model lr) or exp(v) (pr) -- for n values
- * (host arrays); the gradient terms of logistic / Poisson regression
- * (ModelSpecifics.h:540-568, 1508-1543) are built on them.  For checking
- * their accuracy against exp and division. */
-int cyc_model_mean(int model, long long n, const double* v, double* out);
-
 /* Kernels this library has launched in this process (all entry points). */
 long long cyc_launch_count(void);
 
