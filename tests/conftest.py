@@ -93,17 +93,18 @@ def golden_fit(s):
                                  iterations=int(s["iterations"]), return_flag=int(s["return_flag"]))
 
 
-def assert_contract(got, want, iterations=True, log_likelihood=True, what=""):
+def assert_contract(got, want, iterations=True, log_likelihood=True, what="", beta_atol=BETA_ATOL):
     """`got` (beta, log_likelihood, iterations, return_flag) against `want`
     under the precision contract; `iterations=False` drops the cycle count
     (a path whose reported cycles are one phase's), `log_likelihood=False`
-    the likelihood (a record that carries none)."""
+    the likelihood (a record that carries none); `beta_atol` widens the
+    absolute bound near zero where a test states why."""
     assert got.return_flag == want.return_flag, (what, got.return_flag, want.return_flag)
     if iterations:
         assert got.iterations == want.iterations, (what, got.iterations, want.iterations)
     b, w = np.asarray(got.beta, float), np.asarray(want.beta, float)
     np.testing.assert_array_equal(b != 0, w != 0, err_msg=str(what))
-    ok = np.abs(b - w) <= BETA_RTOL * np.abs(w) + BETA_ATOL
+    ok = np.abs(b - w) <= BETA_RTOL * np.abs(w) + beta_atol
     j = int(np.argmin(ok)) if not ok.all() else -1
     assert ok.all(), (what, "column", j, float(b[j]), float(w[j]), "abs", float(abs(b[j] - w[j])))
     if log_likelihood:
