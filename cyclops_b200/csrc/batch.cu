@@ -556,24 +556,19 @@ template <class T, int G>
 struct BatchCache {
     static constexpr int kPieces = (int)(G * sizeof(T)) / 16;          // 16-byte pieces of a row
     static constexpr int kEntryBytes = (int)(G * sizeof(T) + sizeof(int) + sizeof(T) + 1);
-    // (warp, column) segment sums of the balanced partials, at the region's end
-    static constexpr int kSegs = 2 * (kBT / 32) - 1;           // warps + batch columns (kBT / 32) - 1
-    static constexpr int kSegBytes = kSegs * G * (int)sizeof(double2);
-    static constexpr int kRows = ((kAsyncBytes - kSegBytes) / kEntryBytes) / 32 * 32;
+    static constexpr int kRows = (kAsyncBytes / kEntryBytes) / 32 * 32;
     static_assert(kPieces >= 1 && (G * sizeof(T)) % 16 == 0, "rows are whole 16-byte pieces");
-    static_assert(kRows * kEntryBytes + kSegBytes <= kAsyncBytes, "the batch cache exceeds its shared memory");
+    static_assert(kRows * kEntryBytes <= kAsyncBytes, "the batch cache exceeds its shared memory");
     T* v;                  // [kRows][G] linear predictors at the batch's start
     int* row;              // [kRows] row ids
     T* x;                  // [kRows] values (1 for indicators)
     unsigned char* fold;   // [kRows] fold ids (CV grid)
-    double2 (*seg)[G];     // [kSegs][G] (gradient, Hessian) sums of column segments
     __device__ explicit BatchCache(void* base) {
         unsigned char* b = static_cast<unsigned char*>(base);
         v = reinterpret_cast<T*>(b);
         row = reinterpret_cast<int*>(b + (size_t)kRows * G * sizeof(T));
         x = reinterpret_cast<T*>(b + (size_t)kRows * (G * sizeof(T) + sizeof(int)));
         fold = b + (size_t)kRows * (G * sizeof(T) + sizeof(int) + sizeof(T));
-        seg = reinterpret_cast<double2 (*)[G]>(b + kAsyncBytes - kSegBytes);
     }
 };
 
@@ -643,46 +638,6 @@ __device__ __forceinline__ void cache_gh(const BatchCache<T, G>& bc, int b0, int
     }
     #pragma unroll
     for (int f = 0; f < FPT; ++f) { g[f] = ag[f].value(); h[f] = ah[f].value(); }
-}
-
-// Gradient partials of a cached batch, balanced over the CTA's warps: the
-// batch's E entries (columns 0..L-1 at offsets boff) are cut into kBT/32
-// equal contiguous chunks, one per warp, so the longest column no longer
-// bounds the batch (each entry costs its fits' exp(), and a warp's FP64
-// issue rate is the limit).  Warp w sums each column segment of its chunk as
-// cache_gh does and writes the segment's sums to seg[w + c] for column c
-// (walking along the entries, every new segment raises w + c by at least
-// one, so the slot is unique); the caller then adds a column's segments in
-// warp order.  Deterministic.
-template <class T, int G>
-__device__ __forceinline__ void chunk_bounds(int E, int w, int& lo, int& hi) {
-    const int cs = (E + kBT / 32 - 1) / (kBT / 32);
-    lo = min(E, w * cs);
-    hi = min(E, lo + cs);
-}
-
-template <class T, int MODEL, int G, int WM>
-__device__ __forceinline__ void cache_gh_balanced(const BatchCache<T, G>& bc, const int* boff, int L,
-                                                  const int* fmt, const T* wg, const unsigned char* wmask,
-                                                  unsigned done) {
-    using Lay = RowLayout<T, G, false>;
-    constexpr int FPT = Lay::FPT, TPR = Lay::TPR;
-    const int w = threadIdx.x >> 5;
-    int lo, hi;
-    chunk_bounds<T, G>(boff[L], w, lo, hi);
-    for (int c = 0; c < L; ++c) {
-        const int s0 = max(lo, boff[c]), s1 = min(hi, boff[c + 1]);
-        if (s0 >= s1) continue;                      // warp-uniform
-        double g[FPT], h[FPT];
-        cache_gh<T, MODEL, G, WM>(bc, s0, s1, fmt[c] == CYC_INDICATOR, wg, wmask, done, g, h);
-        int fit;
-        bool is_h, holder;
-        const double v = warp_reduce_rows<FPT, TPR>(g, h, fit, is_h, holder);
-        if (holder) {
-            if (is_h) bc.seg[w + c][fit].y = v;
-            else bc.seg[w + c][fit].x = v;
-        }
-    }
 }
 
 // updateXBeta of a cached batch over this CTA's rows: each (entry, part) of a
@@ -1029,21 +984,17 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                                            q, s_cbo, L);
                 // gradient partials of every column from the state at the batch's start
                 if (cached) {
-                    // balanced over the warps: segment sums, then each column's
-                    // segments added in warp order and pushed to every CTA
-                    cache_gh_balanced<T, MODEL, G, WM>(bcache, s_cbo, L, c_fmt + q, wg, s_wmask, done_m);
-                    __syncthreads();
-                    if (threadIdx.x < 2 * G * L) {
-                        const int c = threadIdx.x / (2 * G), f = (threadIdx.x / 2) % G, hh = threadIdx.x & 1;
-                        double v = 0.0;
-                        for (int w = 0; w < kBT / 32; ++w) {
-                            int lo, hi;
-                            chunk_bounds<T, G>(s_cbo[L], w, lo, hi);
-                            if (max(lo, s_cbo[c]) < min(hi, s_cbo[c + 1]))
-                                v += hh ? bcache.seg[w + c][f].y : bcache.seg[w + c][f].x;
+                    if (warp < L) {
+                        double g[LayW::FPT], h[LayW::FPT];
+                        cache_gh<T, MODEL, G, WM>(bcache, s_cbo[warp], s_cbo[warp + 1], c_fmt[q + warp] == CYC_INDICATOR,
+                                                  wg, s_wmask, done_m, g, h);
+                        int fit;
+                        bool is_h, holder;
+                        const double v = warp_reduce_rows<LayW::FPT, LayW::TPR>(g, h, fit, is_h, holder);
+                        if (holder) {
+                            double* dst = is_h ? &s_part[par][rank][warp][fit].y : &s_part[par][rank][warp][fit].x;
+                            for (int r = 0; r < C; ++r) *cluster.map_shared_rank(dst, r) = v;
                         }
-                        double* dst = hh ? &s_part[par][rank][c][f].y : &s_part[par][rank][c][f].x;
-                        for (int r = 0; r < C; ++r) *cluster.map_shared_rank(dst, r) = v;
                     }
                 } else if (warp < L) {
                     const int qq = q + warp, so = c_off[qq];
