@@ -2376,44 +2376,21 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
         }
         CYC_CHECK_CUDA(cudaSetDevice(ds.device));
         const int F = n_folds * n_var;
-        // Fits go to the solver's groups of 8 interleaved over the grid: the
-        // group of slot s holds grid points spread from the weakest to the
-        // strongest prior, so the fits that need the most cycles (weak
-        // priors) are spread over all groups and every group's late cycles
-        // carry few active fits, instead of a few groups of slow fits
-        // setting the launch's length.  A fit's arithmetic does not depend
-        // on its group-mates, so the results are those of any other order.
-        const int ngroups = (F + 7) / 8;
-        std::vector<int> order(F);
-        for (int i = 0; i < F; ++i) order[i] = i;
-        if (F >= 4)
-            std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
-                return std::make_pair(a % ngroups, a / ngroups) < std::make_pair(b % ngroups, b / ngroups);
-            });
         std::vector<cyc_fit_spec> specs(F);
         std::vector<int> fit_fold(F);
-        std::vector<cyc_fit_result> pout(F);
-        for (int s = 0; s < F; ++s) {
-            const int i = order[s];
-            specs[s] = cyc_fit_spec{};
-            specs[s].weights = nullptr;
-            specs[s].variance = variances[i / n_folds];
-            specs[s].start_beta = nullptr;
-            fit_fold[s] = i % n_folds;
-            pout[s] = out[i];
+        for (int i = 0; i < F; ++i) {
+            specs[i].weights = nullptr;
+            specs[i].variance = variances[i / n_folds];
+            specs[i].start_beta = nullptr;
+            fit_fold[i] = i % n_folds;
         }
         StreamScope scope(ds.stream);
         DevBuf<int> d_fold;
         d_fold.alloc(ds.K);
         CYC_CHECK_CUDA(cudaMemcpyAsync(d_fold.get(), fold_of_row, ds.K * sizeof(int), cudaMemcpyHostToDevice, ds.stream));
         CYC_CHECK_CUDA(cudaStreamSynchronize(ds.stream));
-        std::vector<double> spll;
-        run_batch(ds, prior, specs.data(), F, ctl, pout.data(), d_fold.get(), n_folds, &fit_fold, &spll);
-        std::vector<double> pll(F);
-        for (int s = 0; s < F; ++s) {
-            out[order[s]] = pout[s];
-            pll[order[s]] = spll[s];
-        }
+        std::vector<double> pll;
+        run_batch(ds, prior, specs.data(), F, ctl, out, d_fold.get(), n_folds, &fit_fold, &pll);
         // AbstractCrossValidationDriver: NaN for fits that did not converge;
         // the grid point's estimate is the mean over folds ignoring NaN
         // (computePointEstimate, AbstractCrossValidationDriver.cpp:252-264)
