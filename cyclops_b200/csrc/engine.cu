@@ -259,8 +259,6 @@ void Engine::compute_xbeta_device(const double* d_beta) {
 
 void Engine::cox_rescan(int lo) {
     if (lo >= N) return;
-    const int hi = N;
-    const int ntiles = (hi - lo + kScanTile - 1) / kScanTile;
     cox_rescan_gated(nullptr, lo);
 }
 
@@ -366,7 +364,8 @@ int Engine::first_group(int j) const { return h_first_group[j]; }
 void Engine::cox_rescan_gated(const double* gate, int lo) {
     if (lo >= N) return;
     const int hi = N;
-    const int ntiles = (hi - lo + kScanTile - 1) / kScanTile;
+    // tiles start at lo rounded down to a multiple of kScanItems (aligned loads)
+    const int ntiles = (hi - scan_base(lo) + kScanTile - 1) / kScanTile;
     launch(k_scanD_tiles, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), aggD.get());
     launch(k_carryD, 1, kThreads, 0, stream, gate, ntiles, aggD.get(), lo, gstart.get(), D.get());
     launch(k_scanD_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), nw.get(),

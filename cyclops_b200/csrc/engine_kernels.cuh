@@ -333,6 +333,12 @@ __global__ void k_cox_numerator(ColView c, const int* __restrict__ group, const 
 // where P1 / P2 are stratum-segmented prefix sums of n/D and n/D^2 kept
 // (in double-double) by the denominator scan.  One block walks the column's
 // group list in tiles, carrying the segmented running sums across tiles.
+struct SegAB {
+    int f;          // a segment (stratum) starts in the span
+    double a, b;
+};
+__device__ __forceinline__ SegAB seg_combine(SegAB l, SegAB r) { return r.f ? r : SegAB{l.f, l.a + r.a, l.b + r.b}; }
+
 template <bool IND>
 __global__ void k_cox_gradient(const int* __restrict__ list, int L, const int* __restrict__ gstart,
                                const int* __restrict__ gend, const double* __restrict__ numer,
@@ -340,59 +346,83 @@ __global__ void k_cox_gradient(const int* __restrict__ list, int L, const int* _
                                const double* __restrict__ P1l, const double* __restrict__ P2h,
                                const double* __restrict__ P2l, const double* __restrict__ xjy, int j,
                                double* out) {
-    __shared__ double sA[kThreads], sB[kThreads];
-    __shared__ int sK[kThreads];
-    __shared__ double carryA, carryB;
-    __shared__ int carryKey;
-    if (threadIdx.x == 0) { carryA = 0.0; carryB = 0.0; carryKey = -1; }
+    // Each thread takes kItems consecutive groups of the list per tile; the
+    // running sums A (and B) restart at every stratum change and carry
+    // across tiles; threads' spans are combined by warp shuffles and then
+    // across the warps' totals.
+    constexpr int kItems = 4;
+    constexpr int kTile = kThreads * kItems;
+    __shared__ SegAB s_w[kThreads / 32];
+    __shared__ SegAB s_carry;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_carry = SegAB{0, 0.0, 0.0};
     double g = 0.0, h = 0.0;
-    for (int base = 0; base < L; base += blockDim.x) {
-        const int a = base + threadIdx.x;
-        int ga = 0, key = -2;
-        double A = 0.0, B = 0.0;
-        if (a < L) {
-            ga = list[a];
-            key = gstart[ga];
-            A = numer[ga];
-            B = IND ? 0.0 : numer2[ga];
-        }
-        __syncthreads();
-        // inclusive segmented scan over the tile (Hillis-Steele, keys equal => same segment)
-        sA[threadIdx.x] = A; sB[threadIdx.x] = B; sK[threadIdx.x] = key;
-        __syncthreads();
-        for (int off = 1; off < blockDim.x; off <<= 1) {
-            double pa = 0.0, pb = 0.0;
-            bool add = false;
-            if (threadIdx.x >= off && sK[threadIdx.x - off] == key) {
-                // contiguous keys: equal key at distance off => the whole span shares it
-                pa = sA[threadIdx.x - off]; pb = sB[threadIdx.x - off]; add = true;
+    for (int base = 0; base < L; base += kTile) {
+        const int a0 = base + threadIdx.x * kItems;
+        int ga[kItems], key[kItems], fl[kItems];
+        double A[kItems], B[kItems];
+        #pragma unroll
+        for (int q = 0; q < kItems; ++q) {
+            const int a = a0 + q;
+            ga[q] = 0; key[q] = -2; fl[q] = 0; A[q] = 0.0; B[q] = 0.0;
+            if (a < L) {
+                ga[q] = list[a];
+                key[q] = gstart[ga[q]];
+                fl[q] = (a == 0) || gstart[list[a - 1]] != key[q];
+                A[q] = numer[ga[q]];
+                B[q] = IND ? 0.0 : numer2[ga[q]];
             }
-            __syncthreads();
-            if (add) { A += pa; B += pb; sA[threadIdx.x] = A; sB[threadIdx.x] = B; }
-            __syncthreads();
         }
-        if (a < L) {
-            if (key == carryKey) { A += carryA; B += carryB; }
+        // inclusive within the thread's span
+        SegAB run{0, 0.0, 0.0};
+        #pragma unroll
+        for (int q = 0; q < kItems; ++q) run = seg_combine(run, SegAB{fl[q], A[q], B[q]});
+        // exclusive prefix of the span: warp shuffles, then the warps' totals
+        int f = run.f;
+        double va = run.a, vb = run.b;
+        #pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const int uf = __shfl_up_sync(0xffffffffu, f, off);
+            const double ua = __shfl_up_sync(0xffffffffu, va, off);
+            const double ub = __shfl_up_sync(0xffffffffu, vb, off);
+            if (lane >= off) {
+                if (!f) { va = ua + va; vb = ub + vb; }
+                f |= uf;
+            }
+        }
+        int ef = __shfl_up_sync(0xffffffffu, f, 1);
+        double ea = __shfl_up_sync(0xffffffffu, va, 1), eb = __shfl_up_sync(0xffffffffu, vb, 1);
+        if (lane == 0) { ef = 0; ea = 0.0; eb = 0.0; }
+        if (lane == 31) s_w[w] = SegAB{f, va, vb};
+        __syncthreads();
+        SegAB pre = s_carry;
+        for (int q = 0; q < w; ++q) pre = seg_combine(pre, s_w[q]);
+        SegAB cur = seg_combine(pre, SegAB{ef, ea, eb});
+        #pragma unroll
+        for (int q = 0; q < kItems; ++q) {
+            const int a = a0 + q;
+            if (a >= L) break;
+            cur = seg_combine(cur, SegAB{fl[q], A[q], B[q]});
             // interval end: next column group in the same stratum, else the stratum end
-            int ea;
-            if (a + 1 < L && gstart[list[a + 1]] == key) ea = list[a + 1];
-            else ea = gend[ga];
-            const DD p1e{P1h[ea - 1], P1l[ea - 1]};
-            const DD p2e{P2h[ea - 1], P2l[ea - 1]};
-            const DD p1s = (ga == key) ? DD{0.0, 0.0} : DD{P1h[ga - 1], P1l[ga - 1]};
-            const DD p2s = (ga == key) ? DD{0.0, 0.0} : DD{P2h[ga - 1], P2l[ga - 1]};
+            int e_a;
+            if (a + 1 < L && gstart[list[a + 1]] == key[q]) e_a = list[a + 1];
+            else e_a = gend[ga[q]];
+            const DD p1e{P1h[e_a - 1], P1l[e_a - 1]};
+            const DD p2e{P2h[e_a - 1], P2l[e_a - 1]};
+            const DD p1s = (ga[q] == key[q]) ? DD{0.0, 0.0} : DD{P1h[ga[q] - 1], P1l[ga[q] - 1]};
+            const DD p2s = (ga[q] == key[q]) ? DD{0.0, 0.0} : DD{P2h[ga[q] - 1], P2l[ga[q] - 1]};
             const DD d1 = dd_sub(p1e, p1s);
             const DD d2 = dd_sub(p2e, p2s);
             const double s1 = d1.hi + d1.lo;
             const double s2 = d2.hi + d2.lo;
-            g += A * s1;
-            h += IND ? (A * s1 - A * A * s2) : (B * s1 - A * A * s2);
+            g += cur.a * s1;
+            h += IND ? (cur.a * s1 - cur.a * cur.a * s2) : (cur.b * s1 - cur.a * cur.a * s2);
         }
         __syncthreads();
-        // carry: last valid element of the tile
-        const int last = min((int)blockDim.x, L - base) - 1;
-        if (threadIdx.x == last) {
-            carryA = A; carryB = B; carryKey = key;
+        if (threadIdx.x == 0) {                     // the carry into the next tile
+            SegAB t = s_carry;
+            for (int q = 0; q < kThreads / 32; ++q) t = seg_combine(t, s_w[q]);
+            s_carry = SegAB{0, t.a, t.b};
         }
         __syncthreads();
     }
@@ -557,18 +587,144 @@ __device__ T block_exclusive_scan(T v, T identity, T* total) {
     return excl;
 }
 
+// The tile kernels: thread t of a tile holds groups t0 + 8t .. t0 + 8t + 7
+// (tiles start at multiples of 8, so those loads are aligned vectors; groups
+// below `lo` or at or above `hi` are the identity), sums them in order, and
+// the threads' sums are scanned by warp shuffles and then across the warps'
+// totals -- no block-wide barrier rounds.  Segment starts (a group whose
+// stratum starts there, gstart[i] == i) reset the sums.
+
+// warp-inclusive segmented scan of (f, v), lane order
+__device__ __forceinline__ void warp_seg_scan(int& f, double& v) {
+    const int lane = threadIdx.x & 31;
+    #pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int uf = __shfl_up_sync(0xffffffffu, f, off);
+        const double uv = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) {
+            if (!f) v = uv + v;
+            f |= uf;
+        }
+    }
+}
+__device__ __forceinline__ void warp_seg_scan(int& f, DD& a, DD& b) {
+    const int lane = threadIdx.x & 31;
+    #pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int uf = __shfl_up_sync(0xffffffffu, f, off);
+        const DD ua{__shfl_up_sync(0xffffffffu, a.hi, off), __shfl_up_sync(0xffffffffu, a.lo, off)};
+        const DD ub{__shfl_up_sync(0xffffffffu, b.hi, off), __shfl_up_sync(0xffffffffu, b.lo, off)};
+        if (lane >= off) {
+            if (!f) { a = dd_add(ua, a); b = dd_add(ub, b); }
+            f |= uf;
+        }
+    }
+}
+
+// exclusive prefix of this thread's aggregate within the block (identity
+// for thread 0), and the block's total; `s_w` holds the warps' totals
+__device__ __forceinline__ SegD block_seg_excl(SegD mine, SegD* s_w, SegD* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int f = mine.f;
+    double v = mine.v;
+    warp_seg_scan(f, v);
+    int ef = __shfl_up_sync(0xffffffffu, f, 1);
+    double ev = __shfl_up_sync(0xffffffffu, v, 1);
+    if (lane == 0) { ef = 0; ev = 0.0; }
+    if (lane == 31) s_w[w] = SegD{f, v};
+    __syncthreads();
+    SegD pre{0, 0.0};
+    for (int q = 0; q < w; ++q) pre = seg_combine(pre, s_w[q]);
+    if (total) {
+        SegD t{0, 0.0};
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = seg_combine(t, s_w[q]);
+        *total = t;
+    }
+    __syncthreads();
+    return seg_combine(pre, SegD{ef, ev});
+}
+__device__ __forceinline__ SegP block_seg_excl(SegP mine, SegP* s_w, SegP* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int f = mine.f;
+    DD a = mine.a, b = mine.b;
+    warp_seg_scan(f, a, b);
+    int ef = __shfl_up_sync(0xffffffffu, f, 1);
+    DD ea{__shfl_up_sync(0xffffffffu, a.hi, 1), __shfl_up_sync(0xffffffffu, a.lo, 1)};
+    DD eb{__shfl_up_sync(0xffffffffu, b.hi, 1), __shfl_up_sync(0xffffffffu, b.lo, 1)};
+    if (lane == 0) { ef = 0; ea = DD{0.0, 0.0}; eb = DD{0.0, 0.0}; }
+    if (lane == 31) s_w[w] = SegP{f, a, b};
+    __syncthreads();
+    SegP pre{0, {0.0, 0.0}, {0.0, 0.0}};
+    for (int q = 0; q < w; ++q) pre = seg_combine(pre, s_w[q]);
+    if (total) {
+        SegP t{0, {0.0, 0.0}, {0.0, 0.0}};
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t = seg_combine(t, s_w[q]);
+        *total = t;
+    }
+    __syncthreads();
+    return seg_combine(pre, SegP{ef, ea, eb});
+}
+
+// the thread's 8 groups from i0 (a multiple of 8): segment flags and values
+// of `a` (and `b`), groups outside [lo, hi) as identity (flag 0, value 0)
+__device__ __forceinline__ void load8(int i0, int lo, int hi, const int* __restrict__ gstart,
+                                      const double* __restrict__ a, const double* __restrict__ b, int (&f)[kScanItems],
+                                      double (&va)[kScanItems], double (&vb)[kScanItems]) {
+    if (i0 >= lo && i0 + kScanItems <= hi) {
+        const int4* g4 = reinterpret_cast<const int4*>(gstart + i0);
+        const double2* a2 = reinterpret_cast<const double2*>(a + i0);
+        #pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const int4 g = __ldg(g4 + q);
+            f[4 * q] = g.x == i0 + 4 * q;
+            f[4 * q + 1] = g.y == i0 + 4 * q + 1;
+            f[4 * q + 2] = g.z == i0 + 4 * q + 2;
+            f[4 * q + 3] = g.w == i0 + 4 * q + 3;
+        }
+        #pragma unroll
+        for (int q = 0; q < kScanItems / 2; ++q) {
+            const double2 x = __ldg(a2 + q);
+            va[2 * q] = x.x;
+            va[2 * q + 1] = x.y;
+        }
+        if (b) {
+            const double2* b2 = reinterpret_cast<const double2*>(b + i0);
+            #pragma unroll
+            for (int q = 0; q < kScanItems / 2; ++q) {
+                const double2 x = __ldg(b2 + q);
+                vb[2 * q] = x.x;
+                vb[2 * q + 1] = x.y;
+            }
+        }
+    } else {
+        #pragma unroll
+        for (int q = 0; q < kScanItems; ++q) {
+            const int i = i0 + q;
+            const bool in = i >= lo && i < hi;
+            f[q] = in && gstart[i] == i;
+            va[q] = in ? a[i] : 0.0;
+            vb[q] = (in && b) ? b[i] : 0.0;
+        }
+    }
+}
+
+// first group of the tiling: lo rounded down to a multiple of 8
+__host__ __device__ __forceinline__ int scan_base(int lo) { return lo & ~(kScanItems - 1); }
+
 // `gate`: when non-null and *gate == 0 (a zero coordinate step), nothing changed
 __global__ void k_scanD_tiles(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, SegD* __restrict__ agg) {
     if (gate && *gate == 0.0) return;
-    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    __shared__ SegD s_w[kThreads / 32];
+    const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int f[kScanItems];
+    double v[kScanItems], unused[kScanItems];
+    load8(i0, lo, hi, gstart, denom, nullptr, f, v, unused);
     SegD a{0, 0.0};
-    for (int q = 0; q < kScanItems; ++q) {
-        const int i = t0 + q;
-        if (i < hi) a = seg_combine(a, SegD{gstart[i] == i, denom[i]});
-    }
+    #pragma unroll
+    for (int q = 0; q < kScanItems; ++q) a = seg_combine(a, SegD{f[q], v[q]});
     SegD tot;
-    block_exclusive_scan(a, SegD{0, 0.0}, &tot);
+    block_seg_excl(a, s_w, &tot);
     if (threadIdx.x == 0) agg[blockIdx.x] = tot;
 }
 
@@ -613,29 +769,31 @@ __global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __r
                               const double* __restrict__ denom, const double* __restrict__ nw,
                               const SegD* __restrict__ carry, double* __restrict__ D, SegP* __restrict__ aggP) {
     if (gate && *gate == 0.0) return;
-    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    __shared__ SegD s_w[kThreads / 32];
+    __shared__ SegP s_wp[kThreads / 32];
+    const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int f[kScanItems];
+    double v[kScanItems], n[kScanItems];
+    load8(i0, lo, hi, gstart, denom, nw, f, v, n);
     SegD a{0, 0.0};
-    for (int q = 0; q < kScanItems; ++q) {
-        const int i = t0 + q;
-        if (i < hi) a = seg_combine(a, SegD{gstart[i] == i, denom[i]});
-    }
-    SegD tot;
-    SegD ex = block_exclusive_scan(a, SegD{0, 0.0}, &tot);
+    #pragma unroll
+    for (int q = 0; q < kScanItems; ++q) a = seg_combine(a, SegD{f[q], v[q]});
+    const SegD ex = block_seg_excl(a, s_w, nullptr);
     SegD run = seg_combine(carry[blockIdx.x], ex);
     SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
+    #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
-        const int i = t0 + q;
-        if (i < hi) {
-            const int f = gstart[i] == i;
-            run = seg_combine(run, SegD{f, denom[i]});
+        const int i = i0 + q;
+        if (i >= lo && i < hi) {
+            run = seg_combine(run, SegD{f[q], v[q]});
             D[i] = run.v;
-            const double r1 = nw[i] / run.v;
+            const double r1 = n[q] / run.v;
             const double r2 = r1 / run.v;
-            p = seg_combine(p, SegP{f, {r1, 0.0}, {r2, 0.0}});
+            p = seg_combine(p, SegP{f[q], {r1, 0.0}, {r2, 0.0}});
         }
     }
     SegP totp;
-    block_exclusive_scan(p, SegP{0, {0.0, 0.0}, {0.0, 0.0}}, &totp);
+    block_seg_excl(p, s_wp, &totp);
     if (threadIdx.x == 0) aggP[blockIdx.x] = totp;
 }
 
@@ -644,23 +802,28 @@ __global__ void k_scanP_write(const double* gate, int lo, int hi, const int* __r
                               const SegP* __restrict__ carry, double* __restrict__ P1h, double* __restrict__ P1l,
                               double* __restrict__ P2h, double* __restrict__ P2l) {
     if (gate && *gate == 0.0) return;
-    const int t0 = lo + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    __shared__ SegP s_wp[kThreads / 32];
+    const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int f[kScanItems];
+    double d[kScanItems], n[kScanItems];
+    load8(i0, lo, hi, gstart, D, nw, f, d, n);
+    double r1[kScanItems], r2[kScanItems];
     SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
+    #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
-        const int i = t0 + q;
-        if (i < hi) {
-            const double r1 = nw[i] / D[i];
-            p = seg_combine(p, SegP{gstart[i] == i, {r1, 0.0}, {r1 / D[i], 0.0}});
-        }
+        const int i = i0 + q;
+        const bool in = i >= lo && i < hi;
+        r1[q] = in ? n[q] / d[q] : 0.0;
+        r2[q] = in ? r1[q] / d[q] : 0.0;
+        p = seg_combine(p, SegP{f[q], {r1[q], 0.0}, {r2[q], 0.0}});
     }
-    SegP tot;
-    SegP ex = block_exclusive_scan(p, SegP{0, {0.0, 0.0}, {0.0, 0.0}}, &tot);
+    const SegP ex = block_seg_excl(p, s_wp, nullptr);
     SegP run = seg_combine(carry[blockIdx.x], ex);
+    #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
-        const int i = t0 + q;
-        if (i < hi) {
-            const double r1 = nw[i] / D[i];
-            run = seg_combine(run, SegP{gstart[i] == i, {r1, 0.0}, {r1 / D[i], 0.0}});
+        const int i = i0 + q;
+        if (i >= lo && i < hi) {
+            run = seg_combine(run, SegP{f[q], {r1[q], 0.0}, {r2[q], 0.0}});
             P1h[i] = run.a.hi; P1l[i] = run.a.lo;
             P2h[i] = run.b.hi; P2l[i] = run.b.lo;
         }
