@@ -158,6 +158,7 @@ void Engine::regroup(const double* w) {
     glist.alloc(std::max<size_t>(lst.size(), 1));
     D.alloc(N + 1);
     P1h.alloc(N + 1); P1l.alloc(N + 1); P2h.alloc(N + 1); P2l.alloc(N + 1);
+    R1.alloc(N + 1); R2.alloc(N + 1);
     const int ntiles = (N + kScanTile - 1) / kScanTile;
     aggD.alloc(ntiles + 1);
     aggP.alloc(ntiles + 1);
@@ -369,10 +370,11 @@ void Engine::cox_rescan_gated(const double* gate, int lo) {
     launch(k_scanD_tiles, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), aggD.get());
     launch(k_carryD, 1, kThreads, 0, stream, gate, ntiles, aggD.get(), lo, gstart.get(), D.get());
     launch(k_scanD_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), nw.get(),
-                                                   aggD.get(), D.get(), aggP.get());
+                                                   aggD.get(), D.get(), R1.get(), R2.get(), aggP.get());
     launch(k_carryP, 1, kThreads, 0, stream, gate, ntiles, aggP.get(), lo, gstart.get(), P1h.get(), P1l.get(),
                                          P2h.get(), P2l.get());
-    launch(k_scanP_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), D.get(), nw.get(), aggP.get(),
+    launch(k_scanP_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), (const double*)R1.get(),
+                                                   (const double*)R2.get(), aggP.get(),
                                                    P1h.get(), P1l.get(), P2h.get(), P2l.get());
     CYC_CHECK_LAUNCH();
 }

@@ -33,6 +33,7 @@ struct Engine {
     DevBuf<int> group, grow_ptr, gstart, gend, glist;
     DevBuf<long long> glist_ptr;
     DevBuf<double> D, P1h, P1l, P2h, P2l;
+    DevBuf<double> R1, R2;             // scan scratch: n/D and n/D^2 per group
     DevBuf<SegD> aggD;
     DevBuf<SegP> aggP;
     std::vector<long long> h_glist_ptr;

@@ -558,7 +558,7 @@ __global__ void k_update_grouped(ColView c, const double* delta_ptr, double delt
 // computed over [lo, N) in tiles of kScanTile groups with three phases
 // (tile aggregates, carry scan, rewrite) for D and again for P.
 
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 4;
 constexpr int kScanTile = kThreads * kScanItems;
 
 __device__ __forceinline__ SegD seg_combine(SegD l, SegD r) { return r.f ? r : SegD{l.f, l.v + r.v}; }
@@ -587,8 +587,8 @@ __device__ T block_exclusive_scan(T v, T identity, T* total) {
     return excl;
 }
 
-// The tile kernels: thread t of a tile holds groups t0 + 8t .. t0 + 8t + 7
-// (tiles start at multiples of 8, so those loads are aligned vectors; groups
+// The tile kernels: thread t of a tile holds kScanItems consecutive groups
+// (tiles start at multiples of kScanItems, so those loads are aligned vectors; groups
 // below `lo` or at or above `hi` are the identity), sums them in order, and
 // the threads' sums are scanned by warp shuffles and then across the warps'
 // totals -- no block-wide barrier rounds.  Segment starts (a group whose
@@ -665,9 +665,9 @@ __device__ __forceinline__ SegP block_seg_excl(SegP mine, SegP* s_w, SegP* total
     return seg_combine(pre, SegP{ef, ea, eb});
 }
 
-// the thread's 8 groups from i0 (a multiple of 8): segment flags and values
+// the thread's kScanItems groups from i0 (a multiple of kScanItems): segment flags and values
 // of `a` (and `b`), groups outside [lo, hi) as identity (flag 0, value 0)
-__device__ __forceinline__ void load8(int i0, int lo, int hi, const int* __restrict__ gstart,
+__device__ __forceinline__ void load_items(int i0, int lo, int hi, const int* __restrict__ gstart,
                                       const double* __restrict__ a, const double* __restrict__ b, int (&f)[kScanItems],
                                       double (&va)[kScanItems], double (&vb)[kScanItems]) {
     if (i0 >= lo && i0 + kScanItems <= hi) {
@@ -719,7 +719,7 @@ __global__ void k_scanD_tiles(const double* gate, int lo, int hi, const int* __r
     const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int f[kScanItems];
     double v[kScanItems], unused[kScanItems];
-    load8(i0, lo, hi, gstart, denom, nullptr, f, v, unused);
+    load_items(i0, lo, hi, gstart, denom, nullptr, f, v, unused);
     SegD a{0, 0.0};
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) a = seg_combine(a, SegD{f[q], v[q]});
@@ -765,16 +765,18 @@ __global__ void k_carryP(const double* gate, int n, SegP* agg, int lo, const int
     scan_carry(n, agg, init);
 }
 
+// writes D and the P terms r1 = n/D, r2 = n/D^2 (R1, R2) for the P pass
 __global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, const double* __restrict__ nw,
-                              const SegD* __restrict__ carry, double* __restrict__ D, SegP* __restrict__ aggP) {
+                              const SegD* __restrict__ carry, double* __restrict__ D, double* __restrict__ R1,
+                              double* __restrict__ R2, SegP* __restrict__ aggP) {
     if (gate && *gate == 0.0) return;
     __shared__ SegD s_w[kThreads / 32];
     __shared__ SegP s_wp[kThreads / 32];
     const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int f[kScanItems];
     double v[kScanItems], n[kScanItems];
-    load8(i0, lo, hi, gstart, denom, nw, f, v, n);
+    load_items(i0, lo, hi, gstart, denom, nw, f, v, n);
     SegD a{0, 0.0};
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) a = seg_combine(a, SegD{f[q], v[q]});
@@ -789,6 +791,8 @@ __global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __r
             D[i] = run.v;
             const double r1 = n[q] / run.v;
             const double r2 = r1 / run.v;
+            R1[i] = r1;
+            R2[i] = r2;
             p = seg_combine(p, SegP{f[q], {r1, 0.0}, {r2, 0.0}});
         }
     }
@@ -798,25 +802,18 @@ __global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __r
 }
 
 __global__ void k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
-                              const double* __restrict__ D, const double* __restrict__ nw,
+                              const double* __restrict__ R1, const double* __restrict__ R2,
                               const SegP* __restrict__ carry, double* __restrict__ P1h, double* __restrict__ P1l,
                               double* __restrict__ P2h, double* __restrict__ P2l) {
     if (gate && *gate == 0.0) return;
     __shared__ SegP s_wp[kThreads / 32];
     const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int f[kScanItems];
-    double d[kScanItems], n[kScanItems];
-    load8(i0, lo, hi, gstart, D, nw, f, d, n);
     double r1[kScanItems], r2[kScanItems];
+    load_items(i0, lo, hi, gstart, R1, R2, f, r1, r2);          // identity (0) outside [lo, hi)
     SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
     #pragma unroll
-    for (int q = 0; q < kScanItems; ++q) {
-        const int i = i0 + q;
-        const bool in = i >= lo && i < hi;
-        r1[q] = in ? n[q] / d[q] : 0.0;
-        r2[q] = in ? r1[q] / d[q] : 0.0;
-        p = seg_combine(p, SegP{f[q], {r1[q], 0.0}, {r2[q], 0.0}});
-    }
+    for (int q = 0; q < kScanItems; ++q) p = seg_combine(p, SegP{f[q], {r1[q], 0.0}, {r2[q], 0.0}});
     const SegP ex = block_seg_excl(p, s_wp, nullptr);
     SegP run = seg_combine(carry[blockIdx.x], ex);
     #pragma unroll
