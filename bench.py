@@ -404,7 +404,7 @@ def leg_poisson(api):
     return out
 
 
-def leg_cox(api, n_strata=0, whole_fit=True):
+def leg_cox(api, n_strata=0, whole_fit=True, columns=0):
     """Breslow Cox at full size: K = 2M rows sorted by descending time, 50k
     sparse N(0,1) columns at 0.05 % (50M entries), Weibull(1.2) times, 70 %
     censoring, Laplace rate 0.1 (variance 200), default control; one whole
@@ -415,6 +415,8 @@ def leg_cox(api, n_strata=0, whole_fit=True):
     scaled by the column count."""
     t0 = time.perf_counter()
     data = D.synth_cox(n_strata=n_strata)
+    if columns:
+        data = _first_columns(data, columns)
     gen = time.perf_counter() - t0
     ds = api.Dataset(data, 0)
     var = D.laplace_variance(0.1)
@@ -434,11 +436,8 @@ def leg_cox(api, n_strata=0, whole_fit=True):
                          "update_entries": st["update_entries"],
                          "roofline": roofline_of(st["phase_bytes"][0], st["kernel_ms"],
                                                  "cyc_fit cox kernels (numerator, gradient, update, risk-set rescans)")}
-    sub = 500
-    from cyclops_b200.data import CyclopsData
-    sd = CyclopsData(model=data.model, y=data.y, col_format=data.col_format[:sub], col_ptr=data.col_ptr[:sub + 1],
-                     col_idx=data.col_idx[:int(data.col_ptr[sub])], val_ptr=data.val_ptr[:sub + 1],
-                     col_val=data.col_val[:int(data.val_ptr[sub])], pid=data.pid, time=data.time)
+    sub = min(500, data.J)
+    sd = _first_columns(data, sub)
     lib, kind = cpu_ref()
     from oracle import oracle as O
     t0 = time.perf_counter()
@@ -449,6 +448,14 @@ def leg_cox(api, n_strata=0, whole_fit=True):
     out["speedup_per_cycle_vs_cpu"] = cpu / spc
     ds.close()
     return out
+
+
+def _first_columns(data, n):
+    """The same rows with only the first n columns."""
+    from cyclops_b200.data import CyclopsData
+    return CyclopsData(model=data.model, y=data.y, col_format=data.col_format[:n], col_ptr=data.col_ptr[:n + 1],
+                       col_idx=data.col_idx[:int(data.col_ptr[n])], val_ptr=data.val_ptr[:n + 1],
+                       col_val=data.col_val[:int(data.val_ptr[n])], pid=data.pid, time=data.time)
 
 
 def leg_serving():
@@ -658,10 +665,32 @@ def main(argv=None):
     ap.add_argument("--extras", default="all",
                     help="further measurements at N=1: all, none, or a comma list of "
                          "mixed,poisson,cox,cox_strata,serving")
+    ap.add_argument("--workload", default="cv", choices=["cv", "poisson", "cox", "cox_strata", "serving"],
+                    help="cv: the headline CV grid (default); the others run that measurement alone and print "
+                         "its record (profiling runs)")
+    ap.add_argument("--cox-columns", type=int, default=0,
+                    help="with --workload cox*: keep only the first N columns (short profiling runs)")
     args = ap.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "cv":
+        return run_workload(args)
     return run_ours(args)
+
+
+def run_workload(args):
+    """One of the further measurements alone, as its own JSON record."""
+    from cyclops_b200 import api, build as B
+    B.build()
+    if args.workload == "poisson":
+        out = leg_poisson(api)
+    elif args.workload in ("cox", "cox_strata"):
+        out = leg_cox(api, n_strata=10_000 if args.workload == "cox_strata" else 0,
+                      whole_fit=args.workload == "cox", columns=args.cox_columns)
+    else:
+        out = leg_serving()
+    print(json.dumps({"workload": args.workload, **out}))
+    return 0
 
 
 if __name__ == "__main__":
