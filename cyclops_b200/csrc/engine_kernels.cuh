@@ -712,7 +712,7 @@ __device__ __forceinline__ void load_items(int i0, int lo, int hi, const int* __
 __host__ __device__ __forceinline__ int scan_base(int lo) { return lo & ~(kScanItems - 1); }
 
 // `gate`: when non-null and *gate == 0 (a zero coordinate step), nothing changed
-__global__ void k_scanD_tiles(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(kThreads, 4) k_scanD_tiles(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, SegD* __restrict__ agg) {
     if (gate && *gate == 0.0) return;
     __shared__ SegD s_w[kThreads / 32];
@@ -737,7 +737,9 @@ __device__ void scan_carry(int n, T* agg, T init) {
     acc.f = 0;
     T id = acc;
     for (int i = b; i < e; ++i) acc = seg_combine(acc, agg[i]);
-    T excl = block_exclusive_scan(acc, id, (T*)nullptr);
+    __shared__ T s_w[kThreads / 32];
+    (void)id;
+    T excl = block_seg_excl(acc, s_w, (T*)nullptr);     // warp shuffles, then the warps' totals
     T run = seg_combine(init, excl);
     for (int i = b; i < e; ++i) {
         const T t = agg[i];
@@ -766,7 +768,7 @@ __global__ void k_carryP(const double* gate, int n, SegP* agg, int lo, const int
 }
 
 // writes D and the P terms r1 = n/D, r2 = n/D^2 (R1, R2) for the P pass
-__global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, const double* __restrict__ nw,
                               const SegD* __restrict__ carry, double* __restrict__ D, double* __restrict__ R1,
                               double* __restrict__ R2, SegP* __restrict__ aggP) {
@@ -801,7 +803,7 @@ __global__ void k_scanD_write(const double* gate, int lo, int hi, const int* __r
     if (threadIdx.x == 0) aggP[blockIdx.x] = totp;
 }
 
-__global__ void k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(kThreads, 4) k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ R1, const double* __restrict__ R2,
                               const SegP* __restrict__ carry, double* __restrict__ P1h, double* __restrict__ P1l,
                               double* __restrict__ P2h, double* __restrict__ P2l) {
