@@ -60,7 +60,8 @@ class RunStats(C.Structure):
                 ("coordinate_steps", C.c_double), ("index_entries", C.c_double), ("cycles", C.c_double),
                 ("launches", C.c_int), ("phases", C.c_int), ("phase_ms", C.c_double * 2),
                 ("phase_bytes", C.c_double * 2), ("phase_state_bytes", C.c_int * 2),
-                ("cluster_ctas", C.c_int)]
+                ("cluster_ctas", C.c_int), ("batch_cap", C.c_int), ("batch_shared_rows", C.c_int),
+                ("batch_levels", C.c_int)]
 
 
 # name -> argtypes (all return int status unless listed in _RESTYPE)

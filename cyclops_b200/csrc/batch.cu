@@ -701,6 +701,17 @@ constexpr int kRunItems = 8;
 // k_batch).  Columns of at most kBatchCap entries in every CTA's rows join.
 constexpr int kDirtyMax = 32;
 constexpr int kBatchCap = 256;
+
+// The batch shape of an 8-fit group's plan: columns with at most `cap`
+// entries in every CTA's rows are short (batched, a warp per column; the
+// rest stream through the whole CTA), a batch shares at most `dmax` rows
+// between its columns and replays at most `lvl` levels.  The defaults are
+// the largest the kernel's shared memory allows; the shape tuner
+// (tuned_shape) may pick smaller ones for a problem.
+struct BatchShape {
+    int cap = 256, dmax = 32, lvl = 8;
+    bool operator==(const BatchShape& o) const { return cap == o.cap && dmax == o.dmax && lvl == o.lvl; }
+};
 // levels of the serial replay a batch may have (each costs a step chain)
 constexpr int kLevelMax = kRunMax;
 
@@ -1719,7 +1730,7 @@ __global__ void k_batch_llfixed(int K, int G, int F, const double* c, const T* w
 // `batch_rows` > 0 also closes a batch before its entries in any one CTA's
 // rows would exceed that many (the batch cache holds them all).
 static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const std::vector<int>& fixb, int cap,
-                         bool allow, int dmax, int batch_rows = 0) {
+                         bool allow, int dmax, int batch_rows = 0, int lvl_max = kLevelMax) {
     const int J = ds.J, K = ds.K, C = (int)rpart.size() - 1;
     RunPlan P;
     P.len.assign(J, 1);
@@ -1789,7 +1800,7 @@ static RunPlan plan_runs(const Dataset& ds, const std::vector<int>& rpart, const
         bool full = false;
         if (batch_rows > 0)
             for (int r = 0; r < C; ++r) full |= bsum[r] + cnt[r] > batch_rows;
-        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > kLevelMax || full)) {
+        if (start >= 0 && (len == kRunMax || (int)shared.size() + fresh > dmax || level > lvl_max || full)) {
             close();
             level = 1;
         }
@@ -1872,6 +1883,7 @@ struct BatchRunner {
     Dataset& ds;
     cudaStream_t stream;
     int F, G, ngroups, Fp, C;
+    BatchShape shape;
     std::vector<int> rpart;
     DevBuf<int> d_rpart, d_split, d_fixb, d_ptype, d_active, d_iter, d_flag;
     DevBuf<int> d_runlen, d_runlvl, d_rundr0, d_runnd, d_drow, d_deptr, d_ded, d_dee;
@@ -1880,7 +1892,8 @@ struct BatchRunner {
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
 
-    BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_, int C_ = 0) : ds(d), stream(s), F(F_), G(G_) {
+    BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_, int C_ = 0, BatchShape sh = BatchShape{})
+        : ds(d), stream(s), F(F_), G(G_), shape(sh) {
         ngroups = (F + G - 1) / G;
         Fp = ngroups * G;
         const int K = ds.K;
@@ -1942,14 +1955,21 @@ struct BatchRunner {
             // batches are planned without regard to the cache: those whose
             // entries fit it in every CTA take the cached path, the rest stream
             const int brows = 0;
+            const int cap = rows8 ? shape.cap : (32 / G) * kRunItems;
+            const int dmax = rows8 ? shape.dmax : 0;
+            const int lvl = rows8 ? shape.lvl : kLevelMax;
             for (auto& pl : ds.run_plans)
-                if (pl.C == C && pl.G == G && pl.batch_rows == brows && pl.fixed == fixed_cols) plan = &pl;
+                if (pl.C == C && pl.G == G && pl.batch_rows == brows && pl.cap == cap && pl.dmax == dmax &&
+                    pl.max_levels == lvl && pl.fixed == fixed_cols)
+                    plan = &pl;
             if (!plan) {
-                RunPlan pl = plan_runs(ds, rpart, fixb, rows8 ? kBatchCap : (32 / G) * kRunItems,
-                                       model_independent(ds.model), rows8 ? kDirtyMax : 0, brows);
+                RunPlan pl = plan_runs(ds, rpart, fixb, cap, model_independent(ds.model), dmax, brows, lvl);
                 pl.C = C;
                 pl.G = G;
                 pl.batch_rows = brows;
+                pl.cap = cap;
+                pl.dmax = dmax;
+                pl.max_levels = lvl;
                 pl.fixed = fixed_cols;
                 ds.run_plans.push_back(std::move(pl));
                 plan = &ds.run_plans.back();
@@ -2160,8 +2180,8 @@ template <class T>
 float probe_cycle(Dataset& ds, cudaStream_t stream, int F, int G, int C, const cyc_prior& prior,
                   const cyc_fit_spec* specs, const std::vector<double>& beta, const std::vector<double>& hd,
                   const int* d_fold, int n_folds, const std::vector<int>* fit_fold, const cyc_control& ctl,
-                  const std::vector<int>& fixed_cols) {
-    BatchRunner<T> r(ds, stream, F, G, C);
+                  const std::vector<int>& fixed_cols, BatchShape shape = BatchShape{}) {
+    BatchRunner<T> r(ds, stream, F, G, C, shape);
     if (d_fold) r.set_folds(d_fold, n_folds, *fit_fold);
     r.setup(prior, specs, beta, hd, fixed_cols);
     cyc_control one = ctl;
@@ -2198,6 +2218,65 @@ int tuned_cluster(Dataset& ds, cudaStream_t stream, int F, int G, const cyc_prio
     }
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     tuned_sizes()[key] = best;
+    return best;
+}
+
+// ---- batch-shape tuner -------------------------------------------------------
+// Which columns are short (batched, a warp per column) and which stream
+// through the whole CTA is a question of the columns' densities: the bound
+// `cap` on a short column's entries per CTA splits the columns into the two
+// buckets.  With it go the rows a batch may share (`dmax`) and the replay
+// levels it may take (`lvl`).  For an 8-fit group of an independent-rows
+// model large enough to amortise it (the cluster tuner's criteria), the
+// tuner times one cycle of the real problem at the chosen cluster size for
+// the default shape and then, one parameter at a time, for smaller
+// settings (cap 128, 64; dmax 16; lvl 2), keeping each change that is
+// faster; the choice is cached per problem shape for the process.
+// CYC_BATCH_SHAPE="cap,dmax,lvl" sets it without probing.
+std::map<std::pair<TuneKey, int>, BatchShape>& tuned_shapes() {
+    static auto* m = new std::map<std::pair<TuneKey, int>, BatchShape>();   // lives to process exit
+    return *m;
+}
+
+BatchShape tuned_shape(Dataset& ds, cudaStream_t stream, int F, int G, int C, const cyc_prior& prior,
+                       const cyc_fit_spec* specs, const std::vector<double>& beta, const std::vector<double>& hd,
+                       const int* d_fold, int n_folds, const std::vector<int>* fit_fold, const cyc_control& ctl,
+                       const std::vector<int>& fixed_cols) {
+    BatchShape best;
+    if (const char* e = std::getenv("CYC_BATCH_SHAPE")) {
+        int a = best.cap, b = best.dmax, c = best.lvl;
+        if (std::sscanf(e, "%d,%d,%d", &a, &b, &c) == 3) {
+            best.cap = std::max(1, std::min(kBatchCap, a));
+            best.dmax = std::max(0, std::min(kDirtyMax, b));
+            best.lvl = std::max(1, std::min(kLevelMax, c));
+        }
+        return best;
+    }
+    const double work = (double)F * (double)(ds.nnz_idx + ds.nnz_val);
+    if (G != 8 || !model_independent(ds.model) || F < 16 || work < 1e8) return best;
+    const TuneKey key{ds.model, ds.K, ds.J, F, G, ctl.precision, d_fold ? n_folds : 0, fixed_cols, ds.nnz_idx};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        auto it = tuned_shapes().find({key, C});
+        if (it != tuned_shapes().end()) return it->second;
+    }
+    auto time = [&](const BatchShape& sh) {
+        return ctl.precision == CYC_MIXED
+                   ? probe_cycle<float>(ds, stream, F, G, C, prior, specs, beta, hd, d_fold, n_folds, fit_fold, ctl,
+                                        fixed_cols, sh)
+                   : probe_cycle<double>(ds, stream, F, G, C, prior, specs, beta, hd, d_fold, n_folds, fit_fold,
+                                         ctl, fixed_cols, sh);
+    };
+    float best_ms = time(best);
+    auto consider = [&](BatchShape sh) {
+        const float ms = time(sh);
+        if (ms < best_ms) { best = sh; best_ms = ms; }
+    };
+    for (int cap : {128, 64}) { BatchShape sh = best; sh.cap = cap; consider(sh); }
+    { BatchShape sh = best; sh.dmax = 16; consider(sh); }
+    { BatchShape sh = best; sh.lvl = 2; consider(sh); }
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    tuned_shapes()[{key, C}] = best;
     return best;
 }
 
@@ -2295,11 +2374,17 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         NvtxRange range("cyclops batch: cluster tuner");
         C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_cols);
     }
+    BatchShape shape;
+    {
+        NvtxRange range("cyclops batch: shape tuner");
+        shape = tuned_shape(ds, stream, F, G, C, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl,
+                            fixed_cols);
+    }
     int phase = 0;
     if (ctl->precision == CYC_MIXED) {
         // FP32 state + compensated sums to the looser tolerance, then the FP64 polish below
         NvtxRange range("cyclops batch: fp32 phase");
-        BatchRunner<float> r32(ds, stream, F, G, C);
+        BatchRunner<float> r32(ds, stream, F, G, C, shape);
         if (d_fold) r32.set_folds(d_fold, n_folds, *fit_fold);
         r32.setup(*prior, specs, beta, hd, fixed_cols);
         float ms = 0.f;
@@ -2310,7 +2395,7 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         std::fill(hd.begin(), hd.end(), ctl->initial_bound);
     }
     NvtxRange range64("cyclops batch: fp64 phase");
-    BatchRunner<double> r64(ds, stream, F, G, C);
+    BatchRunner<double> r64(ds, stream, F, G, C, shape);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
     r64.setup(*prior, specs, beta, hd, fixed_cols);
     float ms = 0.f;
@@ -2333,6 +2418,11 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     }
     if (pll) pll->assign(p.begin(), p.begin() + F);
     st.cluster_ctas = C;
+    if (G == 8 && model_independent(ds.model)) {
+        st.batch_cap = shape.cap;
+        st.batch_shared_rows = shape.dmax;
+        st.batch_levels = shape.lvl;
+    }
     set_last_stats(st);
 }
 

@@ -206,6 +206,8 @@ struct ColView {
 struct RunPlan {
     int C = 0, G = 0;
     int batch_rows = 0;         // cap on a batch's entries in any one CTA's rows (0: none)
+    int cap = 0, dmax = 0, max_levels = 0;   // the batch shape it was planned with (short-column
+                                             // bound, shared rows, replay levels)
     std::vector<int> fixed;     // columns held fixed besides the offset (ascending)
     std::vector<int> len;       // J: columns in the batch starting here (1 = alone), 0 inside a batch
     std::vector<int> lvl;       // J: level of the column in its batch (1 + max level of earlier sharers)

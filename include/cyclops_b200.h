@@ -101,10 +101,11 @@ typedef struct cyc_dataset cyc_dataset;
 typedef struct cyc_engine cyc_engine;
 
 const char* cyc_last_error(void);
-/* ABI revision: 2 since cyc_control gained use_kkt_swindle, cyc_fit_spec
- * gained fixed / n_fixed and cyc_run_stats gained cluster_ctas (fields
- * appended; zero-initialise these structs, e.g. `cyc_fit_spec s = {0};`). */
-#define CYC_ABI_VERSION 2
+/* ABI revision: 3 since cyc_run_stats gained batch_cap, batch_shared_rows
+ * and batch_levels (2: cyc_control gained use_kkt_swindle, cyc_fit_spec
+ * fixed / n_fixed, cyc_run_stats cluster_ctas); fields are appended:
+ * zero-initialise these structs, e.g. `cyc_fit_spec s = {0};`. */
+#define CYC_ABI_VERSION 3
 int cyc_version(void);
 
 /* Copy a dataset to device `device`.  Replaces the host-side ModelData the
@@ -345,6 +346,11 @@ typedef struct {
     int phase_state_bytes[2];   /* bytes per (row, fit) state element of each phase */
     int cluster_ctas;           /* batched solves: CTAs per thread-block cluster (the
                                    tuner's choice, or CYC_BATCH_CLUSTER); 0 otherwise */
+    int batch_cap;              /* batched solves of 8-fit groups (lr, pr): the batch shape the
+                                   shape tuner chose (or CYC_BATCH_SHAPE): columns with at most
+                                   this many entries in every CTA's rows are batched, */
+    int batch_shared_rows;      /* a batch shares at most this many rows between its columns, */
+    int batch_levels;           /* and replays at most this many levels; 0 otherwise */
 } cyc_run_stats;
 int cyc_last_run_stats(cyc_run_stats* out);
 
