@@ -593,7 +593,11 @@ def run_ours(args):
             "config": desc,
             "run": {"precision": args.precision, "mean_cycles_per_fit": mean_cycles,
                     "max_cycles_per_fit": int(max(f.iterations for f in res.fits)),
-                    "converged": int(sum(f.return_flag == 0 for f in res.fits))},
+                    "converged": int(sum(f.return_flag == 0 for f in res.fits)),
+                    "cluster_ctas": st.get("cluster_ctas"),
+                    "batch_shape": {"short_column_entries_per_cta": st.get("batch_cap"),
+                                    "shared_rows": st.get("batch_shared_rows"),
+                                    "replay_levels": st.get("batch_levels")}},
             "clocks": clocks,
             "e2e": {"value": e2e, "unit": "fits/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
