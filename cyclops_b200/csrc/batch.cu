@@ -25,12 +25,15 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -2280,6 +2283,66 @@ BatchShape tuned_shape(Dataset& ds, cudaStream_t stream, int F, int G, int C, co
     return best;
 }
 
+// Fits the persistent kernel does not take -- Cox, whose risk sets follow
+// each fit's weights and are rescanned after every moving coordinate, and
+// fits under the KKT swindle, each with its own active set -- run
+// concurrently: one device-resident single-fit CCD (cyc_fit: its own engine,
+// stream and CUDA graphs) per host thread, up to CYC_CONCURRENT_FITS (default
+// 8) at a time, so their kernels overlap on the device.  Each fit is the one
+// cyc_fit computes alone.
+void run_fits_concurrently(cyc_dataset* dsh, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
+                           const cyc_control* ctl, cyc_fit_result* out) {
+    int slots = 8;
+    if (const char* e = std::getenv("CYC_CONCURRENT_FITS")) slots = std::max(1, std::atoi(e));
+    slots = std::min(slots, F);
+    for (int f = 0; f < F; ++f)
+        if (specs[f].start_beta) { dsh->ds.ensure_csr(); break; }     // built once, before the threads
+    std::atomic<int> next{0};
+    std::mutex mutex;                  // guards the error and the summed statistics
+    int err_status = CYC_OK;
+    std::string err_text;
+    cyc_run_stats sum{};
+    auto worker = [&] {
+        for (;;) {
+            const int f = next.fetch_add(1);
+            if (f >= F) return;
+            {
+                std::lock_guard<std::mutex> lk(mutex);
+                if (err_status != CYC_OK) return;
+            }
+            const int rc = cyc_fit(dsh, prior, &specs[f], ctl, &out[f]);
+            std::lock_guard<std::mutex> lk(mutex);
+            if (rc != CYC_OK) {
+                if (err_status == CYC_OK) { err_status = rc; err_text = cyc_last_error(); }
+                return;
+            }
+            cyc_run_stats st{};
+            cyc_last_run_stats(&st);   // this worker thread's fit
+            sum.algorithmic_bytes += st.algorithmic_bytes;
+            sum.gradient_entries += st.gradient_entries;
+            sum.update_entries += st.update_entries;
+            sum.coordinate_steps += st.coordinate_steps;
+            sum.index_entries += st.index_entries;
+            sum.cycles += st.cycles;
+            sum.phase_bytes[0] += st.phase_bytes[0];
+            sum.phase_state_bytes[0] = st.phase_state_bytes[0];
+        }
+    };
+    const long long launches0 = cyc_launch_count();
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < slots; ++t) pool.emplace_back(worker);
+    for (auto& t : pool) t.join();
+    CYC_REQUIRE(err_status == CYC_OK, err_status, err_text);
+    // the fits overlap: the time is the whole concurrent section's (every
+    // fit has synchronised its stream when cyc_fit returns)
+    sum.kernel_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    sum.launches = (int)(cyc_launch_count() - launches0);
+    sum.phases = 1;
+    sum.phase_ms[0] = sum.kernel_ms;
+    set_last_stats(sum);
+}
+
 // The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` (fold id
 // per row, `n_folds` of them) and `fit_fold` (the held-out fold of each fit)
 // select the CV-grid weights; otherwise `specs[f].weights`.
@@ -2433,13 +2496,11 @@ extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc
     return guarded([&] {
         NvtxRange range("cyc_batch_fit");
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
-        if (ctl->use_kkt_swindle) {
-            // every fit carries its own active set, which one batch kernel
-            // cannot share: each runs as cyc_fit
-            for (int f = 0; f < F; ++f) {
-                const int rc = cyc_fit(dsh, prior, &specs[f], ctl, &out[f]);
-                CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
-            }
+        if (ctl->use_kkt_swindle || model_cumulative(dsh->ds.model)) {
+            // every fit carries its own active set (swindle) or its own risk
+            // sets (cox), which one batch kernel cannot share: the fits run
+            // as concurrent cyc_fit calls
+            run_fits_concurrently(dsh, prior, specs, F, ctl, out);
             return;
         }
         run_batch(dsh->ds, prior, specs, F, ctl, out, nullptr, 0, nullptr, nullptr);
@@ -2457,7 +2518,8 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
         Dataset& ds = dsh->ds;
         for (int k = 0; k < ds.K; ++k)
             CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
-        if (ctl->use_kkt_swindle) {          // per-fit active sets: the per-fit path, unit weights
+        if (ctl->use_kkt_swindle || model_cumulative(ds.model)) {
+            // per-fit active sets (swindle) or risk sets (cox): the per-fit path, unit weights
             std::vector<double> ones(ds.K, 1.0);
             const int rc = cyc_cv_grid_fit_weighted(dsh, prior, fold_of_row, n_folds, ones.data(), variances, n_var,
                                                     ctl, out, pred_loglik, grid_mean);
@@ -2621,8 +2683,8 @@ extern "C" int cyc_cv_auto_search(cyc_dataset* dsh, const cyc_prior* prior, cons
         for (int step = 0; step < 50; ++step) {            // MAX_STEPS, AutoSearchCrossValidationDriver.cpp:28
             std::vector<double> pll_all;
             for (int r = 0; r < n_reps; ++r) {
-                if (row_weights || ctl->use_kkt_swindle) {
-                    // observation weights or per-fit active sets: the weighted grid path
+                if (row_weights || ctl->use_kkt_swindle || model_cumulative(ds.model)) {
+                    // observation weights, per-fit active sets or risk sets: the weighted grid path
                     std::vector<double> w(row_weights ? row_weights : ones.data(),
                                           (row_weights ? row_weights : ones.data()) + ds.K);
                     std::vector<double> pll(n_folds);
@@ -2713,11 +2775,8 @@ extern "C" int cyc_cv_grid_fit_weighted(cyc_dataset* dsh, const cyc_prior* prior
             specs[i].weights = train.data() + (size_t)(i % n_folds) * K;
             specs[i].variance = variances[i / n_folds];
         }
-        if (ctl->use_kkt_swindle) {          // per-fit active sets: each fit as cyc_fit
-            for (int i = 0; i < F; ++i) {
-                const int rc = cyc_fit(dsh, prior, &specs[i], ctl, &out[i]);
-                CYC_REQUIRE(rc == CYC_OK, rc, cyc_last_error());
-            }
+        if (ctl->use_kkt_swindle || model_cumulative(ds.model)) {   // per-fit active sets or risk sets
+            run_fits_concurrently(dsh, prior, specs.data(), F, ctl, out);
         } else {
             run_batch(ds, prior, specs.data(), F, ctl, out, nullptr, 0, nullptr, nullptr);
         }

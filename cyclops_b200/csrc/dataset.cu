@@ -93,6 +93,7 @@ static void upload(DevBuf<T>& buf, const T* src, size_t n) {
 }
 
 void Dataset::ensure_csr() {
+    std::lock_guard<std::mutex> lock(csr_mutex);
     if (have_csr) return;
     StreamScope scope(stream);
     // counting sort by row; columns visited in ascending order, so each row

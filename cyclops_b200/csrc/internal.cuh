@@ -5,6 +5,7 @@
 #include <nvtx3/nvToolsExt.h>
 #include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -244,7 +245,9 @@ struct Dataset {
     DevBuf<double> d_y, d_time;
     DevBuf<int> d_strat, d_strat_ptr;
 
-    // row-major copy for computeXBeta (built on first use)
+    // row-major copy for computeXBeta (built on first use, once: fits that run
+    // concurrently on one dataset may ask for it together)
+    std::mutex csr_mutex;
     bool have_csr = false;
     DevBuf<long long> d_row_ptr;
     DevBuf<int> d_row_col;

@@ -221,7 +221,12 @@ int cyc_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* spec,
             const cyc_control* control, cyc_fit_result* out);
 
 /* F fits sharing `ds`, advanced together coordinate by coordinate in one
- * persistent kernel (lr, pr, clr, cpr).  Results in `out[0..F)`. */
+ * persistent kernel (lr, pr, clr, cpr).  Results in `out[0..F)`.  Cox fits
+ * (each with its own risk sets under its weights) and fits under
+ * use_kkt_swindle (each with its own active set) run instead as concurrent
+ * cyc_fit solves, up to CYC_CONCURRENT_FITS (default 8) at a time on their
+ * own streams; each result is the one cyc_fit gives alone.  Run statistics
+ * then sum the fits' counts, with kernel_ms the whole section's time. */
 int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* specs, int F,
                   const cyc_control* control, cyc_fit_result* out);
 
@@ -233,7 +238,8 @@ int cyc_batch_fit(cyc_dataset* ds, const cyc_prior* prior, const cyc_fit_spec* s
  * (ModelSpecifics.hpp:652-690).  The per-fold, per-grid-point loop of
  * GridSearchCrossValidationDriver / AbstractCrossValidationDriver
  * (src/cyclops/drivers/GridSearchCrossValidationDriver.cpp:96-140,
- * AbstractCrossValidationDriver.cpp:131-261) as one batched solve.
+ * AbstractCrossValidationDriver.cpp:131-261) as one batched solve (cox,
+ * and use_kkt_swindle: as cyc_cv_grid_fit_weighted with unit weights).
  * `pred_loglik` (F values, NaN where the fit did not converge) and
  * `grid_mean` (n_var values: mean over folds ignoring NaN) may be NULL. */
 int cyc_cv_grid_fit(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds,
@@ -280,8 +286,9 @@ int cyc_profile_log_likelihood_batch(cyc_dataset* ds, const cyc_prior* prior, co
 /* cyc_cv_grid_fit with observation weights (the fit's weights handed to
  * the CV selector, CrossValidationSelector.cpp:72-124): fit (variance v,
  * fold f) trains on the rows outside fold f at their weights and is scored
- * on fold f's rows at their weights (getComplement).  lr, pr, clr, cpr;
- * cold starts; outputs as cyc_cv_grid_fit. */
+ * on fold f's rows at their weights (getComplement).  Fits as
+ * cyc_batch_fit (cox and use_kkt_swindle: concurrent cyc_fit solves); cold
+ * starts; outputs as cyc_cv_grid_fit. */
 int cyc_cv_grid_fit_weighted(cyc_dataset* ds, const cyc_prior* prior, const int* fold_of_row, int n_folds,
                              const double* row_weights, const double* variances, int n_var,
                              const cyc_control* control, cyc_fit_result* out, double* pred_loglik,
@@ -298,8 +305,8 @@ int cyc_cv_grid_fit_weighted(cyc_dataset* ds, const cyc_prior* prior, const int*
  * left out) and lets the search propose the next variance; at most 50
  * steps.  fold_of_row: n_reps x K fold ids (e.g. from cyc_cv_fold_weights);
  * row_weights: K observation weights (NULL: all 1), used as
- * cyc_cv_grid_fit_weighted uses them; with use_kkt_swindle the folds run
- * one by one as cyc_fit.
+ * cyc_cv_grid_fit_weighted uses them; cox folds and use_kkt_swindle folds
+ * run as concurrent cyc_fit solves.
  * Returns the variance the search settles on and its expected value, and
  * the first max_tried points tried (variance, mean, stdev; *n_tried counts
  * all). */

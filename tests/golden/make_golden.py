@@ -385,7 +385,8 @@ CV_AUTO_CASES = [("lr_laplace_small", D.PRIOR_LAPLACE, True, -1.0),
                  ("lr_c1", D.PRIOR_LAPLACE, True, -1.0),
                  ("clr_laplace", D.PRIOR_LAPLACE, False, -1.0),
                  ("cpr_normal", D.PRIOR_NORMAL, False, -1.0),
-                 ("lr_zhang_oles", D.PRIOR_LAPLACE, True, 0.5)]
+                 ("lr_zhang_oles", D.PRIOR_LAPLACE, True, 0.5),
+                 ("cox_strata", D.PRIOR_LAPLACE, True, -1.0)]
 
 
 def save_cv_auto():

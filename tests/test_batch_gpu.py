@@ -93,12 +93,56 @@ def test_cv_folds_times_grid(cuda_lib):
         assert_contract(fit, ref, what=i)
 
 
-def test_batch_rejects_cox(cuda_lib):
-    from cyclops_b200 import api, _native
-    data, s = load_golden("cox_laplace")
-    with pytest.raises(_native.CyclopsError) as ei:
-        api.batch_fit(data, api.create_prior("laplace", 1.0), [1.0, 2.0])
-    assert ei.value.status == 4
+@pytest.mark.parametrize("name", ["cox_laplace", "cox_strata", "cox_ties_weighted"])
+@pytest.mark.parametrize("nfits", [1, 6, 11])
+def test_cox_batch_fits_match_reference(cuda_lib, name, nfits):
+    """Cox fits of a batch (each with the risk sets of its own weights) run
+    as concurrent single-fit solves: every fit is the oracle's at its
+    weights and variance, under the precision contract."""
+    from cyclops_b200 import api
+    data, s = load_golden(name)
+    rng = np.random.default_rng(100 + nfits)
+    var0 = float(s["variance"])
+    base = np.ones(data.K) if s["weights"] is None else np.asarray(s["weights"], float)
+    variances = [var0 * (1.0 + 0.5 * (f % 3)) for f in range(nfits)]
+    weights = [s["weights"] if f == 0 else base * (rng.random(data.K) > 0.2) for f in range(nfits)]
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    fits = api.batch_fit(data, prior, variances, weights, api.create_control())
+    st = api.last_run_stats()
+    assert st["cycles"] == sum(f.iterations for f in fits) and st["launches"] > 0
+    for f in range(nfits):
+        ref = _ref_fit(data, int(s["prior"]), variances[f], weights[f])
+        assert_contract(fits[f], ref, what=(name, f))
+
+
+def test_cox_bootstrap_replicates(cuda_lib):
+    """Bootstrap replicates of a stratified Cox fit (BootstrapSelector's
+    per-row draws) as one cyc_batch_fit call."""
+    from cyclops_b200 import api
+    data, s = load_golden("cox_strata")
+    W = api.bootstrap_weights(data.K, 5, 7)
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    fits = api.batch_fit(data, prior, [float(s["variance"])] * 5, list(W), api.create_control())
+    for r, fit in enumerate(fits):
+        assert_contract(fit, _ref_fit(data, int(s["prior"]), float(s["variance"]), W[r]), what=r)
+
+
+def test_concurrent_fit_count_does_not_change_fits(cuda_lib, monkeypatch):
+    """One, three or eight Cox fits in flight at a time: each fit is its own
+    single-fit solve, so the results are bitwise the same."""
+    from cyclops_b200 import api
+    data, s = load_golden("cox_strata")
+    rng = np.random.default_rng(3)
+    weights = [(rng.random(data.K) > 0.25).astype(float) for _ in range(9)]
+    prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
+    got = {}
+    for slots in (1, 3, 8):
+        monkeypatch.setenv("CYC_CONCURRENT_FITS", str(slots))
+        got[slots] = api.batch_fit(data, prior, [float(s["variance"])] * 9, weights, api.create_control())
+    for slots in (3, 8):
+        for a, b in zip(got[1], got[slots]):
+            assert np.array_equal(a.beta, b.beta) and a.iterations == b.iterations
+            assert a.log_likelihood == b.log_likelihood
 
 
 @pytest.mark.parametrize("name", ["lr_laplace_small", "clr_laplace", "pr_laplace_weighted"])

@@ -11,6 +11,7 @@ import numpy as np
 import pytest
 
 from conftest import ROOT, cvauto_names, load_golden
+from cyclops_b200 import data as D
 from oracle import cv_auto
 from oracle import oracle as O
 
@@ -94,16 +95,19 @@ def test_library_variance_search_replays_reference_trails(tmp_path):
 
 
 @pytest.mark.parametrize("name,weighted", [("lr_laplace_small", True), ("lr_laplace_small", False),
-                                           ("cpr_normal", True)])
+                                           ("cpr_normal", True), ("cox_laplace", False), ("cox_strata", True)])
 def test_restated_grid_cv_matches_reference_driver(name, weighted):
     """The reference's GridSearchCrossValidationDriver (cold starts), with
     the fit's observation weights as the selector's original weights: each
     fold trains at the weights outside it and is scored at the weights
     inside it (getComplement) -- the semantics cyc_cv_grid_fit_weighted
-    implements -- reproduced fold by fold by the restatement."""
+    implements -- reproduced fold by fold by the restatement.  Cox folds
+    are by row (R's "auto" selector picks byRow when a stratum holds at
+    least as many rows as there are strata, R/ModelFit.R:174-184), and a
+    held-out fold is scored against the risk sets of the training rows."""
     data, s = load_golden(name)
     prior = int(s["prior"])
-    by_row = data.pid is None
+    by_row = data.pid is None or data.model == D.COX
     w = (1.0 + (np.arange(data.K) % 3)) if weighted else None
     pts, vals, fp = O.ref().cv_grid(data, prior, fold=5, seed=77, by_row=by_row, lower=0.05, upper=5.0,
                                     grid_steps=3, weights=w)

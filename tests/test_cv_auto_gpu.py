@@ -1,6 +1,7 @@
 """Auto-search cross-validation on the GPU (cyc_cv_auto_search: every step's
-folds one batched solve) against the reference's own
-AutoSearchCrossValidationDriver (fixtures tests/golden/cvauto_*.npz)."""
+folds one batched solve, Cox folds concurrent single-fit solves) against the
+reference's own AutoSearchCrossValidationDriver (fixtures
+tests/golden/cvauto_*.npz, a stratified Cox case among them)."""
 import os
 
 import numpy as np

@@ -170,3 +170,33 @@ def test_weighted_cv_grid_matches_oracle(cuda_lib, name):
         assert_contract(fit, ref, what=i)
         want = O.port().predictive_loglik(data, ref.beta, held, weights=train)
         assert abs(res.pred_loglik[i] - want) <= 1e-8 * abs(want), (i, res.pred_loglik[i], want)
+
+
+@pytest.mark.parametrize("name,weighted", [("cox_laplace", False), ("cox_strata", False), ("cox_ties_weighted", True)])
+def test_cox_cv_grid_matches_oracle(cuda_lib, name, weighted):
+    """Cox cross-validation grids (folds by row, R's choice for these
+    shapes): every fold's fit is the oracle's on its training weights, and
+    its held-out predictive log likelihood is the oracle's, scored against
+    the training rows' risk sets."""
+    from cyclops_b200 import api
+    from oracle import oracle as O
+    data, s = load_golden(name)
+    n_folds = 5
+    masks = api.cv_fold_weights(data.K, n_folds, 23)
+    folds = api.fold_ids_from_weights(masks)
+    w = np.asarray(s["weights"], float) * (1.0 + (np.arange(data.K) % 2)) if weighted else None
+    variances = [float(s["variance"]), 4.0 * float(s["variance"])]
+    prior = api.PriorSpec(int(s["prior"]), 1.0, exclude_for(data))
+    res = api.cv_grid_fit(data, prior, folds, n_folds, variances, api.create_control(), weights=w)
+    base = np.ones(data.K) if w is None else w
+    for i, fit in enumerate(res.fits):
+        v, f = variances[i // n_folds], i % n_folds
+        train = masks[f] * base
+        held = (1.0 - masks[f]) * base
+        ref = O.port().fit(data, int(s["prior"]), v, control=O.make_control(), weights=train)
+        assert ref.return_flag == 0
+        assert_contract(fit, ref, what=(name, i))
+        want = O.port().predictive_loglik(data, ref.beta, held, weights=train)
+        assert abs(res.pred_loglik[i] - want) <= 1e-8 * abs(want), (i, res.pred_loglik[i], want)
+    for v in range(len(variances)):
+        assert rel_err(res.grid_mean[v], np.mean(res.pred_loglik[v * n_folds:(v + 1) * n_folds])) < 1e-12
