@@ -65,6 +65,8 @@ struct BatchArgs {
     const int* strat;             // K (grouped)
     const int* strat_ptr;         // S+1 (grouped)
     const int* fixb;              // J
+    const unsigned char* lane_fix; // [groups][J]: fits (bit f) holding column j at its value in this
+                                  // launch (the inactive columns of the KKT swindle), or null
     const int* ptype;             // J
     void* xb;                     // [groups][K][G] T
     const void* w;                // [groups][K][G] T
@@ -781,6 +783,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     __shared__ int s_cbo[kRunMax + 1];     // the open batch's columns in the batch cache
     // the current chunk of coordinates
     __shared__ int c_fmt[kChunk], c_fix[kChunk], c_pt[kChunk], c_e0[kChunk], c_e1[kChunk], c_run[kChunk];
+    __shared__ unsigned char c_lfix[kChunk];   // fits holding the coordinate fixed (active-set passes)
     __shared__ int c_lvl[kChunk], c_nd[kChunk], c_dr0[kChunk], c_de0[kChunk + 1];
     __shared__ long long c_cp[kChunk], c_vp[kChunk];
     __shared__ int c_off[kChunk];          // staged offset of coordinate q, -1 if not staged
@@ -863,7 +866,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         // over the cluster; called by the thread whose fit lane is f
         auto coord_step = [&](int qq, int f, double g, double h) -> double {
             g -= c_xjy[qq][f];                             // :1181-1183
-            if (s_done[f]) return 0.0;
+            if (s_done[f] || ((c_lfix[qq] >> f) & 1u)) return 0.0;
             if (h < 0.0) { g = 0.0; h = 0.0; }             // :1407-1410
             const double b = c_beta[qq][f];
             double hd = c_hd[qq][f];
@@ -899,6 +902,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             const int f0 = A.fmt[j];
             c_fmt[q] = f0;
             c_fix[q] = A.fixb[j];
+            c_lfix[q] = A.lane_fix ? A.lane_fix[(size_t)grp * A.J + j] : 0;
             c_pt[q] = A.ptype[j];
             c_run[q] = A.run_len[j];
             c_lvl[q] = A.run_lvl[j];
@@ -959,6 +963,13 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         while (q < jn) {
             const int L = c_run[q];
             if (c_fix[q] || L <= 0) { ++q; continue; }
+            if (A.lane_fix) {
+                // a batch (or column) that every running fit holds fixed is
+                // skipped: its steps would all be zero
+                unsigned moving = 0;
+                for (int w = 0; w < L; ++w) moving |= ~(unsigned)c_lfix[q + w];
+                if ((moving & ~done_m & ((1u << G) - 1u)) == 0) { q += L; continue; }
+            }
             if constexpr (kRowStream) {
             if (L > 1) {
                 // ---- a batch of L short columns (planned: plan_runs); warp w takes column q + w
@@ -1228,7 +1239,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                               h += pp.y;
                           }
                           g -= c_xjy[qq][lane];                     // :1181-1183
-                          if (!s_done[lane]) {
+                          if (!s_done[lane] && !((c_lfix[qq] >> lane) & 1u)) {
                               if (h < 0.0) { g = 0.0; h = 0.0; }    // ccdUpdateBeta :1407-1410
                               const double b = c_beta[qq][lane];
                               double hd = c_hd[qq][lane];
@@ -1346,7 +1357,7 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
                   }
                   g -= c_xjy[q][threadIdx.x];                    // :1181-1183
                   double delta = 0.0;
-                  if (!s_done[threadIdx.x]) {
+                  if (!s_done[threadIdx.x] && !((c_lfix[q] >> threadIdx.x) & 1u)) {
                       if (h < 0.0) { g = 0.0; h = 0.0; }          // ccdUpdateBeta :1407-1410
                       const double b = c_beta[q][threadIdx.x];
                       double hd = c_hd[q][threadIdx.x];
@@ -1574,6 +1585,71 @@ __global__ void k_batch_final(int model, int K, int S, int G, int F, const doubl
     if (threadIdx.x == 0) {
         ll[f] = a + ((model == CYC_PR || model == CYC_CPR) ? llfixed[f] : 0.0);
         pll[f] = p;
+    }
+}
+
+// KKT scores of an active-set pass (computeKktConditions,
+// CyclicCoordinateDescent.cpp:817-837): |gradient| of column j for the fits
+// of group blockIdx.y that hold it inactive (bit f of `need`), at their
+// current linear predictors (independent-rows models, FP64 state); one CTA
+// per (column, group), entries strided over the threads, fixed-order sums.
+template <int G>
+__global__ void __launch_bounds__(kBT) k_batch_kkt(int model, int K, int J, const int* __restrict__ fmt,
+                                                   const long long* __restrict__ col_ptr,
+                                                   const long long* __restrict__ val_ptr, const int* __restrict__ idx,
+                                                   const double* __restrict__ val, const double* __restrict__ xb,
+                                                   const double* __restrict__ w, const signed char* __restrict__ fold,
+                                                   const int* __restrict__ fitfold, const double* __restrict__ xjy,
+                                                   const unsigned char* __restrict__ need, double* __restrict__ score) {
+    const int j = blockIdx.x, grp = blockIdx.y;
+    const unsigned nm = need[(size_t)grp * J + j];
+    if (nm == 0) return;
+    __shared__ unsigned char s_wm[128];
+    __shared__ double s_g[kBT / 32][G];
+    if (fold)
+        for (int v = threadIdx.x; v < 128; v += blockDim.x) {
+            unsigned m = 0;
+            for (int f = 0; f < G; ++f) {
+                const int ff = fitfold[grp * G + f];
+                if (ff >= -1 && ff != v) m |= 1u << f;
+            }
+            s_wm[v] = (unsigned char)m;
+        }
+    __syncthreads();
+    const int fm = fmt[j];
+    const bool dense = (fm == CYC_DENSE || fm == CYC_INTERCEPT);
+    const bool ind = (fm == CYC_INDICATOR || fm == CYC_INTERCEPT);
+    const long long n = dense ? (long long)K : col_ptr[j + 1] - col_ptr[j];
+    double g[G];
+    #pragma unroll
+    for (int f = 0; f < G; ++f) g[f] = 0.0;
+    for (long long e = threadIdx.x; e < n; e += blockDim.x) {
+        const int k = dense ? (int)e : idx[col_ptr[j] + e];
+        const double x = ind ? 1.0 : val[val_ptr[j] + e];
+        const size_t o = ((size_t)grp * K + k) * G;
+        const unsigned wm = fold ? (unsigned)s_wm[fold[k]] : 0u;
+        #pragma unroll
+        for (int f = 0; f < G; ++f) {
+            const double wt = fold ? (double)((wm >> f) & 1u) : w[o + f];
+            if (wt == 0.0) continue;
+            const double v = xb[o + f];
+            const double m = model == CYC_LR ? 1.0 / (1.0 + exp(-v)) : exp(v);
+            g[f] += wt * m * x;
+        }
+    }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    #pragma unroll
+    for (int f = 0; f < G; ++f) {
+        double v = g[f];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) s_g[wid][f] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < G && ((nm >> threadIdx.x) & 1u)) {
+        double t = 0.0;
+        for (int q = 0; q < kBT / 32; ++q) t += s_g[q][threadIdx.x];
+        const size_t o = (size_t)(grp * G + threadIdx.x) * J + j;
+        score[o] = fabs(t - xjy[o]);
     }
 }
 
@@ -1894,6 +1970,7 @@ struct BatchRunner {
     DevBuf<double> d_dex;
     DevBuf<double> d_denom, d_nw, d_xjy, d_beta, d_hdelta, d_var, d_llfixed, d_obj, d_stage, d_fixedc;
     DevBuf<unsigned long long> d_counters;
+    DevBuf<unsigned char> d_lfix;
 
     BatchRunner(Dataset& d, cudaStream_t s, int F_, int G_, int C_ = 0, BatchShape sh = BatchShape{})
         : ds(d), stream(s), F(F_), G(G_), shape(sh) {
@@ -2084,7 +2161,7 @@ struct BatchRunner {
         a.fmt = ds.d_fmt.get(); a.col_ptr = ds.d_col_ptr.get(); a.val_ptr = ds.d_val_ptr.get();
         a.idx = ds.d_idx.get(); a.val = ds.d_val.get(); a.split = d_split.get(); a.rpart = d_rpart.get();
         a.y = ds.d_y.get(); a.strat = ds.d_strat.get(); a.strat_ptr = ds.d_strat_ptr.get();
-        a.fixb = d_fixb.get(); a.ptype = d_ptype.get(); a.xb = d_xb.get(); a.w = d_w.get();
+        a.fixb = d_fixb.get(); a.lane_fix = d_lfix.get(); a.ptype = d_ptype.get(); a.xb = d_xb.get(); a.w = d_w.get();
         a.denom = d_denom.get(); a.nw = d_nw.get(); a.xjy = d_xjy.get(); a.beta = d_beta.get();
         a.hdelta = d_hdelta.get(); a.variance = d_var.get(); a.llfixed = d_llfixed.get(); a.active = d_active.get();
         a.fold = d_fold ? d_fold8.get() : nullptr;
@@ -2111,6 +2188,51 @@ struct BatchRunner {
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
         CYC_CHECK_LAUNCH();
+    }
+
+    // active-set passes: the fits (bit f of [group][J]) holding each column
+    // fixed, the fits that run the next launch, and fresh trust regions
+    // (findMode's resetBounds, CyclicCoordinateDescent.cpp:943)
+    void set_pass(const std::vector<unsigned char>& lane_fix, const std::vector<int>& running, double bound) {
+        const int J = ds.J;
+        d_lfix.alloc(lane_fix.size());
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_lfix.get(), lane_fix.data(), lane_fix.size(), cudaMemcpyHostToDevice, stream));
+        std::vector<int> act(Fp, 0);
+        std::copy(running.begin(), running.end(), act.begin());
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_active.get(), act.data(), Fp * sizeof(int), cudaMemcpyHostToDevice, stream));
+        std::vector<double> hd((size_t)Fp * J, bound);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_hdelta.get(), hd.data(), hd.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                       stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
+    }
+
+    // |gradient| of the columns `need` marks (bit f of [group][J]) for those
+    // fits, into score[F][J] (FP64 state of an independent-rows model)
+    void kkt_scores(const std::vector<unsigned char>& need, std::vector<double>& score) {
+        const int J = ds.J;
+        DevBuf<unsigned char> d_need;
+        DevBuf<double> d_score;
+        d_need.alloc(need.size());
+        d_score.alloc((size_t)Fp * J);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(d_need.get(), need.data(), need.size(), cudaMemcpyHostToDevice, stream));
+        CYC_CHECK_CUDA(cudaMemsetAsync(d_score.get(), 0, (size_t)Fp * J * sizeof(double), stream));
+        const dim3 grid(J, ngroups);
+        const double* w = d_fold ? nullptr : (const double*)d_w.get();
+        const signed char* fd = d_fold ? d_fold8.get() : nullptr;
+        const int* ff = d_fold ? d_fitfold.get() : nullptr;
+        if (G == 1)
+            launch(k_batch_kkt<1>, grid, kBT, 0, stream, ds.model, ds.K, J, ds.d_fmt.get(), ds.d_col_ptr.get(),
+                   ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(), (const double*)d_xb.get(), w, fd, ff,
+                   d_xjy.get(), d_need.get(), d_score.get());
+        else
+            launch(k_batch_kkt<8>, grid, kBT, 0, stream, ds.model, ds.K, J, ds.d_fmt.get(), ds.d_col_ptr.get(),
+                   ds.d_val_ptr.get(), ds.d_idx.get(), ds.d_val.get(), (const double*)d_xb.get(), w, fd, ff,
+                   d_xjy.get(), d_need.get(), d_score.get());
+        CYC_CHECK_LAUNCH();
+        score.resize((size_t)F * J);
+        CYC_CHECK_CUDA(cudaMemcpyAsync(score.data(), d_score.get(), score.size() * sizeof(double),
+                                       cudaMemcpyDeviceToHost, stream));
+        CYC_CHECK_CUDA(cudaStreamSynchronize(stream));
     }
 
     // log likelihood (and held-out predictive log likelihood for CV) per fit
@@ -2343,6 +2465,14 @@ void run_fits_concurrently(cyc_dataset* dsh, const cyc_prior* prior, const cyc_f
     set_last_stats(sum);
 }
 
+// Whether the batch kernel runs a solve's KKT-swindle passes itself: the
+// active sets are per-fit masks in the kernel and the inactive columns'
+// scores one launch (independent-rows models, FP64 state).  Other swindle
+// fits run as concurrent cyc_fit solves.
+bool batch_swindle(const Dataset& ds, const cyc_control* ctl) {
+    return model_independent(ds.model) && ctl->precision != CYC_MIXED;
+}
+
 // The shared driver of cyc_batch_fit and cyc_cv_grid_fit.  `d_fold` (fold id
 // per row, `n_folds` of them) and `fit_fold` (the held-out fold of each fit)
 // select the CV-grid weights; otherwise `specs[f].weights`.
@@ -2351,7 +2481,8 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
                std::vector<double>* pll, int fixed_col = -1) {
     CYC_REQUIRE(!model_cumulative(ds.model), CYC_ERR_UNSUPPORTED,
                 "batched fits support lr, pr, clr, cpr (use cyc_fit for cox)");
-    CYC_REQUIRE(!ctl->use_kkt_swindle, CYC_ERR_UNSUPPORTED, "the KKT swindle is offered by cyc_fit only");
+    CYC_REQUIRE(!ctl->use_kkt_swindle || batch_swindle(ds, ctl), CYC_ERR_UNSUPPORTED,
+                "batched KKT-swindle fits support lr and pr at FP64");
     CYC_REQUIRE(ctl->convergence_type == CYC_CONV_GRADIENT || ctl->convergence_type == CYC_CONV_MITTAL ||
                     ctl->convergence_type == CYC_CONV_LANGE,
                 CYC_ERR_UNSUPPORTED, "batched fits support gradient, mittal and lange convergence");
@@ -2392,6 +2523,11 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         if (ds.has_offset) beta[(size_t)f * J] = 1.0;
     }
     const int G = F >= 4 ? 8 : 1;
+    // the swindle runs when some column has a Laplace prior (a KKT boundary,
+    // JointPrior.h:149-157); otherwise it is findMode itself
+    std::vector<int> ptype(J, prior->prior_type);
+    for (int i = 0; i < prior->n_exclude; ++i) ptype[prior->exclude[i]] = CYC_PRIOR_NONE;
+    const bool swindle = ctl->use_kkt_swindle && std::count(ptype.begin(), ptype.end(), (int)CYC_PRIOR_LAPLACE) > 0;
     std::vector<int> iters, flags;
     std::vector<unsigned long long> ctr;
     cyc_run_stats st{};
@@ -2432,13 +2568,15 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
         st.launches += 1;
         st.phases = phase + 1;
     };
-    int C;
-    {
+    // the tuners time whole cycles over every column, which an active-set
+    // pass does not run: swindle solves keep the defaults
+    int C = default_cluster(ds.K);
+    if (!swindle) {
         NvtxRange range("cyclops batch: cluster tuner");
         C = tuned_cluster(ds, stream, F, G, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl, fixed_cols);
     }
     BatchShape shape;
-    {
+    if (!swindle) {
         NvtxRange range("cyclops batch: shape tuner");
         shape = tuned_shape(ds, stream, F, G, C, *prior, specs, beta, hd, d_fold, n_folds, fit_fold, *ctl,
                             fixed_cols);
@@ -2460,12 +2598,100 @@ void run_batch(Dataset& ds, const cyc_prior* prior, const cyc_fit_spec* specs, i
     NvtxRange range64("cyclops batch: fp64 phase");
     BatchRunner<double> r64(ds, stream, F, G, C, shape);
     if (d_fold) r64.set_folds(d_fold, n_folds, *fit_fold);
-    r64.setup(*prior, specs, beta, hd, fixed_cols);
     float ms = 0.f;
-    r64.run(*ctl, ctl->tolerance, &ms);
     std::vector<int> it64;
-    r64.results(beta, hd, it64, flags, ctr);
-    account(phase, ms, it64, (int)sizeof(double));
+    if (!swindle) {
+        r64.setup(*prior, specs, beta, hd, fixed_cols);
+        r64.run(*ctl, ctl->tolerance, &ms);
+        r64.results(beta, hd, it64, flags, ctr);
+        account(phase, ms, it64, (int)sizeof(double));
+    } else {
+        // kktSwindle (CyclicCoordinateDescent.cpp:636-814) for every fit at
+        // once.  The intercept and the columns whose prior has no KKT
+        // boundary start active, the Laplace columns inactive at beta 0.
+        // Each pass is one launch: a fit holds its inactive columns fixed
+        // (findMode over the active set, :617-634, with fresh trust regions),
+        // and a batch every running fit holds fixed is skipped.  Then one
+        // launch scores every running fit's inactive columns (|gradient|)
+        // and each fit moves the columns above its lambda into its active
+        // set.  A fit stops when nothing is inactive, its pass failed, no
+        // column violates, or after max_iterations passes (MAX_ITERATIONS);
+        // an empty active set skips the pass's findMode.  Reported cycles
+        // are the last pass's, as lastIterationCount.
+        const int intercept = ds.has_intercept ? (ds.has_offset ? 1 : 0) : -1;
+        std::vector<char> fixc(J, 0);
+        for (int j : fixed_cols) fixc[j] = 1;
+        if (ds.has_offset) fixc[0] = 1;
+        std::vector<unsigned char> lfix((size_t)r64.ngroups * J, 0);
+        std::vector<int> n_act(F, 0), n_inact(F, 0);
+        for (int f = 0; f < F; ++f)
+            for (int j = 0; j < J; ++j) {
+                if (fixc[j]) continue;
+                if (j == intercept || ptype[j] != CYC_PRIOR_LAPLACE) {
+                    ++n_act[f];
+                } else {
+                    ++n_inact[f];
+                    lfix[(size_t)(f / G) * J + j] |= (unsigned char)(1u << (f % G));
+                    beta[(size_t)f * J + j] = 0.0;          // setBeta(0) of a nonzero start
+                }
+            }
+        r64.setup(*prior, specs, beta, hd, fixed_cols);
+        std::vector<int> running(F, 1), run_k(F, 0), it_last(F, 0), total_it(F, 0), itp, flp;
+        flags.assign(F, CYC_SUCCESS);
+        std::vector<double> score;
+        for (int pass = 1;; ++pass) {
+            bool any = false;
+            for (int f = 0; f < F; ++f) {
+                run_k[f] = running[f] && n_act[f] > 0;
+                any |= run_k[f] != 0;
+                if (running[f]) flags[f] = CYC_SUCCESS;
+            }
+            if (any) {
+                r64.set_pass(lfix, run_k, ctl->initial_bound);
+                float pm = 0.f;
+                r64.run(*ctl, ctl->tolerance, &pm);
+                ms += pm;
+                r64.results(beta, hd, itp, flp, ctr);
+                for (int f = 0; f < F; ++f)
+                    if (run_k[f]) {
+                        it_last[f] = itp[f];
+                        total_it[f] += itp[f];
+                        flags[f] = flp[f];
+                    }
+            }
+            std::vector<unsigned char> need((size_t)r64.ngroups * J, 0);
+            bool any_need = false;
+            for (int f = 0; f < F; ++f) {
+                if (!running[f]) continue;
+                if (n_inact[f] == 0 || flags[f] != CYC_SUCCESS) { running[f] = 0; continue; }
+                if (pass == ctl->max_iterations) { flags[f] = CYC_MAX_ITERATIONS; running[f] = 0; continue; }
+                const unsigned char bit = (unsigned char)(1u << (f % G));
+                const size_t g0 = (size_t)(f / G) * J;
+                for (int j = 0; j < J; ++j)
+                    if (lfix[g0 + j] & bit) need[g0 + j] |= bit;
+                any_need = true;
+            }
+            if (!any_need) break;
+            r64.kkt_scores(need, score);
+            for (int f = 0; f < F; ++f) {
+                if (!running[f]) continue;
+                const double lambda = std::sqrt(2.0 / specs[f].variance);   // getKktBoundary, CovariatePrior.h:235-238
+                const unsigned char bit = (unsigned char)(1u << (f % G));
+                const size_t g0 = (size_t)(f / G) * J;
+                int moved = 0;
+                for (int j = 0; j < J; ++j)
+                    if ((need[g0 + j] & bit) && !(score[(size_t)f * J + j] <= lambda)) {
+                        lfix[g0 + j] &= (unsigned char)~bit;
+                        ++moved;
+                    }
+                if (moved == 0) running[f] = 0;
+                n_act[f] += moved;
+                n_inact[f] -= moved;
+            }
+        }
+        it64 = it_last;
+        account(phase, ms, total_it, (int)sizeof(double));
+    }
     std::vector<double> ll, p;
     r64.finalize(ll, p);
     std::vector<int> pt(J, prior->prior_type);
@@ -2496,10 +2722,10 @@ extern "C" int cyc_batch_fit(cyc_dataset* dsh, const cyc_prior* prior, const cyc
     return guarded([&] {
         NvtxRange range("cyc_batch_fit");
         CYC_REQUIRE(dsh && prior && specs && ctl && out && F > 0, CYC_ERR_ARGUMENT, "null argument");
-        if (ctl->use_kkt_swindle || model_cumulative(dsh->ds.model)) {
-            // every fit carries its own active set (swindle) or its own risk
-            // sets (cox), which one batch kernel cannot share: the fits run
-            // as concurrent cyc_fit calls
+        if (model_cumulative(dsh->ds.model) || (ctl->use_kkt_swindle && !batch_swindle(dsh->ds, ctl))) {
+            // cox fits carry their own risk sets, and swindle fits of grouped
+            // models or mixed precision their own active sets, which one
+            // batch kernel does not share: they run as concurrent cyc_fit calls
             run_fits_concurrently(dsh, prior, specs, F, ctl, out);
             return;
         }
@@ -2518,8 +2744,8 @@ extern "C" int cyc_cv_grid_fit(cyc_dataset* dsh, const cyc_prior* prior, const i
         Dataset& ds = dsh->ds;
         for (int k = 0; k < ds.K; ++k)
             CYC_REQUIRE(fold_of_row[k] >= 0 && fold_of_row[k] < n_folds, CYC_ERR_ARGUMENT, "fold id out of range");
-        if (ctl->use_kkt_swindle || model_cumulative(ds.model)) {
-            // per-fit active sets (swindle) or risk sets (cox): the per-fit path, unit weights
+        if (model_cumulative(ds.model) || (ctl->use_kkt_swindle && !batch_swindle(ds, ctl))) {
+            // per-fit risk sets (cox) or active sets the kernel does not run: the per-fit path, unit weights
             std::vector<double> ones(ds.K, 1.0);
             const int rc = cyc_cv_grid_fit_weighted(dsh, prior, fold_of_row, n_folds, ones.data(), variances, n_var,
                                                     ctl, out, pred_loglik, grid_mean);
@@ -2775,7 +3001,7 @@ extern "C" int cyc_cv_grid_fit_weighted(cyc_dataset* dsh, const cyc_prior* prior
             specs[i].weights = train.data() + (size_t)(i % n_folds) * K;
             specs[i].variance = variances[i / n_folds];
         }
-        if (ctl->use_kkt_swindle || model_cumulative(ds.model)) {   // per-fit active sets or risk sets
+        if (model_cumulative(ds.model) || (ctl->use_kkt_swindle && !batch_swindle(ds, ctl))) {
             run_fits_concurrently(dsh, prior, specs.data(), F, ctl, out);
         } else {
             run_batch(ds, prior, specs.data(), F, ctl, out, nullptr, 0, nullptr, nullptr);

@@ -76,7 +76,8 @@ def test_swindle_warm_start_and_pass_limit(cuda_lib):
 @pytest.mark.parametrize("name", ["swindle_lr_laplace_small", "swindle_clr_laplace"])
 def test_swindle_in_batched_fits(cuda_lib, name):
     """cyc_batch_fit with the swindle runs each fit's own active-set passes
-    (one by one): every fit equals the reference's swindle fit."""
+    (lr: in the batch kernel; clr: concurrent single-fit solves): every fit
+    equals the reference's swindle fit."""
     from cyclops_b200 import api
     data, s = load_golden(name)
     prior = api.PriorSpec(int(s["prior"]), float(s["variance"]), exclude_for(data))
@@ -84,6 +85,88 @@ def test_swindle_in_batched_fits(cuda_lib, name):
                              use_kkt_swindle=True)
     for fit in api.batch_fit(data, prior, [float(s["variance"])] * 2, control=ctl):
         assert_contract(fit, golden_fit(s), what=name, beta_atol=_atol(name))
+
+
+def _swindle_ref(data, s, variance, weights, tol=None, conv=None, max_iterations=1000, start=None):
+    from oracle import oracle as O
+    ctl = O.make_control(tolerance=float(s["tolerance"]) if tol is None else tol,
+                         convergence_type=int(s["convergence"]) if conv is None else conv,
+                         max_iterations=max_iterations, use_kkt_swindle=1)
+    return O.port().fit(data, int(s["prior"]), variance, control=ctl, weights=weights, start=start)
+
+
+@pytest.mark.parametrize("name", ["swindle_lr_laplace_small", "swindle_lr_c1", "swindle_pr_laplace_weighted",
+                                  "swindle_lr_empty_column"])
+@pytest.mark.parametrize("nfits", [1, 6, 11])
+def test_swindle_batch_kernel_matches_reference(cuda_lib, name, nfits):
+    """The batch kernel's own active-set passes: per-fit masks hold each
+    fit's inactive columns fixed (a batch every running fit holds fixed is
+    skipped), one launch scores all inactive columns, and each fit's sets
+    grow as the reference's do.  Every fit -- its own weights and variance
+    -- is the oracle's swindle fit under the precision contract, at 1 fit
+    (the one-fit groups), 6 and 11 (8-fit groups, padding lanes)."""
+    from cyclops_b200 import api
+    data, s = load_golden(name)
+    rng = np.random.default_rng(7 + nfits)
+    var0 = float(s["variance"])
+    base = np.ones(data.K) if s["weights"] is None else np.asarray(s["weights"], float)
+    variances = [var0 * (0.25, 1.0, 4.0)[f % 3] for f in range(nfits)]
+    weights = [s["weights"] if f == 0 else base * (rng.random(data.K) > 0.2) for f in range(nfits)]
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    ctl = api.create_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                             use_kkt_swindle=True)
+    fits = api.batch_fit(data, prior, variances, weights, ctl)
+    for f in range(nfits):
+        ref = _swindle_ref(data, s, variances[f], weights[f])
+        assert_contract(fits[f], ref, what=(name, f), beta_atol=_atol(name))
+
+
+def test_swindle_batch_kernel_tight_and_warm(cuda_lib):
+    """Converged tightly (Mittal 1e-12), with warm starts that are nonzero
+    on inactive columns (zeroed first), and with the pass limit
+    (max_iterations 2: MAX_ITERATIONS for fits that still had violators)."""
+    from cyclops_b200 import api
+    data, s = load_golden("swindle_lr_laplace_small")
+    var0 = float(s["variance"])
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    start = np.where(np.arange(data.J) % 3 == 0, 0.05, 0.0)
+    variances = [var0 * m for m in (0.1, 0.5, 1.0, 2.0, 8.0)]
+    for max_it, tol, conv in ((5000, 1e-12, D.CONV_MITTAL), (2, 1e-8, D.CONV_GRADIENT)):
+        ctl = api.create_control(tolerance=tol, convergence_type=conv, max_iterations=max_it, use_kkt_swindle=True)
+        fits = api.batch_fit(data, prior, variances, None, ctl, starts=[start] * len(variances))
+        for v, fit in zip(variances, fits):
+            ref = _swindle_ref(data, s, v, None, tol=tol, conv=conv, max_iterations=max_it, start=start)
+            assert_contract(fit, ref, what=(max_it, v))
+
+
+def test_swindle_batch_kernel_equals_single_fit_swindle(cuda_lib):
+    """A fit of the batch kernel's swindle equals cyc_fit's swindle of the
+    same fit: same flag, cycles, zero pattern, and beta to 1e-9."""
+    from cyclops_b200 import api
+    data, s = load_golden("swindle_lr_c1")
+    var0 = float(s["variance"])
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    ctl = api.create_control(tolerance=1e-8, use_kkt_swindle=True)
+    variances = [var0 * m for m in (0.5, 1.0, 2.0, 4.0, 8.0, 16.0, 32.0, 64.0, 128.0)]
+    fits = api.batch_fit(data, prior, variances, None, ctl)
+    for v, fit in zip(variances, fits):
+        one = api.fit_cyclops_model(data, api.PriorSpec(int(s["prior"]), v, exclude_for(data)), ctl)
+        assert fit.return_flag == one.return_flag and fit.iterations == one.iterations
+        assert np.array_equal(fit.beta == 0.0, one.beta == 0.0)
+        assert np.max(np.abs(fit.beta - one.beta) / np.maximum(np.abs(one.beta), 1e-3)) < 1e-9, v
+
+
+def test_swindle_mixed_precision_batch_runs_per_fit(cuda_lib):
+    """Mixed precision with the swindle is not a batch-kernel path: its fits
+    run as concurrent single-fit solves, each the oracle's swindle fit."""
+    from cyclops_b200 import api
+    data, s = load_golden("swindle_lr_laplace_small")
+    var0 = float(s["variance"])
+    prior = api.PriorSpec(int(s["prior"]), var0, exclude_for(data))
+    ctl = api.create_control(tolerance=float(s["tolerance"]), convergence_type=int(s["convergence"]),
+                             use_kkt_swindle=True, precision="mixed")
+    for v, fit in zip([var0, 2 * var0], api.batch_fit(data, prior, [var0, 2 * var0], None, ctl)):
+        assert_contract(fit, _swindle_ref(data, s, v, None), what=v)
 
 
 def test_swindle_in_cv_grid_and_auto_search(cuda_lib):
