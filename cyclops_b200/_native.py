@@ -117,11 +117,16 @@ _SIGS = {
     "cyc_cv_auto_search": [C.c_void_p, C.POINTER(Prior), C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_double,
                            C.POINTER(Control), C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
                            C.c_void_p, C.c_int, C.POINTER(C.c_int)],
+    "cyc_ingest_covariates": [C.c_int, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                              C.POINTER(C.c_void_p)],
+    "cyc_ingest_sizes": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)],
+    "cyc_ingest_copy": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
+    "cyc_ingest_free": [C.c_void_p],
     "cyc_profile_bounds": [C.c_void_p, C.POINTER(Prior), C.POINTER(FitSpec), C.POINTER(Control), C.c_void_p,
                            C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                            C.POINTER(FitResult)],
 }
-_RESTYPE = {"cyc_last_error": C.c_char_p, "cyc_launch_count": C.c_longlong}
+_RESTYPE = {"cyc_last_error": C.c_char_p, "cyc_launch_count": C.c_longlong, "cyc_ingest_free": None}
 
 _lock = threading.Lock()
 _lib = None

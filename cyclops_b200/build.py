@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libcyclops_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["dataset.cu", "engine.cu", "fit.cu", "batch.cu", "cv.cu", "noalloc.cu"]
+SOURCES = ["dataset.cu", "engine.cu", "fit.cu", "batch.cu", "cv.cu", "noalloc.cu", "ingest.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -22,7 +22,9 @@ Two halves, as in the reference:
   logTransformCovariate(0), :609-651, via .cyclopsFinalizeData,
   src/RcppModelData.cpp:463-545).
 
-Host-side numpy; the result uploads with `api.Dataset` like any CyclopsData.
+Host-side numpy, or (`device=`) the covariate half on the GPU
+(cyc_ingest_covariates); the result uploads with `api.Dataset` like any
+CyclopsData.
 """
 from __future__ import annotations
 
@@ -114,41 +116,11 @@ def sort_covariates(model: int, covariates: Mapping, outcomes_sorted: Mapping) -
             "position": pos[o]}
 
 
-def load(model: int, outs: dict, covs: dict, add_intercept: bool) -> D.CyclopsData:
-    """ModelData::loadY + loadX(intercept) + loadMultipleX + the Poisson
-    offset, on tables already in the reference's order."""
-    K = outs["rowId"].size
-    # loadY: strata renumbered by runs (:100-122)
-    pid = None
-    if outs["stratumId"] is not None:
-        s = outs["stratumId"]
-        pid = np.concatenate([[0], np.cumsum(s[1:] != s[:-1])]).astype(np.int32) if K else np.zeros(0, np.int32)
+def _covariate_columns(covs: dict):
+    """loadMultipleX on covariates in the reference's order: (formats,
+    row-id offsets, row positions, value offsets, values, covariateIds) of
+    the covariate columns, offsets from 0."""
     fmts, ptr, vptr, idx_parts, val_parts, labels = [], [0], [0], [], [], []
-
-    def add(fmt, rows, vals, label):
-        fmts.append(fmt)
-        labels.append(label)
-        if rows is not None:
-            idx_parts.append(rows.astype(np.int32))
-            ptr.append(ptr[-1] + rows.size)
-        else:
-            ptr.append(ptr[-1])
-        if vals is not None:
-            val_parts.append(vals.astype(np.float64))
-            vptr.append(vptr[-1] + vals.size)
-        else:
-            vptr.append(vptr[-1])
-
-    offset = model in (D.PR, D.CPR)
-    if offset:
-        t = outs["time"]
-        if t is None:
-            raise IngestError("Poisson models need outcomes$time")
-        # setOffsetCovariate(-1) + logTransformCovariate(0): the C library log, as std::log
-        add(D.DENSE, None, np.fromiter(map(math.log, t.tolist()), np.float64, t.size), -1)
-    has_intercept = add_intercept and model in (D.LR, D.PR)
-    if has_intercept:
-        add(D.INTERCEPT, None, None, 0)                # loadX(0, none, none): INTERCEPT, to the front
     cid, pos, val = covs["covariateId"], covs["position"], covs["covariateValue"]
     if cid.size:
         starts = np.flatnonzero(np.concatenate([[True], cid[1:] != cid[:-1]]))
@@ -159,32 +131,124 @@ def load(model: int, outs: dict, covs: dict, add_intercept: bool) -> D.CyclopsDa
         if rep.any():
             i = int(np.flatnonzero(rep)[0]) + 1
             raise IngestError(f"Repeated row-column entry at {rows_all[i]} - {cid[i]}")
-        if val is None:
-            for a, b in zip(starts, ends):
-                add(D.INDICATOR, pos[a:b], None, int(cid[a]))
-        else:
-            nz = val != 0.0
-            not01 = ~((val == 0.0) | (val == 1.0))
-            for a, b in zip(starts, ends):
+        nz = None if val is None else val != 0.0
+        not01 = None if val is None else ~((val == 0.0) | (val == 1.0))
+        for a, b in zip(starts, ends):
+            labels.append(int(cid[a]))
+            if val is None:
+                fmts.append(D.INDICATOR)
+                rows, vals = pos[a:b], None
+            else:
                 keep = nz[a:b]
                 sparse = bool(not01[a:b].any())      # first value, or an upcast (:176-184)
-                rows = pos[a:b][keep]
-                add(D.SPARSE if sparse else D.INDICATOR, rows, val[a:b][keep] if sparse else None, int(cid[a]))
+                fmts.append(D.SPARSE if sparse else D.INDICATOR)
+                rows, vals = pos[a:b][keep], (val[a:b][keep] if sparse else None)
+            idx_parts.append(rows.astype(np.int32))
+            ptr.append(ptr[-1] + rows.size)
+            if vals is not None:
+                val_parts.append(vals.astype(np.float64))
+            vptr.append(vptr[-1] + (0 if vals is None else vals.size))
     col_idx = np.concatenate(idx_parts) if idx_parts else np.zeros(0, np.int32)
     col_val = np.concatenate(val_parts) if val_parts else np.zeros(0)
-    cd = D.CyclopsData(model=model, y=np.ascontiguousarray(outs["y"]), col_format=np.asarray(fmts, np.int32),
-                       col_ptr=np.asarray(ptr, np.int64), col_idx=np.ascontiguousarray(col_idx, np.int32),
-                       val_ptr=np.asarray(vptr, np.int64), col_val=np.ascontiguousarray(col_val),
+    return (np.asarray(fmts, np.int32), np.asarray(ptr, np.int64), col_idx, np.asarray(vptr, np.int64), col_val,
+            np.asarray(labels, np.int64))
+
+
+def _assemble(model: int, outs: dict, cols, add_intercept: bool) -> D.CyclopsData:
+    """ModelData::loadY + loadX(intercept) + the Poisson offset in front of
+    the covariate columns `cols` (as _covariate_columns returns them)."""
+    K = outs["rowId"].size
+    # loadY: strata renumbered by runs (:100-122)
+    pid = None
+    if outs["stratumId"] is not None:
+        s = outs["stratumId"]
+        pid = np.concatenate([[0], np.cumsum(s[1:] != s[:-1])]).astype(np.int32) if K else np.zeros(0, np.int32)
+    fmt, ptr, idx, vptr, val, lab = cols
+    offset = model in (D.PR, D.CPR)
+    has_intercept = add_intercept and model in (D.LR, D.PR)
+    pre_fmt, pre_lab, pre_vptr, pre_val = [], [], [0], []
+    if offset:
+        t = outs["time"]
+        if t is None:
+            raise IngestError("Poisson models need outcomes$time")
+        # setOffsetCovariate(-1) + logTransformCovariate(0): the C library log, as std::log
+        pre_fmt.append(D.DENSE)
+        pre_lab.append(-1)
+        pre_val.append(np.fromiter(map(math.log, t.tolist()), np.float64, t.size))
+        pre_vptr.append(K)
+    if has_intercept:
+        pre_fmt.append(D.INTERCEPT)                    # loadX(0, none, none): INTERCEPT, to the front
+        pre_lab.append(0)
+        pre_vptr.append(pre_vptr[-1])
+    n_pre = len(pre_fmt)
+    col_ptr = np.concatenate([np.zeros(n_pre, np.int64), ptr])
+    val_ptr = np.concatenate([np.asarray(pre_vptr, np.int64), vptr[1:] + pre_vptr[-1]])
+    col_val = np.concatenate(pre_val + [val]) if pre_val else val
+    cd = D.CyclopsData(model=model, y=np.ascontiguousarray(outs["y"]),
+                       col_format=np.concatenate([np.asarray(pre_fmt, np.int32), fmt]).astype(np.int32),
+                       col_ptr=col_ptr, col_idx=np.ascontiguousarray(idx, np.int32),
+                       val_ptr=val_ptr, col_val=np.ascontiguousarray(col_val, np.float64),
                        pid=pid, time=outs["time"], has_offset=offset, has_intercept=has_intercept)
-    cd.labels = np.asarray(labels, np.int64)
+    cd.labels = np.concatenate([np.asarray(pre_lab, np.int64), lab])
     return cd
 
 
+def load(model: int, outs: dict, covs: dict, add_intercept: bool) -> D.CyclopsData:
+    """ModelData::loadY + loadX(intercept) + loadMultipleX + the Poisson
+    offset, on tables already in the reference's order."""
+    return _assemble(model, outs, _covariate_columns(covs), add_intercept)
+
+
+def device_covariate_columns(covariates: Mapping, outs: dict, device: int = 0):
+    """The covariate columns built on the GPU (cyc_ingest_covariates): the
+    same arrays _covariate_columns makes from the host-sorted table, for the
+    unsorted covariate table and the sorted outcomes."""
+    import ctypes as C
+    from . import _native as N
+    cid = _col(covariates, "covariateId", np.int64)
+    row = _col(covariates, "rowId", np.int64)
+    if cid is None or row is None:
+        raise IngestError("covariates need covariateId and rowId")
+    val = _col(covariates, "covariateValue", np.float64)
+    cid, row = np.ascontiguousarray(cid), np.ascontiguousarray(row)
+    val = None if val is None else np.ascontiguousarray(val)
+    orow = np.ascontiguousarray(outs["rowId"], np.int64)
+    L = N.lib()
+    h = C.c_void_p()
+    rc = L.cyc_ingest_covariates(int(device), int(cid.size), cid.ctypes.data, row.ctypes.data,
+                                 None if val is None else val.ctypes.data, int(orow.size), orow.ctypes.data,
+                                 C.byref(h))
+    if rc != 0:
+        msg = L.cyc_last_error().decode()
+        if "Repeated" in msg:
+            raise IngestError(msg)
+        N.check(rc)
+    try:
+        J, n_idx, n_val = C.c_int(), C.c_longlong(), C.c_longlong()
+        N.check(L.cyc_ingest_sizes(h, C.byref(J), C.byref(n_idx), C.byref(n_val)))
+        fmt = np.zeros(J.value, np.int32)
+        ptr = np.zeros(J.value + 1, np.int64)
+        vptr = np.zeros(J.value + 1, np.int64)
+        lab = np.zeros(J.value, np.int64)
+        idx = np.zeros(n_idx.value, np.int32)
+        vals = np.zeros(n_val.value, np.float64)
+        N.check(L.cyc_ingest_copy(h, fmt.ctypes.data, ptr.ctypes.data, idx.ctypes.data, vptr.ctypes.data,
+                                  vals.ctypes.data, lab.ctypes.data))
+    finally:
+        L.cyc_ingest_free(h)
+    return fmt, ptr, idx, vptr, vals, lab
+
+
 def convert_to_cyclops_data(outcomes: Mapping, covariates: Mapping, model_type: str = "lr",
-                            add_intercept: bool = True) -> Tuple[D.CyclopsData, Optional[np.ndarray]]:
+                            add_intercept: bool = True,
+                            device: Optional[int] = None) -> Tuple[D.CyclopsData, Optional[np.ndarray]]:
     """convertToCyclopsData (R/NewDataConversion.R:94-210) for tables given as
     mappings of column name -> array.  Returns the data and the outcome
-    weights (None without an outcomes$weights column), in row order."""
+    weights (None without an outcomes$weights column), in row order.  With
+    `device`, the covariate table is sorted and loaded on that GPU
+    (cyc_ingest_covariates; the outcome table, K rows, is sorted here); a
+    clr / cpr covariate table that carries its own stratumId column is
+    ordered by it, as the reference does, on the host."""
     if model_type not in _MODELS:
         raise IngestError(f"unknown model type {model_type!r}")
     model = _MODELS[model_type]
@@ -195,5 +259,9 @@ def convert_to_cyclops_data(outcomes: Mapping, covariates: Mapping, model_type: 
         if t is None or np.any(t <= 0):
             raise IngestError("time cannot be non-positive")
     outs = sort_outcomes(model, outcomes)
-    covs = sort_covariates(model, covariates, outs)
-    return load(model, outs, covs, add_intercept), outs["weights"]
+    own_strata = model in (D.CLR, D.CPR) and _col(covariates, "stratumId") is not None
+    if device is not None and not own_strata:
+        cols = device_covariate_columns(covariates, outs, device)
+    else:
+        cols = _covariate_columns(sort_covariates(model, covariates, outs))
+    return _assemble(model, outs, cols, add_intercept), outs["weights"]

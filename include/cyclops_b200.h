@@ -335,6 +335,33 @@ int cyc_cv_fold_weights(int K, const int* ids, int folds, long seed, int by_row,
 int cyc_bootstrap_weights(int K, const int* ids, int n_replicates, long seed, const double* unit_exclude,
                           double* out);
 
+/* Device ingest of a long covariate table (rowId, covariateId,
+ * covariateValue): the covariate half of convertToCyclopsData
+ * (R/NewDataConversion.R:131-176) and ModelData::loadMultipleX
+ * (src/cyclops/ModelData.cpp:148-243) on the GPU.  `outcome_row_id` holds
+ * the K outcome rowIds already in the reference's row order (the outcome
+ * sort is the caller's: by rowId; stratum, rowId; or stratum, time
+ * descending, y, rowId); a covariate row takes the position of the last
+ * outcome row with its rowId and is dropped when there is none.  Entries
+ * are ordered by (covariateId, position) -- for every model the reference's
+ * covariate order when a covariate's stratum is its outcome's -- and each
+ * covariateId run becomes a column: INDICATOR unless a value is neither 0
+ * nor 1 (then SPARSE), zero values not stored, all entries stored when
+ * `value` is NULL; a repeated (row, covariate) fails with
+ * "Repeated row-column entry at <rowId> - <covariateId>".  The result stays
+ * on the device until copied: cyc_ingest_sizes gives the column count and
+ * the row-id and value counts, cyc_ingest_copy fills caller buffers (formats
+ * J, col_ptr J+1 and val_ptr J+1 offsets, row positions, values, the
+ * columns' covariateIds), cyc_ingest_free releases it.  Offset and intercept
+ * columns are the caller's to prepend. */
+typedef struct cyc_ingest cyc_ingest;
+int cyc_ingest_covariates(int device, long long n, const long long* covariate_id, const long long* row_id,
+                          const double* value, int K, const long long* outcome_row_id, cyc_ingest** out);
+int cyc_ingest_sizes(const cyc_ingest* h, int* n_columns, long long* n_idx, long long* n_val);
+int cyc_ingest_copy(const cyc_ingest* h, int* col_format, long long* col_ptr, int* col_idx, long long* val_ptr,
+                    double* col_val, long long* labels);
+void cyc_ingest_free(cyc_ingest* h);
+
 /* Statistics of the last cyc_batch_fit / cyc_fit on this thread, for
  * roofline accounting: kernel milliseconds (CUDA events), column entries
  * visited by gradients, entries visited by updates, coordinate steps. */
