@@ -458,6 +458,43 @@ def _first_columns(data, n):
                        col_val=data.col_val[:int(data.val_ptr[n])], pid=data.pid, time=data.time)
 
 
+def leg_ingest(rows=250_000, covariates=100_000, per_row=50, seed=3):
+    """Ingest of a config-2-shaped long table (Poisson outcomes with times;
+    `per_row` Zipf(1.1) indicator covariates per row out of `covariates`,
+    repeats dropped; rows and entries shuffled), bounded to `rows` rows:
+    the host loader (NumPy sorts + a column loop) against the device loader
+    (cyc_ingest_covariates), both from the same unsorted tables to the same
+    column store, the device's result checked equal to the host's."""
+    from cyclops_b200 import ingest
+    rng = np.random.default_rng(seed)
+    t0 = time.perf_counter()
+    r = np.repeat(np.arange(rows, dtype=np.int64), per_row)
+    key = np.unique(r * covariates + (rng.zipf(1.1, r.size) % covariates))
+    perm = rng.permutation(key.size)
+    cov = {"rowId": (key // covariates)[perm], "covariateId": (key % covariates)[perm]}
+    out = {"rowId": rng.permutation(rows).astype(np.int64), "y": rng.poisson(1.0, rows).astype(np.float64),
+           "time": rng.exponential(1.0, rows) + 1e-3}
+    gen = time.perf_counter() - t0
+    ingest.convert_to_cyclops_data({k: v[:1000] for k, v in out.items()},
+                                   {k: v[:10_000] for k, v in cov.items()}, "pr", device=0)   # context, module load
+    dev_s = []
+    for _ in range(2):
+        t = time.perf_counter()
+        dd, _ = ingest.convert_to_cyclops_data(out, cov, "pr", device=0)
+        dev_s.append(time.perf_counter() - t)
+    t = time.perf_counter()
+    dh, _ = ingest.convert_to_cyclops_data(out, cov, "pr")
+    host_s = time.perf_counter() - t
+    equal = all(np.array_equal(getattr(dd, k), getattr(dh, k))
+                for k in ("col_format", "col_ptr", "col_idx", "val_ptr", "col_val", "labels", "y"))
+    return {"workload": f"long table: {rows:,} rows x {per_row} Zipf(1.1) indicators of {covariates:,} covariates "
+                        f"(repeats dropped), poisson with times, seed {seed}",
+            "entries": int(key.size), "columns": int(dd.J), "generation_s": gen,
+            "host_s": host_s, "device_s": min(dev_s), "device_first_s": dev_s[0],
+            "speedup": host_s / min(dev_s), "equal": bool(equal),
+            "device_entries_per_s": key.size / min(dev_s)}
+
+
 def leg_serving():
     """The request stream (2,000 requests at 50/s in full), bounded: its first
     120 requests (about 2.4 s of arrivals), admitted for at most 60 s, stored
@@ -622,7 +659,7 @@ def run_ours(args):
         line["check"] = {"fits_compared": len(ids), "max_rel_err_beta_vs_cpu": err}
     if rank == 0 and world == 1 and args.extras != "none":
         legs = args.extras.split(",") if args.extras != "all" else \
-            ["mixed", "poisson", "cox", "cox_strata", "serving"]
+            ["mixed", "poisson", "cox", "cox_strata", "serving", "ingest"]
         extra = {}
         t_extra = time.perf_counter()
         for leg in legs:
@@ -638,6 +675,8 @@ def run_ours(args):
                     extra[leg] = leg_cox(api, n_strata=10_000, whole_fit=False)
                 elif leg == "serving":
                     extra[leg] = leg_serving()
+                elif leg == "ingest":
+                    extra[leg] = leg_ingest()
                 else:
                     extra[leg] = {"error": "unknown leg"}
             except Exception as e:     # a failed leg is reported; the line still prints
@@ -668,8 +707,8 @@ def main(argv=None):
                     help="cap on CCD cycles per fit (the reference default is 1000)")
     ap.add_argument("--extras", default="all",
                     help="further measurements at N=1: all, none, or a comma list of "
-                         "mixed,poisson,cox,cox_strata,serving")
-    ap.add_argument("--workload", default="cv", choices=["cv", "poisson", "cox", "cox_strata", "serving"],
+                         "mixed,poisson,cox,cox_strata,serving,ingest")
+    ap.add_argument("--workload", default="cv", choices=["cv", "poisson", "cox", "cox_strata", "serving", "ingest"],
                     help="cv: the headline CV grid (default); the others run that measurement alone and print "
                          "its record (profiling runs)")
     ap.add_argument("--cox-columns", type=int, default=0,
@@ -691,6 +730,8 @@ def run_workload(args):
     elif args.workload in ("cox", "cox_strata"):
         out = leg_cox(api, n_strata=10_000 if args.workload == "cox_strata" else 0,
                       whole_fit=args.workload == "cox", columns=args.cox_columns)
+    elif args.workload == "ingest":
+        out = leg_ingest()
     else:
         out = leg_serving()
     print(json.dumps({"workload": args.workload, **out}))
