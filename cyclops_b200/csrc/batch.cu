@@ -929,7 +929,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
             for (int qq = 0; qq < jn; ++qq) {
                 const int n = c_e1[qq] - c_e0[qq];
                 const bool dn = (c_fmt[qq] == CYC_DENSE || c_fmt[qq] == CYC_INTERCEPT);
-                if (!grouped && !c_fix[qq] && !dn && n > 0 && n <= kRegItems * NS && off + n <= kStage) {
+                // a column every running fit holds fixed (an active-set
+                // pass) is not staged: it is skipped, or read in place
+                const bool held = A.lane_fix && ((~(unsigned)c_lfix[qq] & ~done_m & ((1u << G) - 1u)) == 0);
+                if (!grouped && !c_fix[qq] && !held && !dn && n > 0 && n <= kRegItems * NS && off + n <= kStage) {
                     c_off[qq] = off;
                     c_sq[ns] = qq;
                     c_soff[ns] = off;
