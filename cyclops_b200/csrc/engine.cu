@@ -368,13 +368,10 @@ void Engine::cox_rescan_gated(const double* gate, int lo) {
     // tiles start at lo rounded down to a multiple of kScanItems (aligned loads)
     const int ntiles = (hi - scan_base(lo) + kScanTile - 1) / kScanTile;
     launch(k_scanD_tiles, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), aggD.get());
-    launch(k_carryD, 1, kThreads, 0, stream, gate, ntiles, aggD.get(), lo, gstart.get(), D.get());
     launch(k_scanD_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), denom.get(), nw.get(),
-                                                   aggD.get(), D.get(), R1.get(), R2.get(), aggP.get());
-    launch(k_carryP, 1, kThreads, 0, stream, gate, ntiles, aggP.get(), lo, gstart.get(), P1h.get(), P1l.get(),
-                                         P2h.get(), P2l.get());
+                                                   (const SegD*)aggD.get(), D.get(), R1.get(), R2.get(), aggP.get());
     launch(k_scanP_write, ntiles, kThreads, 0, stream, gate, lo, hi, gstart.get(), (const double*)R1.get(),
-                                                   (const double*)R2.get(), aggP.get(),
+                                                   (const double*)R2.get(), (const SegP*)aggP.get(),
                                                    P1h.get(), P1l.get(), P2h.get(), P2l.get());
     CYC_CHECK_LAUNCH();
 }

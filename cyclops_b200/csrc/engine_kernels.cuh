@@ -555,8 +555,12 @@ __global__ void k_update_grouped(ColView c, const double* delta_ptr, double delt
 // D_i  = stratum-segmented inclusive prefix of denom
 // P1_i = stratum-segmented inclusive prefix of n_i / D_i      (double-double)
 // P2_i = stratum-segmented inclusive prefix of n_i / D_i^2    (double-double)
-// computed over [lo, N) in tiles of kScanTile groups with three phases
-// (tile aggregates, carry scan, rewrite) for D and again for P.
+// computed over [lo, N) in tiles of kScanTile groups: a pass of tile
+// aggregates for D, then a rewrite pass for D (which also forms the P terms
+// and their tile aggregates) and one for P.  A rewrite CTA folds the
+// aggregates of the tiles before its own into its carry itself (a few
+// thousand L2-resident values), so no carry-scan launch sits between the
+// passes.
 
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kThreads * kScanItems;
@@ -728,53 +732,53 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanD_tiles(const double* gate,
     if (threadIdx.x == 0) agg[blockIdx.x] = tot;
 }
 
+// the carry into tile `b`: `init` combined with the aggregates of tiles
+// [0, b) in order (each thread folds a contiguous run, then the runs are
+// combined across the block); every thread gets it
 template <class T>
-__device__ void scan_carry(int n, T* agg, T init) {
-    // one block: each thread folds a contiguous run of tiles, then a block scan
-    const int per = (n + blockDim.x - 1) / blockDim.x;
-    const int b = threadIdx.x * per, e = min(n, b + per);
-    T acc{};
-    acc.f = 0;
-    T id = acc;
-    for (int i = b; i < e; ++i) acc = seg_combine(acc, agg[i]);
-    __shared__ T s_w[kThreads / 32];
-    (void)id;
-    T excl = block_seg_excl(acc, s_w, (T*)nullptr);     // warp shuffles, then the warps' totals
-    T run = seg_combine(init, excl);
-    for (int i = b; i < e; ++i) {
-        const T t = agg[i];
-        agg[i] = run;  // exclusive carry into tile i
-        run = seg_combine(run, t);
+__device__ __forceinline__ T tile_carry(const T* __restrict__ agg, int b, T init, T* s_w) {
+    const int per = (b + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int s0 = threadIdx.x * per, s1 = min(b, s0 + per);
+    T acc{};                                       // the identity: no segment start, zero sums
+    // several loads in flight at a time (eight D aggregates, four P ones: a
+    // run is at most eight tiles up to 2M groups)
+    constexpr int U = sizeof(T) > 16 ? 4 : 8;
+    for (int i = s0; i < s1; i += U) {
+        T v[U];
+        #pragma unroll
+        for (int k = 0; k < U; ++k) v[k] = (i + k < s1) ? agg[i + k] : T{};
+        #pragma unroll
+        for (int k = 0; k < U; ++k) acc = seg_combine(acc, v[k]);
     }
+    T tot;
+    block_seg_excl(acc, s_w, &tot);
+    return seg_combine(init, tot);
 }
 
-__global__ void k_carryD(const double* gate, int n, SegD* agg, int lo, const int* __restrict__ gstart,
-                         const double* __restrict__ D) {
-    if (gate && *gate == 0.0) return;
-    const SegD init{0, (lo > 0 && gstart[lo] != lo) ? D[lo - 1] : 0.0};
-    scan_carry(n, agg, init);
+// the carry's starting value: the prefix at lo - 1 when lo continues its stratum
+__device__ __forceinline__ SegD carry_init_D(int lo, const int* __restrict__ gstart, const double* __restrict__ D) {
+    return SegD{0, (lo > 0 && gstart[lo] != lo) ? D[lo - 1] : 0.0};
 }
-
-__global__ void k_carryP(const double* gate, int n, SegP* agg, int lo, const int* __restrict__ gstart,
-                         const double* __restrict__ P1h, const double* __restrict__ P1l,
-                         const double* __restrict__ P2h, const double* __restrict__ P2l) {
-    if (gate && *gate == 0.0) return;
+__device__ __forceinline__ SegP carry_init_P(int lo, const int* __restrict__ gstart, const double* __restrict__ P1h,
+                                             const double* __restrict__ P1l, const double* __restrict__ P2h,
+                                             const double* __restrict__ P2l) {
     SegP init{0, {0.0, 0.0}, {0.0, 0.0}};
     if (lo > 0 && gstart[lo] != lo) {
         init.a = DD{P1h[lo - 1], P1l[lo - 1]};
         init.b = DD{P2h[lo - 1], P2l[lo - 1]};
     }
-    scan_carry(n, agg, init);
+    return init;
 }
 
 // writes D and the P terms r1 = n/D, r2 = n/D^2 (R1, R2) for the P pass
 __global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, const double* __restrict__ nw,
-                              const SegD* __restrict__ carry, double* __restrict__ D, double* __restrict__ R1,
+                              const SegD* __restrict__ aggD, double* __restrict__ D, double* __restrict__ R1,
                               double* __restrict__ R2, SegP* __restrict__ aggP) {
     if (gate && *gate == 0.0) return;
     __shared__ SegD s_w[kThreads / 32];
     __shared__ SegP s_wp[kThreads / 32];
+    const SegD carry = tile_carry(aggD, (int)blockIdx.x, carry_init_D(lo, gstart, D), s_w);
     const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int f[kScanItems];
     double v[kScanItems], n[kScanItems];
@@ -783,7 +787,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate,
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) a = seg_combine(a, SegD{f[q], v[q]});
     const SegD ex = block_seg_excl(a, s_w, nullptr);
-    SegD run = seg_combine(carry[blockIdx.x], ex);
+    SegD run = seg_combine(carry, ex);
     SegP p{0, {0.0, 0.0}, {0.0, 0.0}};
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
@@ -805,10 +809,11 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate,
 
 __global__ void __launch_bounds__(kThreads, 4) k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ R1, const double* __restrict__ R2,
-                              const SegP* __restrict__ carry, double* __restrict__ P1h, double* __restrict__ P1l,
+                              const SegP* __restrict__ aggP, double* __restrict__ P1h, double* __restrict__ P1l,
                               double* __restrict__ P2h, double* __restrict__ P2l) {
     if (gate && *gate == 0.0) return;
     __shared__ SegP s_wp[kThreads / 32];
+    const SegP carry = tile_carry(aggP, (int)blockIdx.x, carry_init_P(lo, gstart, P1h, P1l, P2h, P2l), s_wp);
     const int i0 = scan_base(lo) + blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     int f[kScanItems];
     double r1[kScanItems], r2[kScanItems];
@@ -817,7 +822,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanP_write(const double* gate,
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) p = seg_combine(p, SegP{f[q], {r1[q], 0.0}, {r2[q], 0.0}});
     const SegP ex = block_seg_excl(p, s_wp, nullptr);
-    SegP run = seg_combine(carry[blockIdx.x], ex);
+    SegP run = seg_combine(carry, ex);
     #pragma unroll
     for (int q = 0; q < kScanItems; ++q) {
         const int i = i0 + q;
