@@ -562,7 +562,7 @@ __global__ void k_update_grouped(ColView c, const double* delta_ptr, double delt
 // thousand L2-resident values), so no carry-scan launch sits between the
 // passes.
 
-constexpr int kScanItems = 4;
+constexpr int kScanItems = 8;
 constexpr int kScanTile = kThreads * kScanItems;
 
 __device__ __forceinline__ SegD seg_combine(SegD l, SegD r) { return r.f ? r : SegD{l.f, l.v + r.v}; }
@@ -740,8 +740,8 @@ __device__ __forceinline__ T tile_carry(const T* __restrict__ agg, int b, T init
     const int per = (b + (int)blockDim.x - 1) / (int)blockDim.x;
     const int s0 = threadIdx.x * per, s1 = min(b, s0 + per);
     T acc{};                                       // the identity: no segment start, zero sums
-    // several loads in flight at a time (eight D aggregates, four P ones: a
-    // run is at most eight tiles up to 2M groups)
+    // several loads in flight at a time (eight D aggregates, four P ones; a
+    // run is a few tiles: 2M groups are ~1,000 tiles of 2,048)
     constexpr int U = sizeof(T) > 16 ? 4 : 8;
     for (int i = s0; i < s1; i += U) {
         T v[U];
@@ -771,7 +771,7 @@ __device__ __forceinline__ SegP carry_init_P(int lo, const int* __restrict__ gst
 }
 
 // writes D and the P terms r1 = n/D, r2 = n/D^2 (R1, R2) for the P pass
-__global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(kThreads, 3) k_scanD_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ denom, const double* __restrict__ nw,
                               const SegD* __restrict__ aggD, double* __restrict__ D, double* __restrict__ R1,
                               double* __restrict__ R2, SegP* __restrict__ aggP) {
@@ -795,8 +795,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate,
         if (i >= lo && i < hi) {
             run = seg_combine(run, SegD{f[q], v[q]});
             D[i] = run.v;
-            const double r1 = n[q] / run.v;
-            const double r2 = r1 / run.v;
+            const double inv = 1.0 / run.v;            // one division for both terms
+            const double r1 = n[q] * inv;
+            const double r2 = r1 * inv;
             R1[i] = r1;
             R2[i] = r2;
             p = seg_combine(p, SegP{f[q], {r1, 0.0}, {r2, 0.0}});
@@ -807,7 +808,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_scanD_write(const double* gate,
     if (threadIdx.x == 0) aggP[blockIdx.x] = totp;
 }
 
-__global__ void __launch_bounds__(kThreads, 4) k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
+__global__ void __launch_bounds__(kThreads, 3) k_scanP_write(const double* gate, int lo, int hi, const int* __restrict__ gstart,
                               const double* __restrict__ R1, const double* __restrict__ R2,
                               const SegP* __restrict__ aggP, double* __restrict__ P1h, double* __restrict__ P1l,
                               double* __restrict__ P2h, double* __restrict__ P2l) {
