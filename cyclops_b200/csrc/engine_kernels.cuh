@@ -570,27 +570,6 @@ __device__ __forceinline__ SegP seg_combine(SegP l, SegP r) {
     return r.f ? r : SegP{l.f, dd_add(l.a, r.a), dd_add(l.b, r.b)};
 }
 
-// exclusive block scan of per-thread aggregates in thread order; returns the
-// exclusive prefix for this thread and writes the block total to *total
-template <class T>
-__device__ T block_exclusive_scan(T v, T identity, T* total) {
-    __shared__ T buf[kThreads];
-    buf[threadIdx.x] = v;
-    __syncthreads();
-    for (int off = 1; off < blockDim.x; off <<= 1) {
-        T prev = identity;
-        const bool has = threadIdx.x >= off;
-        if (has) prev = buf[threadIdx.x - off];
-        __syncthreads();
-        if (has) buf[threadIdx.x] = seg_combine(prev, buf[threadIdx.x]);
-        __syncthreads();
-    }
-    T excl = threadIdx.x ? buf[threadIdx.x - 1] : identity;
-    if (total) *total = buf[blockDim.x - 1];
-    __syncthreads();
-    return excl;
-}
-
 // The tile kernels: thread t of a tile holds kScanItems consecutive groups
 // (tiles start at multiples of kScanItems, so those loads are aligned vectors; groups
 // below `lo` or at or above `hi` are the identity), sums them in order, and
