@@ -1953,11 +1953,14 @@ static void launch_model(const BatchArgs& a, int ngroups, cudaStream_t stream) {
 
 // One batched solve at precision T over fits [0, F) with starting
 // coefficients `h_beta` (F x J, updated in place) and trust regions.
-// CTAs per cluster when nothing is tuned: one per 16k rows, at most 8;
-// CYC_BATCH_CLUSTER (1..8) forces a size
+// CTAs per cluster when nothing is tuned: one per 8k rows, at most 8 (single
+// fits measured here: 61k rows 12.7 ms a cycle at 8 CTAs against 14.2 at 4,
+// 24k-35k rows 2-3 % faster at 8; up to ~8k rows one CTA is fastest, the
+// cluster barrier costing more than the rows save); CYC_BATCH_CLUSTER (1..8)
+// forces a size
 static int default_cluster(int K) {
     if (const char* e = std::getenv("CYC_BATCH_CLUSTER")) return std::max(1, std::min(kMaxC, std::atoi(e)));
-    return std::max(1, std::min(kMaxC, (K + 16383) / 16384));
+    return std::max(1, std::min(kMaxC, (K + 8191) / 8192));
 }
 
 template <class T>
