@@ -69,6 +69,8 @@ struct BatchArgs {
                                   // launch (the inactive columns of the KKT swindle), or null
     const int* ptype;             // J
     void* xb;                     // [groups][K][G] T
+    int xb_smem;                  // one-fit groups: a CTA keeps its rows' linear predictors in shared
+                                  // memory when they fit (the capacity in rows), 0 = global memory
     const void* w;                // [groups][K][G] T
     double* denom;                // grouped: [groups][S][G]
     const double* nw;             // grouped: [groups][S][G]
@@ -811,6 +813,17 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
     T (*s_m0)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 2 * kDirtyMax * G);
     T (*s_mc)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 3 * kDirtyMax * G);
     T (*s_dw)[G] = reinterpret_cast<T (*)[G]>(s_dirty + 4 * kDirtyMax * G);
+    // one-fit groups whose rows fit: the CTA's linear predictors live in
+    // shared memory for the launch (every access to them is of the CTA's own
+    // rows), loaded here and written back at the end; xbg then addresses
+    // them by absolute row
+    T* const xb_global = xbg;
+    T* const s_xb = s_dirty + 5 * kDirtyMax * G;
+    const bool xb_local = (G == 1) && A.xb_smem > 0 && (r1 - r0) <= A.xb_smem;
+    if (xb_local) {
+        for (int i = threadIdx.x; i < r1 - r0; i += kBT) s_xb[i] = xb_global[r0 + i];
+        xbg = s_xb - r0;                 // rows r0 .. r1 - 1 only
+    }
 
     const bool use_ll = (A.conv == CYC_CONV_MITTAL || A.conv == CYC_CONV_LANGE);
     if (threadIdx.x < G) {
@@ -1494,6 +1507,10 @@ __global__ void __launch_bounds__(kBT, 2) k_batch(const BatchArgs A) {
         for (int f = 0; f < G; ++f) done_m |= (s_done[f] ? 1u : 0u) << f;
         if (s_all_done) break;
     }
+    if (xb_local) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < r1 - r0; i += kBT) xb_global[r0 + i] = s_xb[i];
+    }
     if (C > 1) cluster.sync();   // no CTA leaves while others may still read its shared memory
     if (rank == 0 && threadIdx.x < G) {
         const int f = fg + threadIdx.x;
@@ -1924,7 +1941,7 @@ static void launch_batch(const BatchArgs& a, int ngroups, cudaStream_t stream) {
     cfg.gridDim = dim3(ngroups * a.C);
     cfg.blockDim = dim3(kBT);
     const size_t dyn = 3 * kChunk * G * sizeof(double) + kStage * sizeof(int) + staged_value_bytes<T, MODEL, G>() +
-                       5 * kDirtyMax * G * sizeof(T);
+                       5 * kDirtyMax * G * sizeof(T) + (G == 1 ? (size_t)a.xb_smem * sizeof(T) : 0);
     CYC_CHECK_CUDA(cudaFuncSetAttribute(k_batch<T, MODEL, G, WM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     cfg.dynamicSmemBytes = dyn;
     cfg.stream = stream;
@@ -2168,6 +2185,15 @@ struct BatchRunner {
         a.idx = ds.d_idx.get(); a.val = ds.d_val.get(); a.split = d_split.get(); a.rpart = d_rpart.get();
         a.y = ds.d_y.get(); a.strat = ds.d_strat.get(); a.strat_ptr = ds.d_strat_ptr.get();
         a.fixb = d_fixb.get(); a.lane_fix = d_lfix.get(); a.ptype = d_ptype.get(); a.xb = d_xb.get(); a.w = d_w.get();
+        // one-fit groups keep a CTA's linear predictors in shared memory when
+        // its rows fit in 128 KB (CYC_BATCH_XB_SMEM=0 keeps them in global memory)
+        a.xb_smem = 0;
+        const char* xs = std::getenv("CYC_BATCH_XB_SMEM");
+        if (G == 1 && !(xs && std::atoi(xs) == 0)) {
+            int rows = 0;
+            for (int r = 0; r < C; ++r) rows = std::max(rows, rpart[r + 1] - rpart[r]);
+            if ((size_t)rows * sizeof(T) <= (size_t)128 * 1024) a.xb_smem = rows;
+        }
         a.denom = d_denom.get(); a.nw = d_nw.get(); a.xjy = d_xjy.get(); a.beta = d_beta.get();
         a.hdelta = d_hdelta.get(); a.variance = d_var.get(); a.llfixed = d_llfixed.get(); a.active = d_active.get();
         a.fold = d_fold ? d_fold8.get() : nullptr;
